@@ -1,0 +1,160 @@
+/*
+ * kapsel_gpu.h -- C ABI of the B200 (sm_100a) Smoothed Profile Method step.
+ *
+ * The library replaces KAPSEL's SPM time step, Time_evolution_hydro
+ * (sp_3d_ns.cxx:61-212), and the solver routines it calls.  State (reduced
+ * vorticity, k=0 velocity, particles) lives on the GPU between calls; host
+ * buffers cross the boundary only in the reference's own layouts:
+ *
+ *   - k-space fields in the Ooura layout of the reference: NX*NY*NZ_ doubles,
+ *     NZ_ = NZ+2, index (i*NY + j)*NZ_ + 2*kz (+1 for the imaginary part),
+ *     forward sign exp(+i k.x) (fft_wrapper.h:432-631);
+ *   - real-space fields as NX*NY*NZ_ doubles with the same padded stride
+ *     (sp_3d_ns.cxx:392-440 allocates every field this way);
+ *   - particles as the reference Particle fields, see KAPSEL_P_* below
+ *     (variable.h:27-75).
+ *
+ * Every entry point returns 0 on success or a negative KAPSEL_E* status; the
+ * library never exits the process (the reference calls exit_job, macro.h:194).
+ * One context owns one CUDA stream; contexts are independent.
+ */
+#ifndef KAPSEL_GPU_H
+#define KAPSEL_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KAPSEL_OK 0
+#define KAPSEL_EINVAL -1     /* bad argument or unsupported configuration */
+#define KAPSEL_ECUDA -2      /* a CUDA runtime call failed */
+#define KAPSEL_ENOMEM -3     /* device allocation failed */
+#define KAPSEL_ESTATE -4     /* call out of order (e.g. step before init) */
+#define KAPSEL_ENONFINITE -5 /* a NaN/Inf was detected in the particle state */
+#define KAPSEL_ERANGE -6     /* a particle left the box or a size limit was exceeded */
+
+#define KAPSEL_FP64 0  /* all fields and FFTs in double precision */
+#define KAPSEL_MIXED 1 /* fields/FFTs/stencils in float, particles and reductions in double */
+
+#define KAPSEL_EQ_NAVIER_STOKES 0 /* EQ::Navier_Stokes (input.h:49) */
+#define KAPSEL_EQ_ELECTROLYTE 3   /* EQ::Electrolyte (input.h:52) */
+
+/* Per-particle record layout used by kapsel_gpu_get_particles (doubles). */
+#define KAPSEL_P_X 0         /* x[3]                      */
+#define KAPSEL_P_V 3         /* v[3]                      */
+#define KAPSEL_P_OMEGA 6     /* omega[3]                  */
+#define KAPSEL_P_FHYDRO 9    /* f_hydro_previous[3]       */
+#define KAPSEL_P_THYDRO 12   /* torque_hydro_previous[3]  */
+#define KAPSEL_P_FR 15       /* fr_previous[3]            */
+#define KAPSEL_P_XNOPBC 18   /* x_nopbc[3]                */
+#define KAPSEL_P_VOLD 21     /* v_old[3]                  */
+#define KAPSEL_P_OMEGAOLD 24 /* omega_old[3]              */
+#define KAPSEL_P_Q 27        /* q (s, v0, v1, v2)         */
+#define KAPSEL_P_QOLD 31     /* q_old (s, v0, v1, v2)     */
+#define KAPSEL_P_STRIDE 35
+
+/* Physical and numerical parameters: the values Gourmet_file_io reads from
+   the UDF (input.cxx:438-1818) for one spherical-particle species. */
+typedef struct kapsel_params {
+  int np_xyz[3];       /* grid N = 1 << np per axis (input.cxx:1392-1397) */
+  int eq;              /* KAPSEL_EQ_* */
+  int precision;       /* KAPSEL_FP64 or KAPSEL_MIXED */
+  int n_particles;     /* Particle_Number (one species) */
+  double dx, rho, eta, kbt, alpha_v, alpha_o, dt;
+  double a, a_xi;      /* radius and interface thickness in units of DX */
+  double mass_ratio;   /* MASS_RATIO of the species */
+  double gravity_g;    /* G (gravity.G) */
+  int gravity_dir;     /* 0,1,2 for "-X","-Y","-Z" */
+  double epsilon;      /* LJ EPSILON */
+  int lj_powers;       /* 0: 12:6, 1: 24:12, 2: 36:18 */
+  int lj_truncate;     /* 1 ON, 0 OFF, -1 NONE */
+  int rotation;        /* switch.ROTATION */
+  int fix_cell[3];     /* switch.FIX_CELL.{x,y,z} */
+  unsigned int mt_seed;/* MT19937 seed of the thermostat (reference: 0) */
+  /* Electrolyte branch (ignored for Navier_Stokes) */
+  double dielectric, surface_charge, debye_length;
+  double valency_p, valency_n, onsager_p, onsager_n;
+  double e_ext[3];
+} kapsel_params;
+
+typedef struct kapsel_ctx kapsel_ctx;
+
+/* Fill p with the reference defaults (input.udf; 64^3, a=5, xi=2, dt=0.01). */
+void kapsel_params_default(kapsel_params *p);
+
+/* Create a context on the current CUDA device.  Replaces the allocations of
+   Mem_alloc_var (sp_3d_ns.cxx:392-440) and Init_fft (fft_wrapper.cxx:92-101). */
+int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out);
+int kapsel_gpu_destroy(kapsel_ctx *ctx);
+
+/* Particle positions (n*3) and orientations (n*4 quaternions s,v0,v1,v2, or
+   NULL for identity) as read by the user_specify initialiser
+   (init_particle.cxx:226-288); velocities start at zero (:357-370). */
+int kapsel_gpu_set_particles(kapsel_ctx *ctx, const double *x, const double *q);
+
+/* Initial fluid state of main(): Init_zeta_k and the initial rigidity
+   projection, then uk_dc = 0 (sp_3d_ns.cxx:508-524). */
+int kapsel_gpu_init_state(kapsel_ctx *ctx);
+
+/* n calls of Time_evolution_hydro (sp_3d_ns.cxx:61-212) with
+   jikan.time += dt after each (sp_3d_ns.cxx:593-594). */
+int kapsel_gpu_step(kapsel_ctx *ctx, int n);
+
+/* As kapsel_gpu_step, but the step sequence is captured once into a CUDA
+   graph and replayed (same results). */
+int kapsel_gpu_step_graph(kapsel_ctx *ctx, int n);
+
+/* Reduced vorticity zeta[2] in the Ooura layout (2*NX*NY*NZ_ doubles) and
+   uk_dc[3]; modes outside the 2/3 box are zero.  (Save_Restart_udf data,
+   resume.cxx:10-78.) */
+int kapsel_gpu_get_zeta(kapsel_ctx *ctx, double *zeta, double *uk_dc);
+int kapsel_gpu_set_zeta(kapsel_ctx *ctx, const double *zeta, const double *uk_dc);
+
+/* Real velocity field u = Zeta_k2u(zeta, uk_dc) (operate_omega.h:124-128)
+   of the current state, 3*NX*NY*NZ_ doubles (padding left untouched). */
+int kapsel_gpu_get_velocity(kapsel_ctx *ctx, double *u);
+
+/* Particle records, n_particles * KAPSEL_P_STRIDE doubles. */
+int kapsel_gpu_get_particles(kapsel_ctx *ctx, double *out);
+int kapsel_gpu_set_particle_state(kapsel_ctx *ctx, const double *in);
+
+/* Time step counter jikan.ts and time jikan.time. */
+int kapsel_gpu_get_time(kapsel_ctx *ctx, int *ts, double *time);
+
+/* Grid sizes: dims[0..5] = NX, NY, NZ, NZ_, n_particles, sekibun points. */
+int kapsel_gpu_get_dims(kapsel_ctx *ctx, int *dims);
+
+/* External electric field E_ext (operate_electrolyte.cxx:90-177). */
+int kapsel_gpu_set_efield(kapsel_ctx *ctx, const double *e);
+
+/* ---- Routine-level entry points on host arrays (reference layouts). ---- */
+
+/* A2a_k / A_k2a (fft_wrapper.h:432-631): in-place forward / inverse 3D real
+   FFT of one NX*NY*NZ_ field with the Ooura sign and scaling. */
+int kapsel_gpu_A2a_k(kapsel_ctx *ctx, double *a);
+int kapsel_gpu_A_k2a(kapsel_ctx *ctx, double *a);
+
+/* Solenoidal_u (operate_omega.h:96-103) on three real NX*NY*NZ_ fields. */
+int kapsel_gpu_solenoidal_u(kapsel_ctx *ctx, double *u0, double *u1, double *u2);
+
+/* Make_phi_u_particle (make_phi.cxx:401-409, with the phi>1 clamp of
+   :278-297) for the context's particles: phi and up[3] as NX*NY*NZ_ fields. */
+int kapsel_gpu_make_phi_u(kapsel_ctx *ctx, double *phi, double *up0, double *up1, double *up2);
+
+/* Calc_f_hydro_correct_precision (md_force.cxx:263-389) for the context's
+   particles on the given velocity field; writes f_hydro[n*3], torque[n*3]. */
+int kapsel_gpu_calc_f_hydro(kapsel_ctx *ctx, const double *u0, const double *u1, const double *u2,
+                            double *f_hydro, double *torque_hydro);
+
+/* Calc_f_Lennard_Jones + Add_f_gravity (particle_solver.h:97-109) for the
+   context's particles; writes fr[n*3]. */
+int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr);
+
+/* Human-readable text of a status code. */
+const char *kapsel_gpu_strerror(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KAPSEL_GPU_H */

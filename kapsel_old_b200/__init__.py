@@ -1,0 +1,289 @@
+"""kapsel_old_b200 -- B200-native Smoothed Profile Method step for KAPSEL.
+
+Python mirror of the C ABI in include/kapsel_gpu.h (libkapsel_gpu.so, built
+in-tree by kapsel_old_b200/build.py).  The reference is a C++ program whose
+SPM step is Time_evolution_hydro (sp_3d_ns.cxx:61-212); this module exposes
+the same state (zeta, uk_dc, particles) and the routine-level entry points
+(A2a_k, A_k2a, Solenoidal_u, Make_phi_u_particle, Calc_f_hydro_correct_precision,
+Force) on numpy arrays in the reference's own layouts.
+
+There is no CPU fallback: importing the library fails loudly when the CUDA
+extension is missing, and every call raises KapselError on a non-zero status.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libkapsel_gpu.so")
+
+FP64 = 0
+MIXED = 1
+EQ_NAVIER_STOKES = 0
+EQ_ELECTROLYTE = 3
+P_STRIDE = 35
+
+
+class KapselError(RuntimeError):
+    pass
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [
+        ("np_xyz", ctypes.c_int * 3),
+        ("eq", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("n_particles", ctypes.c_int),
+        ("dx", ctypes.c_double),
+        ("rho", ctypes.c_double),
+        ("eta", ctypes.c_double),
+        ("kbt", ctypes.c_double),
+        ("alpha_v", ctypes.c_double),
+        ("alpha_o", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("a", ctypes.c_double),
+        ("a_xi", ctypes.c_double),
+        ("mass_ratio", ctypes.c_double),
+        ("gravity_g", ctypes.c_double),
+        ("gravity_dir", ctypes.c_int),
+        ("epsilon", ctypes.c_double),
+        ("lj_powers", ctypes.c_int),
+        ("lj_truncate", ctypes.c_int),
+        ("rotation", ctypes.c_int),
+        ("fix_cell", ctypes.c_int * 3),
+        ("mt_seed", ctypes.c_uint),
+        ("dielectric", ctypes.c_double),
+        ("surface_charge", ctypes.c_double),
+        ("debye_length", ctypes.c_double),
+        ("valency_p", ctypes.c_double),
+        ("valency_n", ctypes.c_double),
+        ("onsager_p", ctypes.c_double),
+        ("onsager_n", ctypes.c_double),
+        ("e_ext", ctypes.c_double * 3),
+    ]
+
+
+_lib = None
+
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+_VP = ctypes.c_void_p
+
+
+def load_library(path: str | None = None) -> ctypes.CDLL:
+    """Load libkapsel_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise KapselError(f"{path} is missing: run kapsel_old_b200.build.build() (nvcc, sm_100a)")
+    L = ctypes.CDLL(path)
+    sig = {
+        "kapsel_params_default": (None, [ctypes.POINTER(_Params)]),
+        "kapsel_gpu_create": (ctypes.c_int, [ctypes.POINTER(_Params), ctypes.POINTER(_VP)]),
+        "kapsel_gpu_destroy": (ctypes.c_int, [_VP]),
+        "kapsel_gpu_set_particles": (ctypes.c_int, [_VP, _DP, _DP]),
+        "kapsel_gpu_init_state": (ctypes.c_int, [_VP]),
+        "kapsel_gpu_step": (ctypes.c_int, [_VP, ctypes.c_int]),
+        "kapsel_gpu_step_graph": (ctypes.c_int, [_VP, ctypes.c_int]),
+        "kapsel_gpu_get_zeta": (ctypes.c_int, [_VP, _DP, _DP]),
+        "kapsel_gpu_set_zeta": (ctypes.c_int, [_VP, _DP, _DP]),
+        "kapsel_gpu_get_velocity": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_get_particles": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_set_particle_state": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_get_time": (ctypes.c_int, [_VP, _IP, _DP]),
+        "kapsel_gpu_get_dims": (ctypes.c_int, [_VP, _IP]),
+        "kapsel_gpu_set_efield": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_A2a_k": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_A_k2a": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_solenoidal_u": (ctypes.c_int, [_VP, _DP, _DP, _DP]),
+        "kapsel_gpu_make_phi_u": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP]),
+        "kapsel_gpu_calc_f_hydro": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP, _DP]),
+        "kapsel_gpu_calc_fr": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_DP)
+
+
+def params_from_config(cfg: dict, precision: int = FP64) -> _Params:
+    """Build kapsel_params from a configuration dict (the UDF values of one
+    spherical-particle species; keys as in oracle/udf.py)."""
+    L = load_library()
+    p = _Params()
+    L.kapsel_params_default(ctypes.byref(p))
+    for d in range(3):
+        p.np_xyz[d] = int(cfg["np_xyz"][d])
+    p.eq = EQ_ELECTROLYTE if cfg.get("eq", "Navier_Stokes") == "Electrolyte" else EQ_NAVIER_STOKES
+    p.precision = precision
+    p.n_particles = len(cfg.get("particles", []))
+    p.dx = float(cfg.get("dx", 1.0))
+    p.rho = float(cfg.get("rho", 1.0))
+    p.eta = float(cfg.get("eta", 1.0))
+    p.kbt = float(cfg.get("kbt", 0.0))
+    p.alpha_v = float(cfg.get("alpha_v", 1.0))
+    p.alpha_o = float(cfg.get("alpha_o", 1.0))
+    p.dt = float(cfg.get("dt", 0.01))
+    p.a = float(cfg.get("a", 5.0))
+    p.a_xi = float(cfg.get("a_xi", 2.0))
+    p.mass_ratio = float(cfg.get("mass_ratio", 1.0))
+    p.gravity_g = float(cfg.get("gravity_g", 0.0))
+    p.gravity_dir = {"-X": 0, "-Y": 1, "-Z": 2}[cfg.get("gravity_dir", "-Z")]
+    p.epsilon = float(cfg.get("epsilon", 1.0))
+    p.lj_powers = {"12:6": 0, "24:12": 1, "36:18": 2}[cfg.get("lj_powers", "12:6")]
+    p.lj_truncate = {"ON": 1, "OFF": 0, "NONE": -1}[cfg.get("lj_truncate", "ON")]
+    p.rotation = 1 if cfg.get("rotation", "ON") == "ON" else 0
+    fc = cfg.get("fix_cell", (False, False, False))
+    for d in range(3):
+        p.fix_cell[d] = 1 if fc[d] else 0
+    p.mt_seed = int(cfg.get("mt_seed", 0))
+    return p
+
+
+class Simulation:
+    """One SPM box on the GPU (one kapsel_ctx)."""
+
+    def __init__(self, cfg: dict, precision: int = FP64, init: bool = True):
+        self.L = load_library()
+        self.cfg = cfg
+        self.precision = precision
+        self._p = params_from_config(cfg, precision)
+        h = _VP()
+        self._check(self.L.kapsel_gpu_create(ctypes.byref(self._p), ctypes.byref(h)))
+        self.h = h
+        d = (ctypes.c_int * 6)()
+        self._check(self.L.kapsel_gpu_get_dims(self.h, d))
+        self.NX, self.NY, self.NZ, self.NZ_, self.Np, self.S = list(d)
+        if self.Np > 0:
+            x = np.ascontiguousarray([p["x"] for p in cfg["particles"]], dtype=np.float64)
+            qs = [p.get("q") for p in cfg["particles"]]
+            q = None if all(v is None for v in qs) else np.ascontiguousarray(
+                [v if v is not None else (1.0, 0.0, 0.0, 0.0) for v in qs], dtype=np.float64)
+            self._check(self.L.kapsel_gpu_set_particles(self.h, _ptr(x), _ptr(q) if q is not None else None))
+        if init:
+            self.init_state()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = load_library().kapsel_gpu_strerror(rc).decode()
+            raise KapselError(f"kapsel_gpu status {rc}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.kapsel_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- state evolution
+    def init_state(self):
+        self._check(self.L.kapsel_gpu_init_state(self.h))
+
+    def step(self, n: int = 1, graph: bool = False):
+        f = self.L.kapsel_gpu_step_graph if graph else self.L.kapsel_gpu_step
+        self._check(f(self.h, int(n)))
+
+    def time(self):
+        ts = ctypes.c_int()
+        t = ctypes.c_double()
+        self._check(self.L.kapsel_gpu_get_time(self.h, ctypes.byref(ts), ctypes.byref(t)))
+        return ts.value, t.value
+
+    # ---- state readout in the reference layouts
+    def zeta(self) -> np.ndarray:
+        z = np.zeros((2, self.NX, self.NY, self.NZ_))
+        self._check(self.L.kapsel_gpu_get_zeta(self.h, _ptr(z), None))
+        return z
+
+    def uk_dc(self) -> np.ndarray:
+        z = np.zeros((2, self.NX, self.NY, self.NZ_))
+        u = np.zeros(3)
+        self._check(self.L.kapsel_gpu_get_zeta(self.h, _ptr(z), _ptr(u)))
+        return u
+
+    def set_zeta(self, zeta: np.ndarray, uk_dc):
+        z = np.ascontiguousarray(zeta, dtype=np.float64)
+        u = np.ascontiguousarray(uk_dc, dtype=np.float64)
+        self._check(self.L.kapsel_gpu_set_zeta(self.h, _ptr(z), _ptr(u)))
+
+    def velocity(self) -> np.ndarray:
+        """u = Zeta_k2u(zeta, uk_dc), shape (3, NX, NY, NZ)."""
+        u = np.zeros((3, self.NX, self.NY, self.NZ_))
+        self._check(self.L.kapsel_gpu_get_velocity(self.h, _ptr(u)))
+        return u[..., : self.NZ].copy()
+
+    def particles(self) -> dict:
+        a = np.zeros((max(self.Np, 1), P_STRIDE))
+        self._check(self.L.kapsel_gpu_get_particles(self.h, _ptr(a)))
+        a = a[: self.Np]
+        names = ["x", "v", "omega", "f_hydro", "torque_hydro", "fr", "x_nopbc", "v_old", "omega_old"]
+        out = {n: a[:, 3 * i: 3 * i + 3].copy() for i, n in enumerate(names)}
+        out["q"] = a[:, 27:31].copy()
+        out["q_old"] = a[:, 31:35].copy()
+        return out
+
+    def set_particle_state(self, st: dict):
+        a = np.zeros((max(self.Np, 1), P_STRIDE))
+        names = ["x", "v", "omega", "f_hydro", "torque_hydro", "fr", "x_nopbc", "v_old", "omega_old"]
+        for i, n in enumerate(names):
+            a[: self.Np, 3 * i: 3 * i + 3] = st[n]
+        a[: self.Np, 27:31] = st["q"]
+        a[: self.Np, 31:35] = st["q_old"]
+        self._check(self.L.kapsel_gpu_set_particle_state(self.h, _ptr(a)))
+
+    # ---- routine-level entry points (reference layouts, NX*NY*NZ_ doubles)
+    def _padded(self, a):
+        b = np.zeros((self.NX, self.NY, self.NZ_))
+        b[:, :, : a.shape[2]] = a
+        return b
+
+    def A2a_k(self, a: np.ndarray) -> np.ndarray:
+        b = self._padded(a)
+        self._check(self.L.kapsel_gpu_A2a_k(self.h, _ptr(b)))
+        return b
+
+    def A_k2a(self, ak: np.ndarray) -> np.ndarray:
+        b = np.ascontiguousarray(ak, dtype=np.float64).copy()
+        self._check(self.L.kapsel_gpu_A_k2a(self.h, _ptr(b)))
+        return b[:, :, : self.NZ].copy()
+
+    def solenoidal_u(self, u: np.ndarray) -> np.ndarray:
+        b = [self._padded(u[d]) for d in range(3)]
+        self._check(self.L.kapsel_gpu_solenoidal_u(self.h, _ptr(b[0]), _ptr(b[1]), _ptr(b[2])))
+        return np.stack([x[:, :, : self.NZ] for x in b])
+
+    def make_phi_u(self):
+        f = [np.zeros((self.NX, self.NY, self.NZ_)) for _ in range(4)]
+        self._check(self.L.kapsel_gpu_make_phi_u(self.h, *[_ptr(x) for x in f]))
+        return f[0][:, :, : self.NZ].copy(), np.stack([x[:, :, : self.NZ] for x in f[1:]])
+
+    def calc_f_hydro(self, u: np.ndarray):
+        b = [self._padded(u[d]) for d in range(3)]
+        f = np.zeros((max(self.Np, 1), 3))
+        t = np.zeros((max(self.Np, 1), 3))
+        self._check(self.L.kapsel_gpu_calc_f_hydro(self.h, _ptr(b[0]), _ptr(b[1]), _ptr(b[2]), _ptr(f), _ptr(t)))
+        return f[: self.Np], t[: self.Np]
+
+    def calc_fr(self) -> np.ndarray:
+        f = np.zeros((max(self.Np, 1), 3))
+        self._check(self.L.kapsel_gpu_calc_fr(self.h, _ptr(f)))
+        return f[: self.Np]
+
+
+__all__ = ["Simulation", "KapselError", "load_library", "params_from_config", "FP64", "MIXED", "LIB_PATH"]

@@ -1,0 +1,1128 @@
+// kapsel_gpu.cu -- host side of the B200 SPM step: context, buffers, launch
+// sequence, CUDA graph replay and the C ABI declared in include/kapsel_gpu.h.
+//
+// One SPM step (Time_evolution_hydro, sp_3d_ns.cxx:61-212, Navier_Stokes
+// branch) is 13 launches:
+//   1 k_x_zeta_to_u        truncated zeta -> u_k -> inverse x
+//   2 k_y_pass<inv>        inverse y (3 comps)
+//   3 k_z_products         inverse z, 5 products, forward z
+//   4 k_y_pass<fwd>        forward y (5 comps)
+//   5 k_x_advect_update    forward x, Omega, slaved Euler, FIX_CELL, u*_k, inverse x
+//   6 k_y_pass<inv>        inverse y (3 comps)
+//   7 k_z_c2r              inverse z -> u* (real)
+//   8 k_particles_position AB2 / Euler positions and orientations
+//   9 k_particles_hydro_velocity  hydro force+torque gather, LJ, gravity, velocity, thermostat
+//  10 k_particles_scatter  phi, phi*u_p
+//  11 k_z_force            clamp, f = up - phi u*, forward z, clear phi/up
+//  12 k_y_pass<fwd>        forward y (3 comps)
+//  13 k_x_force_to_zeta    forward x, solenoidal projection, zeta += zeta(f), uk_dc += f(0)
+// The 20 3D FFTs of the reference become 14 pruned ones because
+// U2zeta_k(u* + f_sol) = trunc(zeta) + U_k2zeta_k(f_sol) (linearity).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "../../include/kapsel_gpu.h"
+#include "particle_kernels.cuh"
+#include "spectral_kernels.cuh"
+
+using namespace kapsel;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// MT19937 (Matsumoto & Nishimura 1998) with the init_genrand seeding, the
+// generator behind the reference thermostat (mt19937ar.c, seeded with 0 by
+// MT_seed at sp_3d_ns.cxx:477).  Written from the published algorithm.
+class MT19937 {
+ public:
+  explicit MT19937(uint32_t s) { seed(s); }
+  void seed(uint32_t s) {
+    mt_[0] = s;
+    for (int i = 1; i < 624; ++i) mt_[i] = 1812433253u * (mt_[i - 1] ^ (mt_[i - 1] >> 30)) + (uint32_t)i;
+    idx_ = 624;
+  }
+  uint32_t next() {
+    if (idx_ >= 624) twist();
+    uint32_t y = mt_[idx_++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+  }
+  // genrand_real3: (y + 0.5) / 2^32, in (0,1)
+  double real3() { return ((double)next() + 0.5) * (1.0 / 4294967296.0); }
+  // Gauss2 (fluct.h:48-60): polar Box-Muller pair
+  void gauss2(double *out) {
+    double x1, x2, rsq;
+    do {
+      x1 = 2. * real3() - 1.;
+      x2 = 2. * real3() - 1.;
+      rsq = x1 * x1 + x2 * x2;
+    } while (rsq >= 1.0 || rsq == 0.0);
+    const double f = std::sqrt(-2. * std::log(rsq) / rsq);
+    out[0] = f * x1;
+    out[1] = f * x2;
+  }
+
+ private:
+  void twist() {
+    for (int i = 0; i < 624; ++i) {
+      const uint32_t y = (mt_[i] & 0x80000000u) | (mt_[(i + 1) % 624] & 0x7fffffffu);
+      mt_[i] = mt_[(i + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+    }
+    idx_ = 0;
+  }
+  uint32_t mt_[624];
+  int idx_;
+};
+
+int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return l;
+}
+
+#define KCHECK(call)                                         \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) {                                 \
+      fprintf(stderr, "kapsel_gpu: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return KAPSEL_ECUDA;                                   \
+    }                                                        \
+  } while (0)
+
+// Sekibun stencil offsets (Particle_domain, profile.cxx:25-74): points with
+// |(i,j,k) DX| < RADIUS + HXI + 1.7321 DX, scanned i, j, k from -nh to nh.
+std::vector<int> sekibun(double A, double A_XI, double DX) {
+  const double radius = A * DX, hxi = 0.5 * A_XI * DX;
+  const int nh = (int)A + (int)A_XI + 2;
+  const double max_r = radius + hxi + 1.7321 * DX;
+  std::vector<int> out;
+  for (int i = -nh; i <= nh; ++i)
+    for (int j = -nh; j <= nh; ++j)
+      for (int k = -nh; k <= nh; ++k) {
+        const double x = i * DX, y = j * DX, z = k * DX;
+        if (std::sqrt(x * x + y * y + z * z) < max_r) {
+          out.push_back(i);
+          out.push_back(j);
+          out.push_back(k);
+        }
+      }
+  return out;
+}
+
+template <typename R, bool INVERSE>
+__global__ void k_col_pass(Geo g, const Cx<R> *twn, int logn, int n, const Cx<R> *in, Cx<R> *out,
+                           long long line_stride, long long elem_stride, int nlines);
+template <typename R>
+__global__ void k_z_c2r_full(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in, R *__restrict__ out, double scale);
+
+// ---------------------------------------------------------------------------
+struct BoxBase {
+  virtual ~BoxBase() {}
+  kapsel_params prm;
+  Geo g;
+  PPar pp;
+  int Np = 0, S = 0;
+  cudaStream_t stream = nullptr;
+  DPart *parts = nullptr;
+  int *cells = nullptr;
+  double *uk_dc = nullptr;
+  int *status = nullptr;
+  double *noise_dev[2] = {nullptr, nullptr};
+  double *noise_host[2] = {nullptr, nullptr};
+  cudaEvent_t noise_ev[2] = {nullptr, nullptr};
+  std::unique_ptr<MT19937> mt;
+  int ts = 0;
+  double time = 0.0;
+  bool initialised = false;
+  bool particles_set = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+
+  virtual int alloc() = 0;
+  virtual void launch_step(const double *noise, int euler) = 0;
+  virtual void launch_init() = 0;
+  virtual int velocity_to_host(double *u) = 0;
+  virtual int zeta_to_host(double *z) = 0;
+  virtual int zeta_from_host(const double *z) = 0;
+  virtual int fft_fwd_host(double *a) = 0;
+  virtual int fft_inv_host(double *a) = 0;
+  virtual int solenoidal_host(double *u0, double *u1, double *u2) = 0;
+  virtual int phi_up_host(double *phi, double *up0, double *up1, double *up2) = 0;
+  virtual int fhydro_host(const double *u0, const double *u1, const double *u2, double *f, double *t) = 0;
+  virtual void free_all() = 0;
+
+  int fill_noise(int slot) {
+    // the normals one call of Add_random_force_thermostat consumes, in order
+    // (fluct.cxx:21-35: Gauss2 x3 per particle)
+    if (!pp.thermostat) return 0;
+    KCHECK(cudaEventSynchronize(noise_ev[slot]));
+    double *h = noise_host[slot];
+    for (int n = 0; n < Np; ++n) {
+      mt->gauss2(h + 6 * n);
+      mt->gauss2(h + 6 * n + 2);
+      mt->gauss2(h + 6 * n + 4);
+    }
+    KCHECK(cudaMemcpyAsync(noise_dev[slot], h, sizeof(double) * 6 * Np, cudaMemcpyHostToDevice, stream));
+    KCHECK(cudaEventRecord(noise_ev[slot], stream));
+    return 0;
+  }
+};
+
+template <typename R>
+struct Box : BoxBase {
+  Cx<R> *zeta = nullptr;  // [2][KXc][KYc][TZ]
+  Cx<R> *bufA = nullptr;  // I1-shaped, 5 comps [c][NX][KYc][TZ]
+  Cx<R> *bufB = nullptr;  // I2-shaped, 5 comps [c][NX][NY][TZ]
+  R *ustar = nullptr;     // [3][NX][NY][NZ]
+  R *phiup = nullptr;     // [4][NX][NY][NZ]
+  Cx<R> *twbuf = nullptr;
+  Twiddles<R> tw;
+  int KCX = 16, KCY = 16;
+  size_t smem_xu = 0, smem_xadv = 0, smem_xf = 0, smem_y = 0, smem_zp = 0, smem_zc = 0, smem_zf = 0;
+
+  size_t npts() const { return (size_t)g.NX * g.NY * g.NZ; }
+
+  int alloc() override {
+    KCX = sizeof(R) == 4 ? 16 : 8;
+    KCY = 16;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    const size_t nA = (size_t)g.NX * g.KYc * g.TZ;
+    const size_t nB = (size_t)g.NX * g.NY * g.TZ;
+    KCHECK(cudaMalloc(&zeta, sizeof(Cx<R>) * 2 * nz));
+    KCHECK(cudaMalloc(&bufA, sizeof(Cx<R>) * 5 * nA));
+    KCHECK(cudaMalloc(&bufB, sizeof(Cx<R>) * 5 * nB));
+    KCHECK(cudaMalloc(&ustar, sizeof(R) * 3 * npts()));
+    KCHECK(cudaMalloc(&phiup, sizeof(R) * 4 * npts()));
+    KCHECK(cudaMemset(zeta, 0, sizeof(Cx<R>) * 2 * nz));
+    KCHECK(cudaMemset(ustar, 0, sizeof(R) * 3 * npts()));
+    KCHECK(cudaMemset(phiup, 0, sizeof(R) * 4 * npts()));
+    // twiddles exp(+2 pi i j/n), computed in double
+    const int ns[4] = {g.NX, g.NY, g.M, g.NZ};
+    std::vector<Cx<R>> h;
+    size_t off[4];
+    for (int t = 0; t < 4; ++t) {
+      off[t] = h.size();
+      for (int j = 0; j < ns[t]; ++j) {
+        const double a = 2.0 * M_PI * (double)j / (double)ns[t];
+        h.push_back({(R)std::cos(a), (R)std::sin(a)});
+      }
+    }
+    KCHECK(cudaMalloc(&twbuf, sizeof(Cx<R>) * h.size()));
+    KCHECK(cudaMemcpy(twbuf, h.data(), sizeof(Cx<R>) * h.size(), cudaMemcpyHostToDevice));
+    tw.x = twbuf + off[0];
+    tw.y = twbuf + off[1];
+    tw.m = twbuf + off[2];
+    tw.z = twbuf + off[3];
+    const size_t C = sizeof(Cx<R>);
+    const int P = g.M + 1;
+    smem_xu = C * (g.NX + (size_t)g.NX * 3 * KCX);
+    smem_xadv = C * (g.NX + (size_t)g.KXc * 2 * KCX + (size_t)g.NX * 5 * KCX);
+    smem_xf = C * (g.NX + (size_t)g.NX * 3 * KCX);
+    smem_y = C * (g.NY + (size_t)g.NY * KCY);
+    smem_zp = C * (g.M + g.NZ + (size_t)ZROWS * 8 * P);
+    smem_zc = C * (g.M + g.NZ + (size_t)ZROWS * P);
+    smem_zf = C * (g.M + g.NZ + (size_t)ZROWS * 3 * P);
+    const size_t mx = 227 * 1024;
+    if (smem_xadv > mx || smem_xu > mx || smem_y > mx || smem_zp > mx) return KAPSEL_ERANGE;
+    KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
+    KCHECK(cudaFuncSetAttribute(k_x_advect_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xadv));
+    KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xf));
+    KCHECK(cudaFuncSetAttribute(k_y_pass<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
+    KCHECK(cudaFuncSetAttribute(k_y_pass<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
+    KCHECK(cudaFuncSetAttribute(k_z_products<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zp));
+    KCHECK(cudaFuncSetAttribute(k_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
+    KCHECK(cudaFuncSetAttribute(k_z_r2c_full<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
+    KCHECK(cudaFuncSetAttribute(k_z_force<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zf));
+    const int nmax = std::max(g.NX, g.NY);
+    const int smem_col = (int)(C * ((size_t)nmax + (size_t)nmax * 16));
+    KCHECK(cudaFuncSetAttribute(k_col_pass<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_col));
+    KCHECK(cudaFuncSetAttribute(k_col_pass<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_col));
+    KCHECK(cudaFuncSetAttribute(k_z_c2r_full<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
+    return 0;
+  }
+
+  dim3 gx() const { return dim3(g.KYc, (g.TZ + KCX - 1) / KCX); }
+  dim3 gy(int nc) const { return dim3(g.NX, nc, (g.TZ + KCY - 1) / KCY); }
+  int gz() const { return (g.NX * g.NY) / ZROWS; }
+
+  // zeta -> u* (real) through launches 1,2,(7); used by the velocity readout
+  void launch_zeta_to_real(R *out, size_t cstride, int pitch) {
+    k_x_zeta_to_u<R><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA, KCX);
+    k_y_pass<R, true><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB, KCY);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, out, cstride, pitch);
+  }
+
+  // f (from phi/up and u*) -> zeta update, launches 11-13
+  void launch_force_to_zeta() {
+    k_z_force<R><<<gz(), 256, smem_zf, stream>>>(g, tw, phiup, ustar, bufB);
+    k_y_pass<R, false><<<gy(3), 256, smem_y, stream>>>(g, tw, bufB, bufA, KCY);
+    k_x_force_to_zeta<R><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc, KCX);
+  }
+
+  void launch_step(const double *noise, int euler) override {
+    k_x_zeta_to_u<R><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA, KCX);
+    k_y_pass<R, true><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB, KCY);
+    k_z_products<R><<<gz(), 256, smem_zp, stream>>>(g, tw, bufB);
+    k_y_pass<R, false><<<gy(5), 256, smem_y, stream>>>(g, tw, bufB, bufA, KCY);
+    k_x_advect_update<R><<<gx(), 256, smem_xadv, stream>>>(g, tw, bufA, zeta, uk_dc, KCX);
+    k_y_pass<R, true><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB, KCY);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, npts(), g.NZ);
+    if (Np > 0) {
+      k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
+      k_particles_hydro_velocity<R><<<Np, 256, 0, stream>>>(pp, parts, ustar, cells, noise, euler, status);
+      k_particles_scatter<R><<<Np, 256, 0, stream>>>(pp, parts, cells, phiup);
+      launch_force_to_zeta();
+    }
+  }
+
+  void launch_init() override {
+    // Init_zeta_k gives zeta = 0 and u = 0 (init_fluid.cxx:10-26); the
+    // initial rigidity projection (sp_3d_ns.cxx:510-524) is then
+    // zeta = U2zeta_k(Solenoidal_u(up - phi*0)), followed by uk_dc = 0.
+    cudaMemsetAsync(zeta, 0, sizeof(Cx<R>) * 2 * (size_t)g.KXc * g.KYc * g.TZ, stream);
+    cudaMemsetAsync(ustar, 0, sizeof(R) * 3 * npts(), stream);
+    cudaMemsetAsync(uk_dc, 0, sizeof(double) * 3, stream);
+    if (Np > 0) {
+      k_particles_scatter<R><<<Np, 256, 0, stream>>>(pp, parts, cells, phiup);
+      launch_force_to_zeta();
+    }
+    cudaMemsetAsync(uk_dc, 0, sizeof(double) * 3, stream);
+  }
+
+  // ---- host <-> device helpers in the reference layouts
+  int velocity_to_host(double *u) override {
+    R *tmp = nullptr;
+    KCHECK(cudaMallocAsync(&tmp, sizeof(R) * 3 * npts(), stream));
+    launch_zeta_to_real(tmp, npts(), g.NZ);
+    std::vector<R> h(3 * npts());
+    KCHECK(cudaMemcpyAsync(h.data(), tmp, sizeof(R) * h.size(), cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaFreeAsync(tmp, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    const int NZ_ = g.NZ + 2;
+    for (int c = 0; c < 3; ++c)
+      for (size_t r = 0; r < (size_t)g.NX * g.NY; ++r)
+        for (int k = 0; k < g.NZ; ++k)
+          u[c * (size_t)g.NX * g.NY * NZ_ + r * NZ_ + k] = (double)h[c * npts() + r * g.NZ + k];
+    return 0;
+  }
+
+  int zeta_to_host(double *z) override {
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    std::vector<Cx<R>> h(2 * nz);
+    KCHECK(cudaMemcpyAsync(h.data(), zeta, sizeof(Cx<R>) * h.size(), cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    const int NZ_ = g.NZ + 2;
+    const size_t plane = (size_t)g.NX * g.NY * NZ_;
+    memset(z, 0, sizeof(double) * 2 * plane);
+    for (int c = 0; c < 2; ++c)
+      for (int ix = 0; ix < g.KXc; ++ix) {
+        const int i = ix < g.TX ? ix : g.NX + ix - g.KXc;
+        for (int iy = 0; iy < g.KYc; ++iy) {
+          const int j = iy < g.TY ? iy : g.NY + iy - g.KYc;
+          for (int k = 0; k < g.TZ; ++k) {
+            const Cx<R> v = h[c * nz + ((size_t)ix * g.KYc + iy) * g.TZ + k];
+            double *o = z + c * plane + ((size_t)i * g.NY + j) * NZ_ + 2 * k;
+            o[0] = (double)v.x;
+            o[1] = (double)v.y;
+          }
+        }
+      }
+    return 0;
+  }
+
+  int zeta_from_host(const double *z) override {
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    std::vector<Cx<R>> h(2 * nz);
+    const int NZ_ = g.NZ + 2;
+    const size_t plane = (size_t)g.NX * g.NY * NZ_;
+    for (int c = 0; c < 2; ++c)
+      for (int ix = 0; ix < g.KXc; ++ix) {
+        const int i = ix < g.TX ? ix : g.NX + ix - g.KXc;
+        for (int iy = 0; iy < g.KYc; ++iy) {
+          const int j = iy < g.TY ? iy : g.NY + iy - g.KYc;
+          for (int k = 0; k < g.TZ; ++k) {
+            const double *o = z + c * plane + ((size_t)i * g.NY + j) * NZ_ + 2 * k;
+            h[c * nz + ((size_t)ix * g.KYc + iy) * g.TZ + k] = {(R)o[0], (R)o[1]};
+          }
+        }
+      }
+    KCHECK(cudaMemcpyAsync(zeta, h.data(), sizeof(Cx<R>) * h.size(), cudaMemcpyHostToDevice, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    return 0;
+  }
+
+  int fft_fwd_host(double *a) override;
+  int fft_inv_host(double *a) override;
+  int solenoidal_host(double *u0, double *u1, double *u2) override;
+  int phi_up_host(double *phi, double *up0, double *up1, double *up2) override;
+  int fhydro_host(const double *u0, const double *u1, const double *u2, double *f, double *t) override;
+
+  void free_all() override {
+    cudaFree(zeta);
+    cudaFree(bufA);
+    cudaFree(bufB);
+    cudaFree(ustar);
+    cudaFree(phiup);
+    cudaFree(twbuf);
+  }
+};
+
+// Host copies of padded NX*NY*NZ_ real fields to packed R device arrays.
+template <typename R>
+std::vector<R> pack_real(const double *a, const Geo &g) {
+  const int NZ_ = g.NZ + 2;
+  std::vector<R> h((size_t)g.NX * g.NY * g.NZ);
+  for (size_t r = 0; r < (size_t)g.NX * g.NY; ++r)
+    for (int k = 0; k < g.NZ; ++k) h[r * g.NZ + k] = (R)a[r * NZ_ + k];
+  return h;
+}
+template <typename R>
+void unpack_real(double *a, const R *h, const Geo &g) {
+  const int NZ_ = g.NZ + 2;
+  for (size_t r = 0; r < (size_t)g.NX * g.NY; ++r)
+    for (int k = 0; k < g.NZ; ++k) a[r * NZ_ + k] = (double)h[r * g.NZ + k];
+}
+
+// The full-spectrum transforms are built from the same passes with a
+// geometry whose "retained" box is the whole half spectrum:
+// KXc = NX (ix == i), KYc = NY, TZ = NZ/2+1.  The x pass kernels of the step
+// are specialised to the SPM operators, so the routine-level transforms use
+// the y pass twice (x and y are both complex transforms over a row of a
+// transposed view) -- here done through a generic column pass below.
+template <typename R, bool INVERSE>
+__global__ void k_col_pass(Geo g, const Cx<R> *twn, int logn, int n, const Cx<R> *in,
+                                                  Cx<R> *out,
+                                                  long long line_stride, long long elem_stride, int nlines) {
+  // generic batched FFT over lines: element e of line l at l*line_stride + e*elem_stride
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<R> *tws = reinterpret_cast<Cx<R> *>(smem_raw);
+  Cx<R> *B = tws + n;  // [n][16]
+  load_twiddles(tws, twn, n);
+  const int l0 = blockIdx.x * 16;
+  for (int it = threadIdx.x; it < n * 16; it += blockDim.x) {
+    const int col = it % 16, e = it / 16;
+    Cx<R> v = {R(0), R(0)};
+    if (l0 + col < nlines) v = in[(long long)(l0 + col) * line_stride + (long long)e * elem_stride];
+    B[bitrev(e, logn) * 16 + col] = v;
+  }
+  __syncthreads();
+  fft_inplace(B, logn, 16, 1, 16, tws, INVERSE ? -1 : 1);
+  for (int it = threadIdx.x; it < n * 16; it += blockDim.x) {
+    const int col = it % 16, e = it / 16;
+    if (l0 + col < nlines) out[(long long)(l0 + col) * line_stride + (long long)e * elem_stride] = B[e * 16 + col];
+  }
+}
+
+// z c2r over all kz (routine-level A_k2a): in [NX*NY][M+1] complex
+template <typename R>
+__global__ void k_z_c2r_full(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
+                                                    R *__restrict__ out, double scale) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int M = g.M, P = M + 1;
+  Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
+  Cx<R> *twz = twm + M;
+  Cx<R> *S = twz + g.NZ;
+  load_twiddles(twm, tw.m, M);
+  load_twiddles(twz, tw.z, g.NZ);
+  __syncthreads();
+  const size_t row0 = (size_t)blockIdx.x * ZROWS;
+  for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
+    const int k = it % M, rr = it / M;
+    S[rr * P + bitrev(k, g.lm)] = c2r_pre(in + (row0 + rr) * (M + 1), k, M, M + 1, twz);
+  }
+  __syncthreads();
+  fft_inplace(S, g.lm, ZROWS, P, 1, twm, -1);
+  for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
+    const int n = it % M, rr = it / M;
+    const Cx<R> v = S[rr * P + n];
+    out[(row0 + rr) * g.NZ + 2 * n] = (R)(v.x * scale);
+    out[(row0 + rr) * g.NZ + 2 * n + 1] = (R)(v.y * scale);
+  }
+}
+
+template <typename R>
+struct FullFFT {
+  // forward: real [NX][NY][NZ] -> complex [NX][NY][M+1] (Ooura sign, unscaled)
+  static int forward(Box<R> &b, const R *in, Cx<R> *out) {
+    const Geo &g = b.g;
+    const int M1 = g.M + 1;
+    const size_t sm_c = sizeof(Cx<R>) * (g.M + g.NZ + (size_t)ZROWS * (g.M + 1));
+    k_z_r2c_full<R><<<b.gz(), 256, sm_c, b.stream>>>(g, b.tw, in, g.NZ, out);
+    // y: lines (x, kz): line stride... lines indexed l = x*M1 + kz -> base x*NY*M1 + kz
+    col_pass(b, out, g.NY, g.ly, b.tw.y, false, 1);
+    col_pass(b, out, g.NX, g.lx, b.tw.x, false, 0);
+    (void)M1;
+    KCHECK(cudaGetLastError());
+    return 0;
+  }
+  static int inverse(Box<R> &b, Cx<R> *in, R *out) {
+    const Geo &g = b.g;
+    col_pass(b, in, g.NX, g.lx, b.tw.x, true, 0);
+    col_pass(b, in, g.NY, g.ly, b.tw.y, true, 1);
+    const size_t sm_c = sizeof(Cx<R>) * (g.M + g.NZ + (size_t)ZROWS * (g.M + 1));
+    k_z_c2r_full<R><<<b.gz(), 256, sm_c, b.stream>>>(g, b.tw, in, out, g.inv_n);
+    KCHECK(cudaGetLastError());
+    return 0;
+  }
+  // axis 0: transform along x (lines = (y,kz), elem stride NY*M1)
+  // axis 1: transform along y (lines = (x,kz), elem stride M1)
+  static void col_pass(Box<R> &b, Cx<R> *data, int n, int logn, const Cx<R> *twn, bool inv, int axis) {
+    const Geo &g = b.g;
+    const int M1 = g.M + 1;
+    const size_t sm = sizeof(Cx<R>) * (n + (size_t)n * 16);
+    if (axis == 0) {
+      const int nlines = g.NY * M1;
+      // lines are contiguous (l = y*M1 + kz), element stride NY*M1
+      if (inv)
+        k_col_pass<R, true><<<(nlines + 15) / 16, 256, sm, b.stream>>>(g, twn, logn, n, data, data, 1,
+                                                                         (long long)g.NY * M1, nlines);
+      else
+        k_col_pass<R, false><<<(nlines + 15) / 16, 256, sm, b.stream>>>(g, twn, logn, n, data, data, 1,
+                                                                          (long long)g.NY * M1, nlines);
+    } else {
+      // per x: lines kz (contiguous), element stride M1; run NX launches' worth
+      // as one launch by treating (x, kz) lines with a 2-level index: use a
+      // launch per x (small sizes only on this routine-level path).
+      for (int x = 0; x < g.NX; ++x) {
+        Cx<R> *base = data + (size_t)x * g.NY * M1;
+        if (inv)
+          k_col_pass<R, true><<<(M1 + 15) / 16, 256, sm, b.stream>>>(g, twn, logn, n, base, base, 1, M1, M1);
+        else
+          k_col_pass<R, false><<<(M1 + 15) / 16, 256, sm, b.stream>>>(g, twn, logn, n, base, base, 1, M1, M1);
+      }
+    }
+  }
+};
+
+template <typename R>
+int Box<R>::fft_fwd_host(double *a) {
+  const size_t npt = npts();
+  const int M1 = g.M + 1;
+  std::vector<R> h = pack_real<R>(a, g);
+  R *din = nullptr;
+  Cx<R> *dout = nullptr;
+  KCHECK(cudaMalloc(&din, sizeof(R) * npt));
+  KCHECK(cudaMalloc(&dout, sizeof(Cx<R>) * (size_t)g.NX * g.NY * M1));
+  KCHECK(cudaMemcpy(din, h.data(), sizeof(R) * npt, cudaMemcpyHostToDevice));
+  int rc = FullFFT<R>::forward(*this, din, dout);
+  std::vector<Cx<R>> o((size_t)g.NX * g.NY * M1);
+  KCHECK(cudaMemcpyAsync(o.data(), dout, sizeof(Cx<R>) * o.size(), cudaMemcpyDeviceToHost, stream));
+  KCHECK(cudaStreamSynchronize(stream));
+  cudaFree(din);
+  cudaFree(dout);
+  if (rc) return rc;
+  const int NZ_ = g.NZ + 2;
+  for (size_t r = 0; r < (size_t)g.NX * g.NY; ++r)
+    for (int k = 0; k < M1; ++k) {
+      a[r * NZ_ + 2 * k] = (double)o[r * M1 + k].x;
+      a[r * NZ_ + 2 * k + 1] = (double)o[r * M1 + k].y;
+    }
+  return 0;
+}
+
+template <typename R>
+int Box<R>::fft_inv_host(double *a) {
+  const size_t npt = npts();
+  const int M1 = g.M + 1, NZ_ = g.NZ + 2;
+  std::vector<Cx<R>> h((size_t)g.NX * g.NY * M1);
+  for (size_t r = 0; r < (size_t)g.NX * g.NY; ++r)
+    for (int k = 0; k < M1; ++k) h[r * M1 + k] = {(R)a[r * NZ_ + 2 * k], (R)a[r * NZ_ + 2 * k + 1]};
+  Cx<R> *din = nullptr;
+  R *dout = nullptr;
+  KCHECK(cudaMalloc(&din, sizeof(Cx<R>) * h.size()));
+  KCHECK(cudaMalloc(&dout, sizeof(R) * npt));
+  KCHECK(cudaMemcpy(din, h.data(), sizeof(Cx<R>) * h.size(), cudaMemcpyHostToDevice));
+  int rc = FullFFT<R>::inverse(*this, din, dout);
+  std::vector<R> o(npt);
+  KCHECK(cudaMemcpyAsync(o.data(), dout, sizeof(R) * npt, cudaMemcpyDeviceToHost, stream));
+  KCHECK(cudaStreamSynchronize(stream));
+  cudaFree(din);
+  cudaFree(dout);
+  if (rc) return rc;
+  unpack_real<R>(a, o.data(), g);
+  return 0;
+}
+
+// Solenoidal_u: forward, 2/3 truncation, projection, inverse -- on the
+// compact spectra through the step's own passes: the forward z/y passes
+// (k_z_r2c via k_z_force with phi = 0 is not usable here), so this path uses
+// the full transforms and a k-space kernel.
+template <typename R>
+__global__ void k_solenoidal_full(Geo g, Cx<R> *u0, Cx<R> *u1, Cx<R> *u2) {
+  const int M1 = g.M + 1;
+  const size_t n = (size_t)g.NX * g.NY * M1;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    const int k = idx % M1;
+    const int j = (idx / M1) % g.NY;
+    const int i = idx / ((size_t)M1 * g.NY);
+    const int KXi = signed_k(i, g.NX), KYi = signed_k(j, g.NY);
+    if (!(abs(KXi) < g.TX && abs(KYi) < g.TY && k < g.TZ)) {
+      u0[idx] = {R(0), R(0)};
+      u1[idx] = {R(0), R(0)};
+      u2[idx] = {R(0), R(0)};
+      continue;
+    }
+    const R kx = R(g.wave[0] * KXi), ky = R(g.wave[1] * KYi), kz = R(g.wave[2] * k);
+    const R K2 = kx * kx + ky * ky + kz * kz;
+    const R IK2 = K2 > R(0) ? R(1) / K2 : R(0);
+    Cx<R> a = u0[idx], b = u1[idx], c = u2[idx];
+    const Cx<R> d = {IK2 * (a.x * kx + b.x * ky + c.x * kz), IK2 * (a.y * kx + b.y * ky + c.y * kz)};
+    u0[idx] = {a.x - d.x * kx, a.y - d.y * kx};
+    u1[idx] = {b.x - d.x * ky, b.y - d.y * ky};
+    u2[idx] = {c.x - d.x * kz, c.y - d.y * kz};
+  }
+}
+
+template <typename R>
+int Box<R>::solenoidal_host(double *u0, double *u1, double *u2) {
+  const size_t npt = npts();
+  const int M1 = g.M + 1;
+  double *hu[3] = {u0, u1, u2};
+  R *din = nullptr;
+  Cx<R> *dk = nullptr;
+  const size_t nk = (size_t)g.NX * g.NY * M1;
+  KCHECK(cudaMalloc(&din, sizeof(R) * 3 * npt));
+  KCHECK(cudaMalloc(&dk, sizeof(Cx<R>) * 3 * nk));
+  for (int c = 0; c < 3; ++c) {
+    std::vector<R> h = pack_real<R>(hu[c], g);
+    KCHECK(cudaMemcpy(din + c * npt, h.data(), sizeof(R) * npt, cudaMemcpyHostToDevice));
+    FullFFT<R>::forward(*this, din + c * npt, dk + c * nk);
+  }
+  k_solenoidal_full<R><<<592, 256, 0, stream>>>(g, dk, dk + nk, dk + 2 * nk);
+  for (int c = 0; c < 3; ++c) {
+    FullFFT<R>::inverse(*this, dk + c * nk, din + c * npt);
+    std::vector<R> o(npt);
+    KCHECK(cudaMemcpyAsync(o.data(), din + c * npt, sizeof(R) * npt, cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    unpack_real<R>(hu[c], o.data(), g);
+  }
+  cudaFree(din);
+  cudaFree(dk);
+  return 0;
+}
+
+template <typename R>
+int Box<R>::phi_up_host(double *phi, double *up0, double *up1, double *up2) {
+  const size_t npt = npts();
+  R *d = nullptr;
+  KCHECK(cudaMalloc(&d, sizeof(R) * 4 * npt));
+  KCHECK(cudaMemsetAsync(d, 0, sizeof(R) * 4 * npt, stream));
+  if (Np > 0) k_particles_scatter<R><<<Np, 256, 0, stream>>>(pp, parts, cells, d);
+  k_clamp_phi<R><<<592, 256, 0, stream>>>(npt, d);
+  KCHECK(cudaGetLastError());
+  std::vector<R> h(4 * npt);
+  KCHECK(cudaMemcpyAsync(h.data(), d, sizeof(R) * h.size(), cudaMemcpyDeviceToHost, stream));
+  KCHECK(cudaStreamSynchronize(stream));
+  cudaFree(d);
+  double *outs[4] = {phi, up0, up1, up2};
+  for (int c = 0; c < 4; ++c) unpack_real<R>(outs[c], h.data() + c * npt, g);
+  return 0;
+}
+
+template <typename R>
+__global__ void k_gather_only(PPar p, const DPart *__restrict__ parts, const R *__restrict__ u,
+                              const int *__restrict__ cells, double *__restrict__ out) {
+  __shared__ double sh[2 * 6 * 32];
+  const int n = blockIdx.x;
+  const DPart &a = parts[n];
+  const double xp[3] = {a.x[0], a.x[1], a.x[2]};
+  const StencilBase b = stencil_base(xp, p);
+  const size_t npts = (size_t)p.N[0] * p.N[1] * p.N[2];
+  KSum acc[6];
+  for (int i = 0; i < 6; ++i) acc[i] = {0.0, 0.0};
+  for (int m = threadIdx.x; m < p.S; m += blockDim.x) {
+    int rm[3];
+    double r[3], dist;
+    stencil_point(b, cells + 3 * m, xp, p, rm, r, dist);
+    const double ph = prof_phi(dist, p);
+    double vr[3] = {0.0, 0.0, 0.0};
+    if (p.rotation) {
+      vr[0] = a.omega[1] * r[2] - a.omega[2] * r[1];
+      vr[1] = a.omega[2] * r[0] - a.omega[0] * r[2];
+      vr[2] = a.omega[0] * r[1] - a.omega[1] * r[0];
+    }
+    const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
+    double fp[3];
+    for (int d = 0; d < 3; ++d) {
+      fp[d] = ((a.v[d] + vr[d]) - (double)u[d * npts + im]) * ph;
+      acc[d].add(fp[d]);
+    }
+    acc[3].add(r[1] * fp[2] - r[2] * fp[1]);
+    acc[4].add(r[2] * fp[0] - r[0] * fp[2]);
+    acc[5].add(r[0] * fp[1] - r[1] * fp[0]);
+  }
+  block_reduce<6>(acc, sh);
+  if (threadIdx.x == 0)
+    for (int d = 0; d < 3; ++d) {
+      out[6 * n + d] = p.fh_coef * (acc[d].s + acc[d].c);
+      out[6 * n + 3 + d] = p.rotation ? p.fh_coef * (acc[3 + d].s + acc[3 + d].c) : 0.0;
+    }
+}
+
+template <typename R>
+int Box<R>::fhydro_host(const double *u0, const double *u1, const double *u2, double *f, double *t) {
+  const size_t npt = npts();
+  R *d = nullptr;
+  double *o = nullptr;
+  KCHECK(cudaMalloc(&d, sizeof(R) * 3 * npt));
+  KCHECK(cudaMalloc(&o, sizeof(double) * 6 * (Np > 0 ? Np : 1)));
+  const double *hu[3] = {u0, u1, u2};
+  for (int c = 0; c < 3; ++c) {
+    std::vector<R> h = pack_real<R>(hu[c], g);
+    KCHECK(cudaMemcpy(d + c * npt, h.data(), sizeof(R) * npt, cudaMemcpyHostToDevice));
+  }
+  if (Np > 0) k_gather_only<R><<<Np, 256, 0, stream>>>(pp, parts, d, cells, o);
+  KCHECK(cudaGetLastError());
+  std::vector<double> h(6 * (size_t)Np);
+  KCHECK(cudaMemcpyAsync(h.data(), o, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream));
+  KCHECK(cudaStreamSynchronize(stream));
+  cudaFree(d);
+  cudaFree(o);
+  for (int n = 0; n < Np; ++n)
+    for (int c = 0; c < 3; ++c) {
+      f[3 * n + c] = h[6 * n + c];
+      t[3 * n + c] = h[6 * n + 3 + c];
+    }
+  return 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct kapsel_ctx {
+  std::unique_ptr<BoxBase> box;
+};
+
+extern "C" {
+
+void kapsel_params_default(kapsel_params *p) {
+  memset(p, 0, sizeof(*p));
+  p->np_xyz[0] = p->np_xyz[1] = p->np_xyz[2] = 6;
+  p->eq = KAPSEL_EQ_NAVIER_STOKES;
+  p->precision = KAPSEL_FP64;
+  p->dx = 1.0;
+  p->rho = 1.0;
+  p->eta = 1.0;
+  p->kbt = 0.0;
+  p->alpha_v = 1.0;
+  p->alpha_o = 1.0;
+  p->dt = 0.01;
+  p->a = 5.0;
+  p->a_xi = 2.0;
+  p->mass_ratio = 1.0;
+  p->gravity_dir = 2;
+  p->epsilon = 1.0;
+  p->lj_powers = 0;
+  p->lj_truncate = 1;
+  p->rotation = 1;
+  p->mt_seed = 0;
+}
+
+const char *kapsel_gpu_strerror(int s) {
+  switch (s) {
+    case KAPSEL_OK: return "ok";
+    case KAPSEL_EINVAL: return "invalid argument or unsupported configuration";
+    case KAPSEL_ECUDA: return "CUDA runtime error";
+    case KAPSEL_ENOMEM: return "device allocation failed";
+    case KAPSEL_ESTATE: return "call out of order";
+    case KAPSEL_ENONFINITE: return "non-finite particle state";
+    case KAPSEL_ERANGE: return "particle out of box or size limit exceeded";
+    default: return "unknown status";
+  }
+}
+
+int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
+  if (!p || !out) return KAPSEL_EINVAL;
+  *out = nullptr;
+  for (int d = 0; d < 3; ++d)
+    if (p->np_xyz[d] < 4 || p->np_xyz[d] > 9) return KAPSEL_EINVAL;  // 16..512 per axis
+  if (p->eq != KAPSEL_EQ_NAVIER_STOKES) return KAPSEL_EINVAL;
+  if (p->precision != KAPSEL_FP64 && p->precision != KAPSEL_MIXED) return KAPSEL_EINVAL;
+  if (p->n_particles < 0 || p->dx <= 0 || p->rho <= 0 || p->eta <= 0 || p->dt <= 0 || p->a <= 0 || p->a_xi <= 0)
+    return KAPSEL_EINVAL;
+  if (p->lj_powers < 0 || p->lj_powers > 2 || p->gravity_dir < 0 || p->gravity_dir > 2) return KAPSEL_EINVAL;
+  std::unique_ptr<BoxBase> b;
+  if (p->precision == KAPSEL_FP64)
+    b.reset(new (std::nothrow) Box<double>());
+  else
+    b.reset(new (std::nothrow) Box<float>());
+  if (!b) return KAPSEL_ENOMEM;
+  b->prm = *p;
+  Geo &g = b->g;
+  g.NX = 1 << p->np_xyz[0];
+  g.NY = 1 << p->np_xyz[1];
+  g.NZ = 1 << p->np_xyz[2];
+  g.M = g.NZ / 2;
+  g.lx = ilog2(g.NX);
+  g.ly = ilog2(g.NY);
+  g.lm = ilog2(g.M);
+  g.TX = (g.NX + 2) / 3;
+  g.TY = (g.NY + 2) / 3;
+  g.TZ = (g.NZ + 2) / 3;
+  g.KXc = 2 * g.TX - 1;
+  g.KYc = 2 * g.TY - 1;
+  const double L[3] = {g.NX * p->dx, g.NY * p->dx, g.NZ * p->dx};
+  for (int d = 0; d < 3; ++d) g.wave[d] = 2.0 * M_PI / L[d];
+  g.nu = p->eta / p->rho;
+  g.dt = p->dt;
+  for (int d = 0; d < 3; ++d) g.fix_cell[d] = p->fix_cell[d] ? 1 : 0;
+  g.fp64_exp = p->precision == KAPSEL_FP64 ? 1 : 0;
+  g.inv_n = 1.0 / ((double)g.NX * g.NY * g.NZ);
+
+  // particle constants: Set_global_parameters (input.cxx:274-431)
+  PPar &pp = b->pp;
+  std::vector<int> cells = sekibun(p->a, p->a_xi, p->dx);
+  b->Np = p->n_particles;
+  b->S = (int)cells.size() / 3;
+  pp.Np = b->Np;
+  pp.S = b->S;
+  pp.N[0] = g.NX;
+  pp.N[1] = g.NY;
+  pp.N[2] = g.NZ;
+  for (int d = 0; d < 3; ++d) pp.L[d] = L[d];
+  pp.DX = p->dx;
+  pp.RADIUS = p->a * p->dx;
+  const double XI = p->a_xi * p->dx;
+  pp.HXI = XI * 0.5;
+  pp.dt = p->dt;
+  const double rho_p = p->mass_ratio * p->rho;
+  const double mass = rho_p * 4. / 3. * M_PI * (pp.RADIUS * pp.RADIUS * pp.RADIUS);
+  const double moi = 2. / 5. * mass * (pp.RADIUS * pp.RADIUS);
+  pp.IMASS = 1. / mass;
+  pp.IMOI = 1. / moi;
+  const double DX3 = p->dx * p->dx * p->dx;
+  pp.fh_coef = (-DX3 * p->rho) / p->dt;
+  pp.rotation = p->rotation ? 1 : 0;
+  pp.lj_on = p->lj_truncate >= 0 ? 1 : 0;
+  pp.lj_powers = p->lj_powers;
+  const double sigma = 2.0 * pp.RADIUS;
+  double a_r_cutoff = 0.0;
+  if (p->lj_truncate > 0) {
+    const double pw[3] = {1. / 6., 1. / 12., 1. / 18.};
+    a_r_cutoff = std::pow(2., pw[p->lj_powers]);
+  } else if (p->lj_truncate == 0) {
+    const int nmin = std::min(g.NX, std::min(g.NY, g.NZ));
+    a_r_cutoff = std::min(nmin * p->dx * .5 / sigma, 2.5);
+  }
+  pp.lj_dia = sigma;
+  pp.lj_cut = a_r_cutoff * sigma;
+  pp.lj_coeff = 24. * (p->lj_powers + 1) * p->epsilon;
+  pp.lc[0] = g.NX / 16;
+  pp.lc[1] = g.NY / 16;
+  pp.lc[2] = g.NZ / 16;
+  pp.lc_r = 16 * p->dx;
+  const double gravity_on_fluid = p->gravity_g * p->rho * 4. / 3. * M_PI * (pp.RADIUS * pp.RADIUS) * pp.RADIUS;
+  pp.grav = p->gravity_g != 0.0 ? gravity_on_fluid * (p->mass_ratio - 1.0) : 0.0;
+  pp.gdir = p->gravity_dir;
+  pp.thermostat = (p->kbt > 0.0 && b->Np > 0) ? 1 : 0;
+  const double zeta_drag = 6. * M_PI * p->eta * pp.RADIUS;
+  const double zeta_drag_rot = 8. * M_PI * p->eta * (pp.RADIUS * pp.RADIUS * pp.RADIUS);
+  pp.noise_v = 1.439 * std::sqrt(zeta_drag * p->dt * p->kbt * p->alpha_v);
+  pp.noise_o = 1.22 * std::sqrt(zeta_drag_rot * p->dt * p->kbt * p->alpha_o);
+  b->mt.reset(new MT19937(p->mt_seed));
+
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return KAPSEL_ECUDA;
+  int rc = b->alloc();
+  if (rc) return rc;
+  const int np1 = b->Np > 0 ? b->Np : 1;
+  if (cudaMalloc(&b->parts, sizeof(DPart) * np1) != cudaSuccess) return KAPSEL_ENOMEM;
+  if (cudaMemset(b->parts, 0, sizeof(DPart) * np1) != cudaSuccess) return KAPSEL_ECUDA;
+  if (cudaMalloc(&b->cells, sizeof(int) * cells.size()) != cudaSuccess) return KAPSEL_ENOMEM;
+  if (cudaMemcpy(b->cells, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return KAPSEL_ECUDA;
+  if (cudaMalloc(&b->uk_dc, sizeof(double) * 3) != cudaSuccess) return KAPSEL_ENOMEM;
+  cudaMemset(b->uk_dc, 0, sizeof(double) * 3);
+  if (cudaMalloc(&b->status, sizeof(int)) != cudaSuccess) return KAPSEL_ENOMEM;
+  cudaMemset(b->status, 0, sizeof(int));
+  for (int s = 0; s < 2; ++s) {
+    if (cudaMalloc(&b->noise_dev[s], sizeof(double) * 6 * np1) != cudaSuccess) return KAPSEL_ENOMEM;
+    if (cudaMallocHost(&b->noise_host[s], sizeof(double) * 6 * np1) != cudaSuccess) return KAPSEL_ENOMEM;
+    if (cudaEventCreateWithFlags(&b->noise_ev[s], cudaEventDisableTiming) != cudaSuccess) return KAPSEL_ECUDA;
+    cudaMemset(b->noise_dev[s], 0, sizeof(double) * 6 * np1);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return KAPSEL_ECUDA;
+  kapsel_ctx *c = new (std::nothrow) kapsel_ctx;
+  if (!c) return KAPSEL_ENOMEM;
+  c->box = std::move(b);
+  *out = c;
+  return 0;
+}
+
+int kapsel_gpu_destroy(kapsel_ctx *ctx) {
+  if (!ctx) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (b) {
+    cudaStreamSynchronize(b->stream);
+    for (int s = 0; s < 2; ++s) {
+      if (b->graph[s]) cudaGraphExecDestroy(b->graph[s]);
+      cudaFree(b->noise_dev[s]);
+      cudaFreeHost(b->noise_host[s]);
+      if (b->noise_ev[s]) cudaEventDestroy(b->noise_ev[s]);
+    }
+    b->free_all();
+    cudaFree(b->parts);
+    cudaFree(b->cells);
+    cudaFree(b->uk_dc);
+    cudaFree(b->status);
+    cudaStreamDestroy(b->stream);
+  }
+  delete ctx;
+  return 0;
+}
+
+int kapsel_gpu_set_particles(kapsel_ctx *ctx, const double *x, const double *q) {
+  if (!ctx || (!x && ctx->box->Np > 0)) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  std::vector<DPart> h(b->Np > 0 ? b->Np : 1);
+  memset(h.data(), 0, sizeof(DPart) * h.size());
+  for (int n = 0; n < b->Np; ++n) {
+    for (int d = 0; d < 3; ++d) {
+      const double v = x[3 * n + d];
+      if (!(v >= 0.0 && v < b->pp.L[d])) return KAPSEL_ERANGE;
+      h[n].x[d] = v;
+      h[n].x_nopbc[d] = v;
+    }
+    double qq[4] = {1.0, 0.0, 0.0, 0.0};
+    if (q) {
+      // user_dir orientations are normalised (init_particle.cxx:281-286)
+      double nrm = 0.0;
+      for (int i = 0; i < 4; ++i) nrm += q[4 * n + i] * q[4 * n + i];
+      nrm = std::sqrt(nrm);
+      if (!(nrm > 0.0)) return KAPSEL_EINVAL;
+      nrm = 1.0 / nrm;
+      for (int i = 0; i < 4; ++i) qq[i] = q[4 * n + i] * nrm;
+    }
+    for (int i = 0; i < 4; ++i) h[n].q[i] = h[n].q_old[i] = qq[i];
+  }
+  if (cudaMemcpy(b->parts, h.data(), sizeof(DPart) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return KAPSEL_ECUDA;
+  b->particles_set = true;
+  return 0;
+}
+
+int kapsel_gpu_init_state(kapsel_ctx *ctx) {
+  if (!ctx) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (b->Np > 0 && !b->particles_set) return KAPSEL_ESTATE;
+  b->launch_init();
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
+  if (cudaGetLastError() != cudaSuccess) return KAPSEL_ECUDA;
+  b->ts = 0;
+  b->time = 0.0;
+  b->initialised = true;
+  return 0;
+}
+
+static int check_status(BoxBase *b) {
+  int st = 0;
+  if (cudaMemcpyAsync(&st, b->status, sizeof(int), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess)
+    return KAPSEL_ECUDA;
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
+  if (cudaGetLastError() != cudaSuccess) return KAPSEL_ECUDA;
+  return st;
+}
+
+static int step_impl(kapsel_ctx *ctx, int n, bool use_graph) {
+  if (!ctx || n < 0) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (!b->initialised) return KAPSEL_ESTATE;
+  for (int s = 0; s < n; ++s) {
+    const int slot = b->ts & 1;
+    int rc = b->fill_noise(slot);
+    if (rc) return rc;
+    const int euler = b->ts == 0 ? 1 : 0;
+    if (use_graph && !euler) {
+      if (!b->graph[slot]) {
+        cudaGraph_t gr;
+        if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return KAPSEL_ECUDA;
+        b->launch_step(b->noise_dev[slot], 0);
+        if (cudaStreamEndCapture(b->stream, &gr) != cudaSuccess) return KAPSEL_ECUDA;
+        if (cudaGraphInstantiate(&b->graph[slot], gr, 0) != cudaSuccess) return KAPSEL_ECUDA;
+        cudaGraphDestroy(gr);
+      }
+      if (cudaGraphLaunch(b->graph[slot], b->stream) != cudaSuccess) return KAPSEL_ECUDA;
+    } else {
+      b->launch_step(b->noise_dev[slot], euler);
+    }
+    b->ts += 1;
+    b->time += b->prm.dt;
+  }
+  return check_status(b);
+}
+
+int kapsel_gpu_step(kapsel_ctx *ctx, int n) { return step_impl(ctx, n, false); }
+int kapsel_gpu_step_graph(kapsel_ctx *ctx, int n) { return step_impl(ctx, n, true); }
+
+int kapsel_gpu_get_zeta(kapsel_ctx *ctx, double *zeta, double *uk_dc) {
+  if (!ctx || !zeta) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  int rc = b->zeta_to_host(zeta);
+  if (rc) return rc;
+  if (uk_dc) {
+    if (cudaMemcpy(uk_dc, b->uk_dc, sizeof(double) * 3, cudaMemcpyDeviceToHost) != cudaSuccess) return KAPSEL_ECUDA;
+  }
+  return 0;
+}
+
+int kapsel_gpu_set_zeta(kapsel_ctx *ctx, const double *zeta, const double *uk_dc) {
+  if (!ctx || !zeta || !uk_dc) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  int rc = b->zeta_from_host(zeta);
+  if (rc) return rc;
+  if (cudaMemcpy(b->uk_dc, uk_dc, sizeof(double) * 3, cudaMemcpyHostToDevice) != cudaSuccess) return KAPSEL_ECUDA;
+  b->initialised = true;
+  return 0;
+}
+
+int kapsel_gpu_get_velocity(kapsel_ctx *ctx, double *u) {
+  if (!ctx || !u) return KAPSEL_EINVAL;
+  return ctx->box->velocity_to_host(u);
+}
+
+int kapsel_gpu_get_particles(kapsel_ctx *ctx, double *out) {
+  if (!ctx || (!out && ctx->box->Np > 0)) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  std::vector<DPart> h(b->Np > 0 ? b->Np : 1);
+  if (cudaMemcpyAsync(h.data(), b->parts, sizeof(DPart) * h.size(), cudaMemcpyDeviceToHost, b->stream) !=
+      cudaSuccess)
+    return KAPSEL_ECUDA;
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
+  for (int n = 0; n < b->Np; ++n) {
+    double *o = out + (size_t)KAPSEL_P_STRIDE * n;
+    const DPart &a = h[n];
+    for (int d = 0; d < 3; ++d) {
+      o[KAPSEL_P_X + d] = a.x[d];
+      o[KAPSEL_P_V + d] = a.v[d];
+      o[KAPSEL_P_OMEGA + d] = a.omega[d];
+      o[KAPSEL_P_FHYDRO + d] = a.f_hydro_prev[d];
+      o[KAPSEL_P_THYDRO + d] = a.t_hydro_prev[d];
+      o[KAPSEL_P_FR + d] = a.fr_prev[d];
+      o[KAPSEL_P_XNOPBC + d] = a.x_nopbc[d];
+      o[KAPSEL_P_VOLD + d] = a.v_old[d];
+      o[KAPSEL_P_OMEGAOLD + d] = a.omega_old[d];
+    }
+    for (int i = 0; i < 4; ++i) {
+      o[KAPSEL_P_Q + i] = a.q[i];
+      o[KAPSEL_P_QOLD + i] = a.q_old[i];
+    }
+  }
+  return 0;
+}
+
+int kapsel_gpu_set_particle_state(kapsel_ctx *ctx, const double *in) {
+  if (!ctx || (!in && ctx->box->Np > 0)) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  std::vector<DPart> h(b->Np > 0 ? b->Np : 1);
+  memset(h.data(), 0, sizeof(DPart) * h.size());
+  for (int n = 0; n < b->Np; ++n) {
+    const double *o = in + (size_t)KAPSEL_P_STRIDE * n;
+    DPart &a = h[n];
+    for (int d = 0; d < 3; ++d) {
+      a.x[d] = o[KAPSEL_P_X + d];
+      if (!(a.x[d] >= 0.0 && a.x[d] < b->pp.L[d])) return KAPSEL_ERANGE;
+      a.v[d] = o[KAPSEL_P_V + d];
+      a.omega[d] = o[KAPSEL_P_OMEGA + d];
+      a.f_hydro_prev[d] = o[KAPSEL_P_FHYDRO + d];
+      a.t_hydro_prev[d] = o[KAPSEL_P_THYDRO + d];
+      a.fr_prev[d] = o[KAPSEL_P_FR + d];
+      a.x_nopbc[d] = o[KAPSEL_P_XNOPBC + d];
+      a.v_old[d] = o[KAPSEL_P_VOLD + d];
+      a.omega_old[d] = o[KAPSEL_P_OMEGAOLD + d];
+    }
+    for (int i = 0; i < 4; ++i) {
+      a.q[i] = o[KAPSEL_P_Q + i];
+      a.q_old[i] = o[KAPSEL_P_QOLD + i];
+    }
+  }
+  if (cudaMemcpy(b->parts, h.data(), sizeof(DPart) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return KAPSEL_ECUDA;
+  b->particles_set = true;
+  return 0;
+}
+
+int kapsel_gpu_get_time(kapsel_ctx *ctx, int *ts, double *time) {
+  if (!ctx) return KAPSEL_EINVAL;
+  if (ts) *ts = ctx->box->ts;
+  if (time) *time = ctx->box->time;
+  return 0;
+}
+
+int kapsel_gpu_get_dims(kapsel_ctx *ctx, int *dims) {
+  if (!ctx || !dims) return KAPSEL_EINVAL;
+  const BoxBase *b = ctx->box.get();
+  dims[0] = b->g.NX;
+  dims[1] = b->g.NY;
+  dims[2] = b->g.NZ;
+  dims[3] = b->g.NZ + 2;
+  dims[4] = b->Np;
+  dims[5] = b->S;
+  return 0;
+}
+
+int kapsel_gpu_set_efield(kapsel_ctx *ctx, const double *e) {
+  if (!ctx || !e) return KAPSEL_EINVAL;
+  for (int d = 0; d < 3; ++d) ctx->box->prm.e_ext[d] = e[d];
+  return ctx->box->prm.eq == KAPSEL_EQ_ELECTROLYTE ? 0 : KAPSEL_EINVAL;
+}
+
+int kapsel_gpu_A2a_k(kapsel_ctx *ctx, double *a) {
+  if (!ctx || !a) return KAPSEL_EINVAL;
+  return ctx->box->fft_fwd_host(a);
+}
+int kapsel_gpu_A_k2a(kapsel_ctx *ctx, double *a) {
+  if (!ctx || !a) return KAPSEL_EINVAL;
+  return ctx->box->fft_inv_host(a);
+}
+int kapsel_gpu_solenoidal_u(kapsel_ctx *ctx, double *u0, double *u1, double *u2) {
+  if (!ctx || !u0 || !u1 || !u2) return KAPSEL_EINVAL;
+  return ctx->box->solenoidal_host(u0, u1, u2);
+}
+int kapsel_gpu_make_phi_u(kapsel_ctx *ctx, double *phi, double *up0, double *up1, double *up2) {
+  if (!ctx || !phi || !up0 || !up1 || !up2) return KAPSEL_EINVAL;
+  return ctx->box->phi_up_host(phi, up0, up1, up2);
+}
+int kapsel_gpu_calc_f_hydro(kapsel_ctx *ctx, const double *u0, const double *u1, const double *u2, double *f,
+                            double *t) {
+  if (!ctx || !u0 || !u1 || !u2 || !f || !t) return KAPSEL_EINVAL;
+  return ctx->box->fhydro_host(u0, u1, u2, f, t);
+}
+
+int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr) {
+  // Runs the particle kernel on a copy of the particle state with zero hydro
+  // input is not separable; the LJ + gravity force is recovered from one
+  // velocity update on a scratch copy: fr = fr_prev after an Euler update.
+  if (!ctx || !fr) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (b->Np == 0) return 0;
+  DPart *scratch = nullptr;
+  if (cudaMalloc(&scratch, sizeof(DPart) * b->Np) != cudaSuccess) return KAPSEL_ENOMEM;
+  cudaMemcpyAsync(scratch, b->parts, sizeof(DPart) * b->Np, cudaMemcpyDeviceToDevice, b->stream);
+  PPar p = b->pp;
+  p.S = 0;           // no hydro gather
+  p.thermostat = 0;  // no kick
+  // u is never read with S == 0
+  if (b->prm.precision == KAPSEL_FP64)
+    k_particles_hydro_velocity<double><<<b->Np, 256, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
+                                                                     b->status);
+  else
+    k_particles_hydro_velocity<float><<<b->Np, 256, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
+                                                                    b->status);
+  std::vector<DPart> h(b->Np);
+  cudaMemcpyAsync(h.data(), scratch, sizeof(DPart) * b->Np, cudaMemcpyDeviceToHost, b->stream);
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
+  cudaFree(scratch);
+  for (int n = 0; n < b->Np; ++n)
+    for (int d = 0; d < 3; ++d) fr[3 * n + d] = h[n].fr_prev[d];
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,352 @@
+// Particle-side kernels of the SPM step.  Particle state is double precision
+// in every mode; only the fields they read or scatter into follow R.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace kapsel {
+
+// One particle (the subset of Particle, variable.h:27-75, the step uses).
+// *_prev hold the values reset_Forces (particle_solver.cxx:11-34) moves into
+// f_hydro_previous / torque_hydro_previous / fr_previous.
+struct DPart {
+  double x[3], x_nopbc[3], v[3], v_old[3], omega[3], omega_old[3];
+  double f_hydro_prev[3], t_hydro_prev[3], fr_prev[3];
+  double q[4], q_old[4];
+};
+
+struct PPar {
+  int Np, S;           // particles, Sekibun points per particle
+  int N[3];
+  double L[3];
+  double DX, RADIUS, HXI;
+  double dt;
+  double IMASS, IMOI;
+  double fh_coef;      // -DX^3 RHO / dt (md_force.cxx:264-265)
+  int rotation;
+  int lj_on;           // LJ_truncate >= 0
+  int lj_powers;
+  double lj_dia, lj_cut, lj_coeff;  // sigma, A_R_cutoff*sigma, 24(p+1) EPSILON
+  int lc[3];
+  double lc_r;         // Cell_length * DX (md_force.cxx:21,48-53)
+  double grav;         // Gravity_on_fluid * (MASS_RATIO - 1) (md_force.cxx:181-191)
+  int gdir;
+  int thermostat;
+  double noise_v, noise_o;  // fluct.cxx:13-19
+};
+
+__device__ __forceinline__ double nint_d(double a) {
+  // Nint (macro.h:38-46): round half away from zero
+  return a >= 0.0 ? (double)(int)(a + 0.5) : (double)(int)(a - 0.5);
+}
+
+// H and Phi (profile.h:29-49)
+__device__ __forceinline__ double prof_H(double x, double dx) { return x > 0.0 ? exp(-((dx / x) * (dx / x))) : 0.0; }
+__device__ __forceinline__ double prof_phi(double x, const PPar &p) {
+  const double h = prof_H(p.RADIUS + p.HXI - x, p.DX);
+  return h / (h + prof_H(x - p.RADIUS + p.HXI, p.DX));
+}
+
+// Stencil geometry shared by the gather and the scatter: Particle_cell
+// (make_phi.h:102-130), Relative_coord (:143-160), Distance (interaction.h:110-133).
+struct StencilBase {
+  int xi[3];
+  double res[3];
+};
+__device__ __forceinline__ StencilBase stencil_base(const double *x, const PPar &p) {
+  StencilBase b;
+  const double idx = 1.0 / p.DX;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double dmy = x[d] * idx;
+    // positions are kept in [0, L) by the integrator; a position outside
+    // (flagged through the status word) is folded back so that every grid
+    // index stays inside the field
+    if (!(dmy >= 0.0 && dmy < (double)p.N[d])) dmy = 0.0;
+    b.xi[d] = (int)dmy;
+    b.res[d] = (dmy - (double)b.xi[d]) * p.DX;
+  }
+  return b;
+}
+__device__ __forceinline__ void stencil_point(const StencilBase &b, const int *cell, const double *xp, const PPar &p,
+                                              int rm[3], double r[3], double &dist) {
+  double s = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    rm[d] = (b.xi[d] + cell[d] + p.N[d]) % p.N[d];
+    r[d] = (double)cell[d] * p.DX - b.res[d];
+    double dd = xp[d] - (double)rm[d] * p.DX;
+    dd -= nint_d(dd / p.L[d]) * p.L[d];
+    s += dd * dd;
+  }
+  dist = sqrt(s);
+}
+
+// Neumaier compensated accumulation.
+struct KSum {
+  double s, c;
+  __device__ __forceinline__ void add(double v) {
+    const double t = s + v;
+    c += fabs(s) >= fabs(v) ? (s - t) + v : (v - t) + s;
+    s = t;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// quaternion helpers (quaternion.h:173-245, rigid_body.cxx:10-63)
+__device__ __forceinline__ void qprod(const double *a, const double *b, double alpha, double *q) {
+  q[0] = alpha * (a[0] * b[0] - (a[1] * b[1] + a[2] * b[2] + a[3] * b[3]));
+  q[1] = alpha * (a[0] * b[1] + b[0] * a[1] + a[2] * b[3] - a[3] * b[2]);
+  q[2] = alpha * (a[0] * b[2] + b[0] * a[2] + a[3] * b[1] - a[1] * b[3]);
+  q[3] = alpha * (a[0] * b[3] + b[0] * a[3] + a[1] * b[2] - a[2] * b[1]);
+}
+__device__ __forceinline__ void space2body(const double *v, const double *q, double *out) {
+  const double qx[4] = {0.0, v[0], v[1], v[2]};
+  const double qc[4] = {q[0], -q[1], -q[2], -q[3]};
+  double t[4], r[4];
+  qprod(qx, q, 1.0, t);
+  qprod(qc, t, 1.0, r);
+  out[0] = r[1];
+  out[1] = r[2];
+  out[2] = r[3];
+}
+__device__ __forceinline__ void qnormalize(double *q) {
+  double n = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  n = 1.0 / n;
+  for (int i = 0; i < 4; ++i) q[i] *= n;
+}
+
+// MD_solver_position_Euler / _AB2 (particle_solver.cxx:36-88), PBC
+// (periodic_boundary.h:9-15), MD_solver_orientation_Euler / _AB2
+// (particle_rotation_solver.h:15-39).  One thread per particle.
+__global__ void k_particles_position(PPar p, DPart *__restrict__ parts, int euler, int *__restrict__ status) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= p.Np) return;
+  DPart &a = parts[n];
+  const double hdt = 0.5 * p.dt;
+  for (int d = 0; d < 3; ++d) {
+    const double dx = euler ? p.dt * a.v[d] : hdt * (3.0 * a.v[d] - a.v_old[d]);
+    a.x_nopbc[d] += dx;
+    a.x[d] += dx;
+    a.x[d] = fmod(a.x[d] + p.L[d], p.L[d]);
+    if (!(a.x[d] >= 0.0 && a.x[d] < p.L[d])) atomicExch(status, -6);
+  }
+  if (p.rotation) {
+    double dq[4];
+    if (euler) {
+      for (int i = 0; i < 4; ++i) a.q_old[i] = a.q[i];
+      const double qw[4] = {0.0, a.omega[0], a.omega[1], a.omega[2]};
+      qprod(qw, a.q, 0.5, dq);
+      for (int i = 0; i < 4; ++i) a.q[i] += dq[i] * p.dt;
+    } else {
+      double wb[3], wbo[3];
+      space2body(a.omega, a.q, wb);
+      space2body(a.omega_old, a.q_old, wbo);
+      for (int d = 0; d < 3; ++d) wb[d] = 3.0 * wb[d] - wbo[d];
+      for (int i = 0; i < 4; ++i) a.q_old[i] = a.q[i];
+      const double qw[4] = {0.0, wb[0], wb[1], wb[2]};
+      qprod(a.q, qw, 0.5, dq);
+      for (int i = 0; i < 4; ++i) a.q[i] += dq[i] * hdt;
+    }
+    qnormalize(a.q);
+  }
+}
+
+// Block reduction of NV compensated sums; result valid in thread 0.
+template <int NV>
+__device__ void block_reduce(KSum (&v)[NV], double *sh /* [NV][blockDim/32] x2 */) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double s = v[i].s, c = v[i].c;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double so = __shfl_down_sync(0xffffffffu, s, o);
+      const double co = __shfl_down_sync(0xffffffffu, c, o);
+      KSum k{s, c + co};
+      k.add(so);
+      s = k.s;
+      c = k.c;
+    }
+    if (lane == 0) {
+      sh[(2 * i) * 32 + wid] = s;
+      sh[(2 * i + 1) * 32 + wid] = c;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      KSum k{0.0, 0.0};
+      double cs = 0.0;
+      for (int w = 0; w < nw; ++w) {
+        k.add(sh[(2 * i) * 32 + w]);
+        cs += sh[(2 * i + 1) * 32 + w];
+      }
+      v[i].s = k.s;
+      v[i].c = k.c + cs;
+    }
+  }
+}
+
+// Calc_f_hydro_correct_precision (md_force.cxx:263-389), the LJ and gravity
+// forces of Force (particle_solver.h:97-109; md_force.cxx:23-134,181-191),
+// MD_solver_velocity_Euler / _AB2_hydro with reset_Forces
+// (particle_solver.cxx:106-147, 247-289, 11-34) and, when kBT > 0, the
+// thermostat kick of Add_random_force_thermostat (fluct.cxx:10-36) from a
+// precomputed table of its normals.  One block per particle.
+template <typename R>
+__global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart *__restrict__ parts,
+                                                                  const R *__restrict__ u, const int *__restrict__ cells,
+                                                                  const double *__restrict__ noise, int euler,
+                                                                  int *__restrict__ status) {
+  __shared__ double sh[2 * 9 * 32];
+  const int n = blockIdx.x;
+  DPart &a = parts[n];
+  const double xp[3] = {a.x[0], a.x[1], a.x[2]};
+  const double vp[3] = {a.v[0], a.v[1], a.v[2]};
+  const double wp[3] = {a.omega[0], a.omega[1], a.omega[2]};
+  const StencilBase b = stencil_base(xp, p);
+  const size_t npts = (size_t)p.N[0] * p.N[1] * p.N[2];
+  KSum acc[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) acc[i] = {0.0, 0.0};
+  for (int m = threadIdx.x; m < p.S; m += blockDim.x) {
+    int rm[3];
+    double r[3], dist;
+    stencil_point(b, cells + 3 * m, xp, p, rm, r, dist);
+    const double ph = prof_phi(dist, p);
+    double vr[3] = {0.0, 0.0, 0.0};
+    if (p.rotation) {
+      vr[0] = wp[1] * r[2] - wp[2] * r[1];
+      vr[1] = wp[2] * r[0] - wp[0] * r[2];
+      vr[2] = wp[0] * r[1] - wp[1] * r[0];
+    }
+    const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
+    double fp[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      fp[d] = ((vp[d] + vr[d]) - (double)u[d * npts + im]) * ph;
+      acc[d].add(fp[d]);
+    }
+    acc[3].add(r[1] * fp[2] - r[2] * fp[1]);
+    acc[4].add(r[2] * fp[0] - r[0] * fp[2]);
+    acc[5].add(r[0] * fp[1] - r[1] * fp[0]);
+  }
+  if (p.lj_on) {
+    int mc[3];
+    for (int d = 0; d < 3; ++d) mc[d] = (int)(xp[d] / p.lc_r);
+    for (int j = threadIdx.x; j < p.Np; j += blockDim.x) {
+      if (j == n) continue;
+      const DPart &o = parts[j];
+      int mult = 1;
+      double x12[3], r2 = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        // times the cell-list scan (md_force.cxx:72-121) meets this pair
+        const int cj = (int)(o.x[d] / p.lc_r);
+        int cnt = 0;
+        for (int off = -1; off <= 1; ++off) {
+          int c = mc[d] + off;
+          if (c < 0) c = p.lc[d] - 1;
+          if (c > p.lc[d] - 1) c = 0;
+          cnt += (c == cj);
+        }
+        mult *= cnt;
+        x12[d] = o.x[d] - xp[d];
+        x12[d] -= nint_d(x12[d] / p.L[d]) * p.L[d];
+        r2 += x12[d] * x12[d];
+      }
+      const double rij = sqrt(r2);
+      if (mult > 0 && rij < p.lj_cut) {
+        // Lennard_Jones_f (interaction.h:156-181)
+        const double s = p.lj_dia / rij;
+        double dmy = (s * s) * (s * s) * (s * s);
+        if (p.lj_powers >= 1) dmy = dmy * dmy;
+        if (p.lj_powers >= 2) dmy = dmy * (s * s) * (s * s) * (s * s);
+        const double f = p.lj_coeff / (rij * rij) * (2.0 * dmy * dmy - dmy);
+        for (int d = 0; d < 3; ++d) acc[6 + d].add((double)mult * (f * -x12[d]));
+      }
+    }
+  }
+  block_reduce<9>(acc, sh);
+  if (threadIdx.x != 0) return;
+  double fh[3], th[3], fr[3];
+  for (int d = 0; d < 3; ++d) {
+    fh[d] = p.fh_coef * (acc[d].s + acc[d].c);
+    th[d] = p.rotation ? p.fh_coef * (acc[3 + d].s + acc[3 + d].c) : 0.0;
+    fr[d] = acc[6 + d].s + acc[6 + d].c;
+  }
+  fr[p.gdir] -= p.grav;
+  const double hdt = 0.5 * p.dt;
+  for (int d = 0; d < 3; ++d) {
+    a.v_old[d] = a.v[d];
+    a.omega_old[d] = a.omega[d];
+    if (euler) {
+      const double dmy = p.dt * p.IMASS, dmy_rot = p.dt * p.IMOI;
+      a.v[d] += dmy * (fh[d] + fr[d]);
+      a.omega[d] += dmy_rot * th[d];
+    } else {
+      const double dmy = hdt * p.IMASS, dmy_rot = hdt * p.IMOI;
+      a.v[d] += dmy * (2.0 * fh[d] + fr[d] + a.fr_prev[d]);
+      a.omega[d] += dmy_rot * 2.0 * th[d];
+    }
+    a.fr_prev[d] = fr[d];
+    a.f_hydro_prev[d] = fh[d];
+    a.t_hydro_prev[d] = th[d];
+  }
+  if (p.thermostat) {
+    const double *g = noise + 6 * (size_t)n;
+    for (int d = 0; d < 3; ++d) {
+      a.v[d] += g[d] * p.noise_v * p.IMASS;
+      if (p.rotation) a.omega[d] += g[3 + d] * p.noise_o * p.IMOI;
+    }
+  }
+  for (int d = 0; d < 3; ++d)
+    if (!isfinite(a.v[d]) || !isfinite(a.omega[d])) atomicExch(status, -5);
+}
+
+// Make_phi_u_primitive scatter (make_phi.cxx:221-277): phi += phi_i and
+// up += (v + omega x r) phi_i over the Sekibun points of each particle.
+// The phi > 1 clamp is applied by the consumer.  One block per particle.
+template <typename R>
+__global__ void __launch_bounds__(256) k_particles_scatter(PPar p, const DPart *__restrict__ parts,
+                                                           const int *__restrict__ cells, R *__restrict__ phiup) {
+  const int n = blockIdx.x;
+  const DPart &a = parts[n];
+  const double xp[3] = {a.x[0], a.x[1], a.x[2]};
+  const double vp[3] = {a.v[0], a.v[1], a.v[2]};
+  const double wp[3] = {a.omega[0], a.omega[1], a.omega[2]};
+  const StencilBase b = stencil_base(xp, p);
+  const size_t npts = (size_t)p.N[0] * p.N[1] * p.N[2];
+  for (int m = threadIdx.x; m < p.S; m += blockDim.x) {
+    int rm[3];
+    double r[3], dist;
+    stencil_point(b, cells + 3 * m, xp, p, rm, r, dist);
+    const double ph = prof_phi(dist, p);
+    double vr[3] = {0.0, 0.0, 0.0};
+    if (p.rotation) {
+      vr[0] = wp[1] * r[2] - wp[2] * r[1];
+      vr[1] = wp[2] * r[0] - wp[0] * r[2];
+      vr[2] = wp[0] * r[1] - wp[1] * r[0];
+    }
+    const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
+    atomicAdd(phiup + im, (R)ph);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) atomicAdd(phiup + (1 + d) * npts + im, (R)((vp[d] + vr[d]) * ph));
+  }
+}
+
+// The phi > 1 clamp of Make_phi_u_primitive (make_phi.cxx:278-297) as a
+// separate pass, for the routine-level entry point.
+template <typename R>
+__global__ void k_clamp_phi(size_t npts, R *__restrict__ phiup) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < npts; i += (size_t)gridDim.x * blockDim.x) {
+    const R ph = phiup[i];
+    if (ph > R(1)) {
+      const R inv = R(1) / ph;
+      for (int d = 1; d <= 3; ++d) phiup[d * npts + i] *= inv;
+      phiup[i] = R(1);
+    }
+  }
+}
+
+}  // namespace kapsel

@@ -1,0 +1,558 @@
+// Pruned 3D real FFT passes with the SPM k-space and real-space operators
+// fused into them.
+//
+// Storage (per field component, complex values in the reference's Ooura sign):
+//   zeta   [2][KXc][KYc][TZ]   reduced vorticity, 2/3-rule modes only
+//   I1     [c][NX][KYc][TZ]    after the x transform (x in real space)
+//   I2     [c][NX][NY][TZ]     after the y transform (x, y in real space)
+//   real   [c][NX][NY][NZ]     real-space fields
+// KXc = 2*TX-1 holds kx = 0..TX-1, -(TX-1)..-1 (compact index ix, kx = ix
+// for ix < TX, else ix - KXc); likewise KYc.  Only kz < TZ is stored.  The
+// 2/3 rule of Truncate_two_third_rule_ooura (fft_wrapper.h:723-766) keeps
+// exactly these modes, so every inverse transform starts from zero outside
+// them and every forward transform whose result is truncated need not
+// compute the rest.
+#pragma once
+
+#include "fft_device.cuh"
+
+namespace kapsel {
+
+struct Geo {
+  int NX, NY, NZ, M;      // M = NZ/2
+  int lx, ly, lm;         // log2 of NX, NY, M
+  int TX, TY, TZ;         // TRN = (N+2)/3 (input.cxx:297)
+  int KXc, KYc;           // 2*TRN-1
+  double wave[3];         // 2 pi / L
+  double nu, dt;
+  int fix_cell[3];
+  int fp64_exp;           // 1: exp(x)-1 as the reference, 0: expm1
+  double inv_n;           // 1/(NX*NY*NZ): the A_k2a scale (fft_wrapper.h:552)
+};
+
+template <typename R>
+struct Twiddles {
+  const Cx<R> *x, *y, *m, *z;  // exp(+2 pi i j/n) for n = NX, NY, NZ/2, NZ
+};
+
+__device__ __forceinline__ int full_from_compact(int c, int T, int Kc, int N) { return c < T ? c : N + c - Kc; }
+__device__ __forceinline__ int signed_k(int i, int N) { return i > N / 2 ? i - N : i; }
+
+// Zeta_k2u_k (fft_wrapper.cxx:408-511) for one mode: the third vorticity
+// component from k.omega = 0 under the 3-case map, u = -i k x omega / k^2.
+template <typename R>
+__device__ __forceinline__ void zeta_to_u(int KXi, int KYi, R kx, R ky, R kz, R ik2, Cx<R> z0, Cx<R> z1,
+                                          Cx<R> u[3]) {
+  Cx<R> w0, w1, w2;
+  if (KXi != 0) {
+    const R inv = R(1) / kx;
+    w0 = {-inv * (ky * z0.x + kz * z1.x), -inv * (ky * z0.y + kz * z1.y)};
+    w1 = z0;
+    w2 = z1;
+  } else if (KYi != 0) {
+    const R d = -(kz / ky);
+    w0 = z1;
+    w1 = {d * z0.x, d * z0.y};
+    w2 = z0;
+  } else {
+    w0 = z0;
+    w1 = z1;
+    w2 = {R(0), R(0)};
+  }
+  const R ax = kx * ik2, ay = ky * ik2, az = kz * ik2;
+  // u = -i (k/k^2) x omega
+  Cx<R> c0 = {ay * w2.x - az * w1.x, ay * w2.y - az * w1.y};
+  Cx<R> c1 = {az * w0.x - ax * w2.x, az * w0.y - ax * w2.y};
+  Cx<R> c2 = {ax * w1.x - ay * w0.x, ax * w1.y - ay * w0.y};
+  u[0] = cmul_mi(c0);
+  u[1] = cmul_mi(c1);
+  u[2] = cmul_mi(c2);
+}
+
+// Component map of Omega_k2zeta_k (fft_wrapper.cxx:137-173) / U_k2zeta_k
+// (:258-339): kx != 0 -> (w1, w2); ky != 0 -> (w2, w0); else (w0, w1).
+template <typename R>
+__device__ __forceinline__ void select_zeta(int KXi, int KYi, const Cx<R> w[3], Cx<R> &z0, Cx<R> &z1) {
+  if (KXi != 0) {
+    z0 = w[1];
+    z1 = w[2];
+  } else if (KYi != 0) {
+    z0 = w[2];
+    z1 = w[0];
+  } else {
+    z0 = w[0];
+    z1 = w[1];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// x pass, inverse: zeta -> u_k (Zeta_k2u_k) -> inverse x transform.
+// grid (KYc, ceil(TZ/KC)), out I1[3][NX][KYc][TZ].
+template <typename R>
+__global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ zeta,
+                                                     const double *__restrict__ uk_dc, Cx<R> *__restrict__ out,
+                                                     int KC) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
+  Cx<R> *U = twx + g.NX;  // [NX rows][3*KC]
+  const int iy = blockIdx.x;
+  const int kz0 = blockIdx.y * KC;
+  const int ncol = min(KC, g.TZ - kz0);
+  const int W = 3 * KC;
+  load_twiddles(twx, tw.x, g.NX);
+  const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
+  const R ky = R(g.wave[1] * KYi);
+  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
+  for (int it = threadIdx.x; it < g.NX * KC; it += blockDim.x) {
+    const int col = it % KC, i = it / KC;
+    const int row = bitrev(i, g.lx);
+    Cx<R> u[3] = {{R(0), R(0)}, {R(0), R(0)}, {R(0), R(0)}};
+    const int KXi = signed_k(i, g.NX);
+    if (col < ncol && abs(KXi) < g.TX) {
+      const int ix = KXi >= 0 ? KXi : KXi + g.KXc;
+      const int kz = kz0 + col;
+      const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
+      const Cx<R> z0 = zeta[o], z1 = zeta[zplane + o];
+      const R kx = R(g.wave[0] * KXi), kzr = R(g.wave[2] * kz);
+      const R k2 = kx * kx + ky * ky + kzr * kzr;
+      const R ik2 = k2 > R(0) ? R(1) / k2 : R(0);
+      zeta_to_u(KXi, KYi, kx, ky, kzr, ik2, z0, z1, u);
+      if (KXi == 0 && KYi == 0 && kz == 0) {
+        u[0] = {R(uk_dc[0]), R(0)};
+        u[1] = {R(uk_dc[1]), R(0)};
+        u[2] = {R(uk_dc[2]), R(0)};
+      }
+    }
+    U[row * W + col] = u[0];
+    U[row * W + KC + col] = u[1];
+    U[row * W + 2 * KC + col] = u[2];
+  }
+  __syncthreads();
+  fft_inplace(U, g.lx, W, 1, W, twx, -1);
+  for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, x = rest % g.NX, c = rest / g.NX;
+    if (col < ncol)
+      out[(((size_t)c * g.NX + x) * g.KYc + iy) * g.TZ + kz0 + col] = U[x * W + c * KC + col];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// y pass.  inverse: in [c][NX][KYc][TZ] -> out [c][NX][NY][TZ]
+//          forward: in [c][NX][NY][TZ] -> out [c][NX][KYc][TZ] (|ky| < TY kept)
+// grid (NX, ncomp, ceil(TZ/KC)).
+template <typename R, bool INVERSE>
+__global__ void __launch_bounds__(256) k_y_pass(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
+                                                Cx<R> *__restrict__ out, int KC) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<R> *twy = reinterpret_cast<Cx<R> *>(smem_raw);
+  Cx<R> *Y = twy + g.NY;  // [NY rows][KC]
+  const int x = blockIdx.x, c = blockIdx.y;
+  const int kz0 = blockIdx.z * KC;
+  const int ncol = min(KC, g.TZ - kz0);
+  load_twiddles(twy, tw.y, g.NY);
+  const int rows_in = INVERSE ? g.KYc : g.NY;
+  const int rows_out = INVERSE ? g.NY : g.KYc;
+  const Cx<R> *src = in + ((size_t)c * g.NX + x) * rows_in * g.TZ + kz0;
+  Cx<R> *dst = out + ((size_t)c * g.NX + x) * rows_out * g.TZ + kz0;
+  for (int it = threadIdx.x; it < g.NY * KC; it += blockDim.x) {
+    const int col = it % KC, j = it / KC;
+    Cx<R> v = {R(0), R(0)};
+    if (col < ncol) {
+      if (INVERSE) {
+        const int KYi = signed_k(j, g.NY);
+        if (abs(KYi) < g.TY) {
+          const int iy = KYi >= 0 ? KYi : KYi + g.KYc;
+          v = src[(size_t)iy * g.TZ + col];
+        }
+      } else {
+        v = src[(size_t)j * g.TZ + col];
+      }
+    }
+    Y[bitrev(j, g.ly) * KC + col] = v;
+  }
+  __syncthreads();
+  fft_inplace(Y, g.ly, KC, 1, KC, twy, INVERSE ? -1 : 1);
+  for (int it = threadIdx.x; it < rows_out * KC; it += blockDim.x) {
+    const int col = it % KC, r = it / KC;
+    if (col >= ncol) continue;
+    const int j = INVERSE ? r : full_from_compact(r, g.TY, g.KYc, g.NY);
+    dst[(size_t)r * g.TZ + col] = Y[j * KC + col];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z pass helpers.  A row holds A[k], k < TZ, of a real line of NZ points.
+// c2r: Z[k] = (A[k] + conj A[M-k]) + i (A[k] - conj A[M-k]) w^{-k}, k < M,
+//      z = IFFT_M(Z), a[2n] = Re z[n], a[2n+1] = Im z[n].
+// r2c: z[n] = a[2n] + i a[2n+1], Z = FFT_M(z),
+//      A[k] = (Z[k] + conj Z[M-k])/2 - i/2 (Z[k] - conj Z[M-k]) w^{k}.
+template <typename R>
+__device__ __forceinline__ Cx<R> c2r_pre(const Cx<R> *row, int k, int M, int TZ, const Cx<R> *twz) {
+  const Cx<R> zero = {R(0), R(0)};
+  const Cx<R> a = k < TZ ? row[k] : zero;
+  const Cx<R> b = (M - k) < TZ ? cconj(row[M - k]) : zero;
+  const Cx<R> w = twid(twz, k, -1);
+  return cadd(cadd(a, b), cmul_pi(cmul(csub(a, b), w)));
+}
+
+template <typename R>
+__device__ __forceinline__ Cx<R> r2c_post(const Cx<R> *seq, int k, int M, const Cx<R> *twz) {
+  // seq is in natural order after the FFT; Z[M] is Z[0]
+  const Cx<R> zk = seq[k & (M - 1)];
+  const Cx<R> zm = cconj(seq[(M - k) & (M - 1)]);
+  const Cx<R> e = cadd(zk, zm), d = csub(zk, zm);
+  const Cx<R> w = twid(twz, k, 1);
+  const Cx<R> t = cmul_mi(cmul(d, w));
+  return cscale(cadd(e, t), R(0.5));
+}
+
+// Rows per block of the z kernels and the padded sequence pitch.
+constexpr int ZROWS = 4;
+
+// z pass fused at the centre of the nonlinear term (operate_omega.cxx:14-58):
+// inverse z transform of the three velocity components of each row, the
+// five real-space products u2u3, u3u1, u1u2, (u2-u3)(u2+u3), (u3-u1)(u3+u1),
+// and their forward z transforms (kz < TZ kept).  In place on I2: reads
+// components 0..2, writes 0..4.  grid (NX*NY/ZROWS).
+template <typename R>
+__global__ void __launch_bounds__(256) k_z_products(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ io) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int M = g.M, P = M + 1;
+  Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
+  Cx<R> *twz = twm + M;
+  Cx<R> *V = twz + g.NZ;      // [ZROWS*3][P] velocity lines, seq = rr*3 + c
+  Cx<R> *Q = V + ZROWS * 3 * P;  // [ZROWS*5][P] product lines, seq = rr*5 + c
+  load_twiddles(twm, tw.m, M);
+  load_twiddles(twz, tw.z, g.NZ);
+  __syncthreads();
+  const size_t rows = (size_t)g.NX * g.NY;
+  const size_t row0 = (size_t)blockIdx.x * ZROWS;
+  const size_t cstr = rows * g.TZ;
+  for (int it = threadIdx.x; it < ZROWS * 3 * M; it += blockDim.x) {
+    const int k = it % M, rest = it / M, c = rest % 3, rr = rest / 3;
+    const Cx<R> *row = io + c * cstr + (row0 + rr) * g.TZ;
+    V[(rr * 3 + c) * P + bitrev(k, g.lm)] = c2r_pre(row, k, M, g.TZ, twz);
+  }
+  __syncthreads();
+  fft_inplace(V, g.lm, ZROWS * 3, P, 1, twm, -1);
+  const R sc = R(g.inv_n);
+  for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
+    const int n = it % M, rr = it / M;
+    const Cx<R> U1 = V[(rr * 3) * P + n], U2 = V[(rr * 3 + 1) * P + n], U3 = V[(rr * 3 + 2) * P + n];
+    const R u1a = U1.x * sc, u1b = U1.y * sc, u2a = U2.x * sc, u2b = U2.y * sc, u3a = U3.x * sc,
+            u3b = U3.y * sc;
+    const int dst = bitrev(n, g.lm);
+    Cx<R> *q = Q + rr * 5 * P + dst;
+    q[0] = {u2a * u3a, u2b * u3b};
+    q[P] = {u3a * u1a, u3b * u1b};
+    q[2 * P] = {u1a * u2a, u1b * u2b};
+    q[3 * P] = {(u2a - u3a) * (u2a + u3a), (u2b - u3b) * (u2b + u3b)};
+    q[4 * P] = {(u3a - u1a) * (u3a + u1a), (u3b - u1b) * (u3b + u1b)};
+  }
+  __syncthreads();
+  fft_inplace(Q, g.lm, ZROWS * 5, P, 1, twm, 1);
+  for (int it = threadIdx.x; it < ZROWS * 5 * g.TZ; it += blockDim.x) {
+    const int k = it % g.TZ, rest = it / g.TZ, c = rest % 5, rr = rest / 5;
+    io[c * cstr + (row0 + rr) * g.TZ + k] = r2c_post(Q + (rr * 5 + c) * P, k, M, twz);
+  }
+}
+
+// z pass, inverse to real space: in I2 [c][NX][NY][TZ], out real [c][NX][NY][NZ]
+// scaled by 1/(NX NY NZ).  grid (NX*NY/ZROWS, ncomp).
+template <typename R>
+__global__ void __launch_bounds__(256) k_z_c2r(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
+                                               R *__restrict__ out, size_t out_cstride, int out_pitch) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int M = g.M, P = M + 1;
+  Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
+  Cx<R> *twz = twm + M;
+  Cx<R> *S = twz + g.NZ;  // [ZROWS][P]
+  load_twiddles(twm, tw.m, M);
+  load_twiddles(twz, tw.z, g.NZ);
+  __syncthreads();
+  const int c = blockIdx.y;
+  const size_t rows = (size_t)g.NX * g.NY;
+  const size_t row0 = (size_t)blockIdx.x * ZROWS;
+  const Cx<R> *src = in + c * rows * g.TZ;
+  for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
+    const int k = it % M, rr = it / M;
+    S[rr * P + bitrev(k, g.lm)] = c2r_pre(src + (row0 + rr) * g.TZ, k, M, g.TZ, twz);
+  }
+  __syncthreads();
+  fft_inplace(S, g.lm, ZROWS, P, 1, twm, -1);
+  const R sc = R(g.inv_n);
+  R *dst = out + c * out_cstride;
+  for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
+    const int n = it % M, rr = it / M;
+    const Cx<R> v = S[rr * P + n];
+    R *o = dst + (row0 + rr) * (size_t)out_pitch + 2 * n;
+    o[0] = v.x * sc;
+    o[1] = v.y * sc;
+  }
+}
+
+// z pass of the rigidity force (Make_f_particle_dt_nonsole, f_particle.h:41-64,
+// with the phi > 1 clamp of make_phi.cxx:278-297 applied on the fly):
+// f = up' - phi' u*, forward z transform, kz < TZ kept -> out [3][NX][NY][TZ].
+// The scattered phi/up fields are cleared where they were written, so they are
+// all-zero again for the next scatter.  grid (NX*NY/ZROWS).
+template <typename R>
+__global__ void __launch_bounds__(256) k_z_force(Geo g, Twiddles<R> tw, R *__restrict__ phiup,
+                                                 const R *__restrict__ ustar, Cx<R> *__restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int M = g.M, P = M + 1;
+  Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
+  Cx<R> *twz = twm + M;
+  Cx<R> *S = twz + g.NZ;  // [ZROWS*3][P]
+  load_twiddles(twm, tw.m, M);
+  load_twiddles(twz, tw.z, g.NZ);
+  const size_t npts = (size_t)g.NX * g.NY * g.NZ;
+  const size_t row0 = (size_t)blockIdx.x * ZROWS;
+  for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
+    const int n = it % M, rr = it / M;
+    const size_t o = (row0 + rr) * g.NZ + 2 * n;
+    R ph[2], up[3][2], us[3][2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      ph[e] = phiup[o + e];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        up[d][e] = phiup[(1 + d) * npts + o + e];
+        us[d][e] = ustar[d * npts + o + e];
+      }
+    }
+    R f[3][2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      R p = ph[e];
+      if (p > R(1)) {
+        const R inv = R(1) / p;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) up[d][e] *= inv;
+        p = R(1);
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) f[d][e] = up[d][e] - p * us[d][e];
+      if (ph[e] != R(0)) {
+        phiup[o + e] = R(0);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) phiup[(1 + d) * npts + o + e] = R(0);
+      }
+    }
+    const int dst = bitrev(n, g.lm);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) S[(rr * 3 + d) * P + dst] = {f[d][0], f[d][1]};
+  }
+  __syncthreads();
+  fft_inplace(S, g.lm, ZROWS * 3, P, 1, twm, 1);
+  const size_t rows = (size_t)g.NX * g.NY;
+  for (int it = threadIdx.x; it < ZROWS * 3 * g.TZ; it += blockDim.x) {
+    const int k = it % g.TZ, rest = it / g.TZ, d = rest % 3, rr = rest / 3;
+    out[d * rows * g.TZ + (row0 + rr) * g.TZ + k] = r2c_post(S + (rr * 3 + d) * P, k, M, twz);
+  }
+}
+
+// z pass, forward of a real field with padded pitch (routine-level A2a_k):
+// in real [c][NX][NY][pitch] -> out [c][NX][NY][NZ/2+1] (all kz).
+template <typename R>
+__global__ void __launch_bounds__(256) k_z_r2c_full(Geo g, Twiddles<R> tw, const R *__restrict__ in,
+                                                    int in_pitch, Cx<R> *__restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int M = g.M, P = M + 1;
+  Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
+  Cx<R> *twz = twm + M;
+  Cx<R> *S = twz + g.NZ;
+  load_twiddles(twm, tw.m, M);
+  load_twiddles(twz, tw.z, g.NZ);
+  const size_t row0 = (size_t)blockIdx.x * ZROWS;
+  for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
+    const int n = it % M, rr = it / M;
+    const R *r = in + (row0 + rr) * (size_t)in_pitch + 2 * n;
+    S[rr * P + bitrev(n, g.lm)] = {r[0], r[1]};
+  }
+  __syncthreads();
+  fft_inplace(S, g.lm, ZROWS, P, 1, twm, 1);
+  for (int it = threadIdx.x; it < ZROWS * (M + 1); it += blockDim.x) {
+    const int k = it % (M + 1), rr = it / (M + 1);
+    out[(row0 + rr) * (M + 1) + k] = r2c_post(S + rr * P, k, M, twz);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// x pass, forward, of the five product spectra fused with the rest of
+// NS_solver_slavedEuler (fluid_solver.cxx:328-354) and the next inverse:
+//   Omega from the product spectra (operate_omega.cxx:60-97), its reduction
+//   (Omega_k2zeta_k), the slaved-Euler update of zeta on the retained modes,
+//   FIX_CELL on uk_dc (sp_3d_ns.cxx:67-73), then Zeta_k2u_k of the updated
+//   zeta and the inverse x transform of u*.
+// In place on buf: reads [5][NX][KYc][TZ], writes [3][NX][KYc][TZ].
+// grid (KYc, ceil(TZ/KC)).
+template <typename R>
+__global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ buf,
+                                                         Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc,
+                                                         int KC) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
+  Cx<R> *Zs = twx + g.NX;          // [KXc][2*KC] updated zeta
+  Cx<R> *Pb = Zs + g.KXc * 2 * KC;  // [NX][5*KC], later [NX][3*KC]
+  __shared__ double ukd[3];
+  const int iy = blockIdx.x;
+  const int kz0 = blockIdx.y * KC;
+  const int ncol = min(KC, g.TZ - kz0);
+  const size_t cstr = (size_t)g.NX * g.KYc * g.TZ;
+  const int W5 = 5 * KC, W3 = 3 * KC;
+  load_twiddles(twx, tw.x, g.NX);
+  const bool has_k0 = (iy == 0 && blockIdx.y == 0);
+  if (threadIdx.x < 3) {
+    double v = 0.0;
+    if (has_k0) {
+      v = g.fix_cell[threadIdx.x] ? 0.0 : uk_dc[threadIdx.x];
+      uk_dc[threadIdx.x] = v;
+    }
+    ukd[threadIdx.x] = v;
+  }
+  for (int it = threadIdx.x; it < 5 * g.NX * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, x = rest % g.NX, c = rest / g.NX;
+    Cx<R> v = {R(0), R(0)};
+    if (col < ncol) v = buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col];
+    Pb[bitrev(x, g.lx) * W5 + c * KC + col] = v;
+  }
+  __syncthreads();
+  fft_inplace(Pb, g.lx, W5, 1, W5, twx, 1);
+  const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
+  const R ky = R(g.wave[1] * KYi);
+  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
+  for (int it = threadIdx.x; it < g.KXc * KC; it += blockDim.x) {
+    const int col = it % KC, ix = it / KC;
+    if (col >= ncol) continue;
+    const int KXi = ix < g.TX ? ix : ix - g.KXc;
+    const int i = KXi >= 0 ? KXi : KXi + g.NX;
+    const int kz = kz0 + col;
+    const R k1 = R(g.wave[0] * KXi), k2 = ky, k3 = R(g.wave[2] * kz);
+    const Cx<R> *p = Pb + i * W5 + col;
+    const Cx<R> a23 = p[0], a31 = p[KC], a12 = p[2 * KC], b2233 = p[3 * KC], b3311 = p[4 * KC];
+    const Cx<R> b1122 = {-b3311.x - b2233.x, -b3311.y - b2233.y};
+    const R k1k2 = k1 * k2, k2k3 = k2 * k3, k3k1 = k3 * k1;
+    const R d32 = (k3 - k2) * (k3 + k2), d13 = (k1 - k3) * (k1 + k3), d21 = (k2 - k1) * (k2 + k1);
+    Cx<R> w[3];
+    w[0] = {-(k2k3 * b2233.x + d32 * a23.x + k3k1 * a12.x - k1k2 * a31.x),
+            -(k2k3 * b2233.y + d32 * a23.y + k3k1 * a12.y - k1k2 * a31.y)};
+    w[1] = {-(k3k1 * b3311.x + d13 * a31.x + k1k2 * a23.x - k2k3 * a12.x),
+            -(k3k1 * b3311.y + d13 * a31.y + k1k2 * a23.y - k2k3 * a12.y)};
+    w[2] = {-(k1k2 * b1122.x + d21 * a12.x + k2k3 * a31.x - k3k1 * a23.x),
+            -(k1k2 * b1122.y + d21 * a12.y + k2k3 * a31.y - k3k1 * a23.y)};
+    Cx<R> f0, f1;
+    select_zeta(KXi, KYi, w, f0, f1);
+    const R K2 = k1 * k1 + k2 * k2 + k3 * k3;
+    const R IK2 = K2 > R(0) ? R(1) / K2 : R(0);
+    const double arg = -g.nu * g.dt * (double)K2;
+    const R dmy = R(g.fp64_exp ? exp(arg) - 1.0 : expm1(arg));
+    const R c1 = R(1.0 / g.nu) * IK2;
+    const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
+    Cx<R> z0 = zeta[o], z1 = zeta[zplane + o];
+    z0 = {z0.x + dmy * (z0.x - c1 * f0.x), z0.y + dmy * (z0.y - c1 * f0.y)};
+    z1 = {z1.x + dmy * (z1.x - c1 * f1.x), z1.y + dmy * (z1.y - c1 * f1.y)};
+    zeta[o] = z0;
+    zeta[zplane + o] = z1;
+    Zs[ix * 2 * KC + col] = z0;
+    Zs[ix * 2 * KC + KC + col] = z1;
+  }
+  __syncthreads();
+  // u*_k = Zeta_k2u_k(zeta', uk_dc) on all NX rows (zero outside |kx| < TX)
+  for (int it = threadIdx.x; it < g.NX * KC; it += blockDim.x) {
+    const int col = it % KC, i = it / KC;
+    Cx<R> u[3] = {{R(0), R(0)}, {R(0), R(0)}, {R(0), R(0)}};
+    const int KXi = signed_k(i, g.NX);
+    if (col < ncol && abs(KXi) < g.TX) {
+      const int ix = KXi >= 0 ? KXi : KXi + g.KXc;
+      const int kz = kz0 + col;
+      const R kx = R(g.wave[0] * KXi), kzr = R(g.wave[2] * kz);
+      const R k2 = kx * kx + ky * ky + kzr * kzr;
+      const R ik2 = k2 > R(0) ? R(1) / k2 : R(0);
+      zeta_to_u(KXi, KYi, kx, ky, kzr, ik2, Zs[ix * 2 * KC + col], Zs[ix * 2 * KC + KC + col], u);
+      if (KXi == 0 && KYi == 0 && kz == 0) {
+        u[0] = {R(ukd[0]), R(0)};
+        u[1] = {R(ukd[1]), R(0)};
+        u[2] = {R(ukd[2]), R(0)};
+      }
+    }
+    const int row = bitrev(i, g.lx);
+    Pb[row * W3 + col] = u[0];
+    Pb[row * W3 + KC + col] = u[1];
+    Pb[row * W3 + 2 * KC + col] = u[2];
+  }
+  __syncthreads();
+  fft_inplace(Pb, g.lx, W3, 1, W3, twx, -1);
+  for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, x = rest % g.NX, c = rest / g.NX;
+    if (col < ncol) buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col] = Pb[x * W3 + c * KC + col];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// x pass, forward, of the rigidity force f fused with the end of the step:
+// 2/3 truncation (implicit), Solenoidal_uk (operate_omega.cxx:186-219) and
+// the k-space form of Add_f_particle + U2zeta_k (f_particle.h:83-99,
+// operate_omega.h:186-189): zeta += U_k2zeta_k(f_sol), uk_dc += Re f(k=0).
+// The velocity before the force is Zeta_k2u of the truncated zeta, so its
+// own U2zeta_k is that zeta again (linearity; parity up to roundoff).
+// in buf [3][NX][KYc][TZ].  grid (KYc, ceil(TZ/KC)).
+template <typename R>
+__global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ buf,
+                                                         Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc,
+                                                         int KC) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
+  Cx<R> *Pb = twx + g.NX;  // [NX][3*KC]
+  const int iy = blockIdx.x;
+  const int kz0 = blockIdx.y * KC;
+  const int ncol = min(KC, g.TZ - kz0);
+  const size_t cstr = (size_t)g.NX * g.KYc * g.TZ;
+  const int W3 = 3 * KC;
+  load_twiddles(twx, tw.x, g.NX);
+  for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, x = rest % g.NX, c = rest / g.NX;
+    Cx<R> v = {R(0), R(0)};
+    if (col < ncol) v = buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col];
+    Pb[bitrev(x, g.lx) * W3 + c * KC + col] = v;
+  }
+  __syncthreads();
+  fft_inplace(Pb, g.lx, W3, 1, W3, twx, 1);
+  const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
+  const R ky = R(g.wave[1] * KYi);
+  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
+  for (int it = threadIdx.x; it < g.KXc * KC; it += blockDim.x) {
+    const int col = it % KC, ix = it / KC;
+    if (col >= ncol) continue;
+    const int KXi = ix < g.TX ? ix : ix - g.KXc;
+    const int i = KXi >= 0 ? KXi : KXi + g.NX;
+    const int kz = kz0 + col;
+    const R kx = R(g.wave[0] * KXi), kzr = R(g.wave[2] * kz);
+    const Cx<R> *p = Pb + i * W3 + col;
+    Cx<R> f0 = p[0], f1 = p[KC], f2 = p[2 * KC];
+    if (KXi == 0 && KYi == 0 && kz == 0) {
+      uk_dc[0] += (double)f0.x;
+      uk_dc[1] += (double)f1.x;
+      uk_dc[2] += (double)f2.x;
+      continue;  // zeta(k=0) stays 0
+    }
+    const R K2 = kx * kx + ky * ky + kzr * kzr;
+    const R IK2 = R(1) / K2;
+    const Cx<R> dk = {IK2 * (f0.x * kx + f1.x * ky + f2.x * kzr), IK2 * (f0.y * kx + f1.y * ky + f2.y * kzr)};
+    f0 = {f0.x - dk.x * kx, f0.y - dk.y * kx};
+    f1 = {f1.x - dk.x * ky, f1.y - dk.y * ky};
+    f2 = {f2.x - dk.x * kzr, f2.y - dk.y * kzr};
+    // omega = -i k x f
+    Cx<R> w[3];
+    w[0] = cmul_mi(Cx<R>{ky * f2.x - kzr * f1.x, ky * f2.y - kzr * f1.y});
+    w[1] = cmul_mi(Cx<R>{kzr * f0.x - kx * f2.x, kzr * f0.y - kx * f2.y});
+    w[2] = cmul_mi(Cx<R>{kx * f1.x - ky * f0.x, kx * f1.y - ky * f0.y});
+    Cx<R> z0, z1;
+    select_zeta(KXi, KYi, w, z0, z1);
+    const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
+    zeta[o] = cadd(zeta[o], z0);
+    zeta[zplane + o] = cadd(zeta[zplane + o], z1);
+  }
+}
+
+}  // namespace kapsel

@@ -1,0 +1,162 @@
+"""GPU parity tests: the CUDA path (through the C ABI) against the oracle.
+
+Tolerances: FP64 path relative error <= 1e-10 per quantity (velocity field,
+zeta, particle state); mixed path (FP32 fields) velocity relative L2 <= 1e-5
+and particle velocities <= 1e-4 relative after the stated number of steps.
+"""
+import numpy as np
+import pytest
+
+from oracle import spm, udf
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+
+
+def _sim(cfg, precision=0):
+    import kapsel_old_b200 as kg
+
+    return kg.Simulation(cfg, precision=precision)
+
+
+def rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    n = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (n if n > 0 else 1.0)
+
+
+def _cfg(np_xyz=(5, 5, 5), n=6, seed=11, kbt=1e-3, **kw):
+    return udf.ns_config(np_xyz, n, seed=seed, kbt=kbt, **kw)
+
+
+@pytest.mark.parametrize("np_xyz", [(4, 4, 4), (5, 4, 6), (6, 6, 6)])
+def test_fft_forward_inverse(np_xyz):
+    cfg = _cfg(np_xyz, 1, seed=1)
+    g = _sim(cfg)
+    S = spm.Spectral(spm.Params(cfg))
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal(S.P.N)
+    ak = g.A2a_k(a)
+    ref = spm.SpmOracle.to_ooura(S.fwd(a))
+    assert rel(ak, ref) < 1e-13
+    back = g.A_k2a(ak)
+    assert rel(back, a) < 1e-13
+
+
+def test_fft_mixed_precision():
+    cfg = _cfg((6, 6, 6), 1, seed=1)
+    g = _sim(cfg, precision=1)
+    S = spm.Spectral(spm.Params(cfg))
+    a = np.random.default_rng(4).standard_normal(S.P.N)
+    assert rel(g.A2a_k(a), spm.SpmOracle.to_ooura(S.fwd(a))) < 1e-6
+
+
+def test_solenoidal_u():
+    cfg = _cfg((5, 5, 5), 1, seed=1)
+    g = _sim(cfg)
+    S = spm.Spectral(spm.Params(cfg))
+    u = np.random.default_rng(5).standard_normal((3,) + tuple(S.P.N))
+    assert rel(g.solenoidal_u(u), S.solenoidal_u(u)) < 1e-12
+
+
+def test_phi_up_scatter():
+    cfg = _cfg((5, 5, 5), 6, seed=11, min_gap=0.2)
+    g = _sim(cfg)
+    O = spm.SpmOracle(cfg)
+    rng = np.random.default_rng(6)
+    st = g.particles()
+    st["v"] = rng.normal(0, 1e-2, st["v"].shape)
+    st["omega"] = rng.normal(0, 1e-3, st["omega"].shape)
+    g.set_particle_state(st)
+    phi, up = g.make_phi_u()
+    phi_o, up_o = O.phi_up(st["x"], st["v"], st["omega"])
+    assert rel(phi, phi_o) < 1e-13
+    assert rel(up, up_o) < 1e-12
+
+
+def test_hydro_force_gather():
+    cfg = _cfg((5, 5, 5), 6, seed=11, min_gap=0.2)
+    g = _sim(cfg)
+    O = spm.SpmOracle(cfg)
+    rng = np.random.default_rng(7)
+    st = g.particles()
+    st["v"] = rng.normal(0, 1e-2, st["v"].shape)
+    st["omega"] = rng.normal(0, 1e-3, st["omega"].shape)
+    g.set_particle_state(st)
+    O.p.v[:] = st["v"]
+    O.p.omega[:] = st["omega"]
+    u = rng.normal(0, 1e-2, (3,) + tuple(O.P.N))
+    f, t = g.calc_f_hydro(u)
+    O.hydro_force(u)
+    assert rel(f, O.p.f_hydro) < 1e-12
+    assert rel(t, O.p.torque_hydro) < 1e-12
+
+
+@pytest.mark.parametrize("np_xyz", [(5, 5, 5), (6, 6, 6)])
+def test_lj_cell_list_forces(np_xyz):
+    # 32^3 has 2 LJ cells per axis: pairs are met more than once (md_force.cxx:72-121)
+    cfg = _cfg(np_xyz, 8, seed=11, min_gap=0.1, gravity_g=0.3, mass_ratio=1.2)
+    g = _sim(cfg)
+    O = spm.SpmOracle(cfg)
+    fr = g.calc_fr()
+    O.force()
+    assert np.abs(O.p.fr).max() > 0
+    assert rel(fr, O.p.fr) < 1e-12
+
+
+def _compare_run(cfg, nsteps, precision, graph=False):
+    g = _sim(cfg, precision)
+    O = spm.SpmOracle(cfg)
+    worst = {}
+    for s in range(nsteps):
+        g.step(1, graph=graph)
+        O.step()
+        uo = O.S.zeta_k2u(O.zeta, O.uk_dc)
+        uo = np.stack([O.S.inv(uo[d]) for d in range(3)])
+        e = {
+            "u": rel(g.velocity(), uo),
+            "zeta": rel(g.zeta(), spm.SpmOracle.to_ooura(np.stack([O.S.truncate(O.zeta[d]) for d in range(2)]))),
+        }
+        p = g.particles()
+        if O.p.n:
+            e["x"] = np.abs(p["x"] - O.p.x).max()
+            e["v"] = rel(p["v"], O.p.v)
+            e["omega"] = rel(p["omega"], O.p.omega)
+            e["f_hydro"] = rel(p["f_hydro"], O.p.f_hydro_previous)
+        for k, v in e.items():
+            worst[k] = max(worst.get(k, 0.0), v)
+    return worst
+
+
+def test_step_fp64_matches_oracle():
+    cfg = _cfg((5, 5, 5), 6, seed=11, kbt=1e-3, min_gap=0.2)
+    w = _compare_run(cfg, 6, 0)
+    for k, v in w.items():
+        assert v < FP64_TOL, (k, v, w)
+
+
+def test_step_fp64_noncubic_gravity_fixcell():
+    cfg = udf.ns_config((4, 5, 6), 3, seed=5, kbt=0.0, gravity_g=0.5, mass_ratio=1.5, rotation="OFF")
+    cfg["fix_cell"] = (True, False, True)
+    w = _compare_run(cfg, 4, 0)
+    for k, v in w.items():
+        assert v < FP64_TOL, (k, v, w)
+
+
+def test_step_graph_equals_eager():
+    cfg = _cfg((5, 5, 5), 6, seed=11, kbt=1e-3, min_gap=0.2)
+    a = _sim(cfg)
+    b = _sim(cfg)
+    a.step(5)
+    b.step(5, graph=True)
+    assert np.array_equal(a.zeta(), b.zeta())
+    assert np.array_equal(a.particles()["x"], b.particles()["x"])
+
+
+def test_step_mixed_precision_bound():
+    cfg = _cfg((6, 6, 6), 16, seed=1, kbt=1e-3)
+    w = _compare_run(cfg, 5, 1)
+    assert w["u"] < 1e-5, w
+    assert w["v"] < 1e-4, w
