@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""SPM steps/s at 128^3 with 256 colloids on B200: mixed precision vs FP64.
+
+Workload (one box per GPU): 128^3 periodic grid, 256 spheres a=5, xi=2,
+kBT=1e-3 thermal kicks, dt=0.01, seeded non-overlapping positions
+(kapsel_old_b200.workload.mixed_128_256).  A step is one
+Time_evolution_hydro of the reference (sp_3d_ns.cxx:61-212).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm: W untimed steps, then K timed steps.  Before every timed step a
+256 MiB buffer is written (L2 flush, the L2 is 126 MB); each step is timed
+with CUDA events on the library's stream; the state is device resident.
+`e2e` repeats K steps through the public C ABI with the per-step host work
+(thermostat normals generated on the host and copied in, particle records
+copied out) inside a wall-clock timed region.  Under torchrun each rank runs
+an independent replica (the north-star path is single-GPU: replicas only);
+the timed region is bracketed by a barrier and the max over ranks is used.
+
+Reference arm: the unmodified KAPSEL sources built by oracle/Makefile
+(oracle/_ref, OpenMP loops on all host cores) timed by wall clock on the same
+workload, min(K, 30) steps after W warm-up steps; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "SPM steps/s at 128³, 256 colloids: mixed vs FP64 on B200, % of HBM roofline"
+UNIT = "steps/s"
+WORKLOAD = "SPM Navier-Stokes step, 128^3 grid, 256 spheres a=5 xi=2, kBT=1e-3, dt=0.01"
+REF_MAX_STEPS = 30
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes of each launch (compulsory reads + writes of the stored
+# operands; complex values 2R, real values R bytes)
+def kernel_bytes(cfg, R: int):
+    NX, NY, NZ = [1 << p for p in cfg["np_xyz"]]
+    T = [(n + 2) // 3 for n in (NX, NY, NZ)]
+    KXc, KYc, TZ = 2 * T[0] - 1, 2 * T[1] - 1, T[2]
+    C = 2 * R
+    N = NX * NY * NZ
+    zeta = 2 * KXc * KYc * TZ * C
+    I1 = NX * KYc * TZ * C  # one component after the x pass
+    I2 = NX * NY * TZ * C  # one component after the y pass
+    Np = len(cfg["particles"])
+    S = sekibun_count(cfg)
+    part = Np * 26 * 8
+    return {
+        "k_x_zeta_to_u": zeta + 3 * I1,
+        "k_y_pass<inv>": 3 * I1 + 3 * I2,
+        "k_z_products": 3 * I2 + 5 * I2,
+        "k_y_pass<fwd>#5": 5 * I2 + 5 * I1,
+        "k_x_advect_update": 5 * I1 + 2 * zeta + 3 * I1,
+        "k_y_pass<inv>#2": 3 * I1 + 3 * I2,
+        "k_z_c2r": 3 * I2 + 3 * N * R,
+        "k_particles_position": 2 * part,
+        "k_particles_hydro_velocity": 3 * Np * S * R + 2 * part,
+        "k_particles_scatter": 2 * 4 * Np * S * R + part,
+        "k_z_force": 7 * N * R + 3 * I2,
+        "k_y_pass<fwd>#3": 3 * I2 + 3 * I1,
+        "k_x_force_to_zeta": 3 * I1 + 2 * zeta,
+    }
+
+
+def sekibun_count(cfg):
+    a, axi = float(cfg.get("a", 5.0)), float(cfg.get("a_xi", 2.0))
+    nh = int(a) + int(axi) + 2
+    rmax = a + 0.5 * axi + 1.7321
+    n = 0
+    for i in range(-nh, nh + 1):
+        for j in range(-nh, nh + 1):
+            for k in range(-nh, nh + 1):
+                if math.sqrt(i * i + j * j + k * k) < rmax:
+                    n += 1
+    return n
+
+
+def step_bytes_model(cfg, R: int):
+    """Compulsory bytes of one step: 40.6 field passes of N*R at 128^3 with
+    256 spheres (stage table in DESIGN.md: 5+7+5 spectral, 0.71 gather,
+    4 phi/up reset, 1.89 scatter, 10 force, 7 zeta update)."""
+    NX, NY, NZ = [1 << p for p in cfg["np_xyz"]]
+    N = NX * NY * NZ
+    Np = len(cfg["particles"])
+    S = sekibun_count(cfg)
+    frac = Np * S / N
+    passes = 5 + 7 + 5 + 3 * frac + 4 + 4 * 2 * frac + 10 + 7
+    return passes * N * R, passes
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import kapsel_old_b200 as kg
+    from kapsel_old_b200 import workload
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+    cfg = workload.mixed_128_256()
+    hbm, peak_kind = peaks()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    L = kg.load_library()
+
+    def timed(precision, steps, warmup):
+        sim = kg.Simulation(cfg, precision=precision)
+        sp = ctypes.c_void_p()
+        sim._check(L.kapsel_gpu_get_stream(sim.h, ctypes.byref(sp)))
+        stream = torch.cuda.ExternalStream(sp.value)
+        sim.step(max(warmup, 3), graph=True)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for k in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+                evs[k][0].record(stream)
+            sim._check(L.kapsel_gpu_step_graph(sim.h, 1))
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        if dist:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return sim, stream, ms
+
+    # ---- mixed precision (headline) with clocks sampled during the timed region
+    clk = ClockSampler(local_rank)
+    clk.start()
+    sim_m, stream_m, ms_m = timed(kg.MIXED, args.steps, args.warmup)
+    clocks = clk.stop()
+    # ---- FP64 path, same workload
+    sim_d, _, ms_d = timed(kg.FP64, args.steps, args.warmup)
+    sim_d.close()
+
+    # ---- per-kernel durations (CUDA events between launches on the library stream)
+    nker = kg.load_library().kapsel_gpu_launches_per_step(sim_m.h)
+    prof_steps = max(5, min(args.steps, 20))
+    acc = np.zeros(13)
+    buf = (ctypes.c_float * 13)()
+    for k in range(prof_steps):
+        with torch.cuda.stream(stream_m):
+            flush.fill_(float(k))
+        torch.cuda.synchronize()
+        sim_m._check(L.kapsel_gpu_profile_step(sim_m.h, buf))
+        acc += np.frombuffer(buf, dtype=np.float32)
+    acc /= prof_steps
+    names = list(kernel_bytes(cfg, 4).keys())
+    shares = {names[i]: float(acc[i]) for i in range(nker)}
+    top = max(range(nker), key=lambda i: acc[i])
+    kb = kernel_bytes(cfg, 4)
+    top_name = names[top]
+    achieved = kb[top_name] / (acc[top] * 1e-3) / 1e9
+
+    # ---- end to end through the public API: host noise + H2D, step, particle D2H
+    Np = sim_m.Np
+    rec = np.zeros((Np, kg.P_STRIDE))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim_m._check(L.kapsel_gpu_step_graph(sim_m.h, 1))
+        sim_m._check(L.kapsel_gpu_get_particles(sim_m.h, rec.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    sim_m.close()
+
+    steps_total = args.steps * world
+    value = steps_total / (ms_m * 1e-3)
+    fp64_value = steps_total / (ms_d * 1e-3)
+    bstep, passes = step_bytes_model(cfg, 4)
+    line = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_m / args.steps, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded positions, PCG64 seed 2; MT19937 seed 0 thermostat)",
+        "config": {
+            "workload": WORKLOAD,
+            "grid": [128, 128, 128],
+            "particles": 256,
+            "precision": "mixed: f32 fields/FFTs/stencil fields, f64 particles, reductions, k=0 mode",
+            "l2": "256 MiB buffer written before every timed step (L2 126 MB)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "cuda_graph": True,
+        },
+        "fp64": {"value": round(fp64_value, 3), "ms_per_step": round(ms_d / args.steps, 5),
+                 "mixed_over_fp64": round(value / fp64_value, 3)},
+        "roofline": {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": hbm,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                     "algorithmic_bytes_per_launch": kb[top_name], "avg_launch_ms": round(float(acc[top]), 5),
+                     "traffic": None},
+        "step_roofline": {"bytes_per_step_model": int(bstep), "field_passes": round(passes, 2),
+                          "achieved_gbs": round(bstep / (ms_m / args.steps * 1e-3) / 1e9, 1),
+                          "frac": round(bstep / (ms_m / args.steps * 1e-3) / 1e9 / hbm, 4)},
+        "kernel_ms": {k: round(v, 5) for k, v in shares.items()},
+        "e2e": {"value": round(steps_total / e2e_s, 3), "unit": UNIT, "h2d_bytes_per_step": 6 * 8 * Np,
+                "d2h_bytes_per_step": kg.P_STRIDE * 8 * Np + 4},
+        "gpu_launches": nker * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, warmup=1, steps=min(args.steps, 12))
+    return line
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(cfg, warmup: int, steps: int, threads: int | None = None):
+    """Reference CPU timing on the host cores (oracle/_ref; else the numpy port)."""
+    from oracle import ref, udf
+
+    threads = threads or os.cpu_count() or 1
+    exe = os.path.join(ref.REF_DIR, "kapsel_ref_omp")
+    if os.path.exists(exe):
+        with tempfile.TemporaryDirectory() as td:
+            kv = udf.write_udf(os.path.join(td, "in.kv"), cfg)
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+            out = subprocess.run([exe, kv, str(warmup), str(steps)], capture_output=True, text=True, env=env,
+                                 timeout=900)
+            d = json.loads(out.stdout.strip().splitlines()[-1])
+        return {"value": round(1.0 / d["s_per_step"], 4), "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"{steps} steps of the same 128^3/256-sphere workload after {warmup} warm-up, "
+                          f"unmodified KAPSEL sources (OpenMP loops, Ooura FFT), wall clock"}
+    from oracle import spm
+
+    o = spm.SpmOracle(cfg)
+    o.run(warmup)
+    t = time.perf_counter()
+    n = max(1, min(steps, 3))
+    o.run(n)
+    dt = (time.perf_counter() - t) / n
+    return {"value": round(1.0 / dt, 4), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} steps of the same workload, numpy restatement"}
+
+
+def run_reference(args):
+    from kapsel_old_b200 import workload
+
+    cfg = workload.mixed_128_256()
+    steps = max(1, min(args.steps, REF_MAX_STEPS))
+    cb = cpu_baseline(cfg, warmup=max(1, min(args.warmup, 3)), steps=steps)
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": cb["value"],
+        "unit": UNIT,
+        "n_gpus": 0,
+        "steps": steps,
+        "warmup": max(1, min(args.warmup, 3)),
+        "ms_per_step": round(1000.0 / cb["value"], 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded positions, PCG64 seed 2; MT19937 seed 0 thermostat)",
+        "config": {"workload": WORKLOAD, "grid": [128, 128, 128], "particles": 256,
+                   "precision": "reference FP64 CPU"},
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    line = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -150,6 +150,22 @@ int kapsel_gpu_calc_f_hydro(kapsel_ctx *ctx, const double *u0, const double *u1,
    context's particles; writes fr[n*3]. */
 int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr);
 
+/* ---- Measurement hooks. ---- */
+
+/* Number of kernel launches of one step (and its upper bound). */
+#define KAPSEL_N_STEP_KERNELS 13
+int kapsel_gpu_launches_per_step(kapsel_ctx *ctx);
+const char *kapsel_gpu_kernel_name(int i);
+
+/* The context's CUDA stream (a cudaStream_t), for recording events around
+   its work. */
+int kapsel_gpu_get_stream(kapsel_ctx *ctx, void **stream);
+
+/* One step with a CUDA event between consecutive launches on the context's
+   stream; ms[i] receives the duration of launch i (KAPSEL_N_STEP_KERNELS
+   floats).  Advances the state exactly like kapsel_gpu_step(ctx, 1). */
+int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms);
+
 /* Human-readable text of a status code. */
 const char *kapsel_gpu_strerror(int status);
 

@@ -148,7 +148,7 @@ struct BoxBase {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
 
   virtual int alloc() = 0;
-  virtual void launch_step(const double *noise, int euler) = 0;
+  virtual void launch_step(const double *noise, int euler, cudaEvent_t *ev = nullptr) = 0;
   virtual void launch_init() = 0;
   virtual int velocity_to_host(double *u) = 0;
   virtual int zeta_to_host(double *z) = 0;
@@ -268,19 +268,39 @@ struct Box : BoxBase {
     k_x_force_to_zeta<R><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc, KCX);
   }
 
-  void launch_step(const double *noise, int euler) override {
+  void launch_step(const double *noise, int euler, cudaEvent_t *ev = nullptr) override {
+    int e = 0;
+    auto mark = [&]() {
+      if (ev) cudaEventRecord(ev[e++], stream);
+    };
+    mark();
     k_x_zeta_to_u<R><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA, KCX);
+    mark();
     k_y_pass<R, true><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB, KCY);
+    mark();
     k_z_products<R><<<gz(), 256, smem_zp, stream>>>(g, tw, bufB);
+    mark();
     k_y_pass<R, false><<<gy(5), 256, smem_y, stream>>>(g, tw, bufB, bufA, KCY);
+    mark();
     k_x_advect_update<R><<<gx(), 256, smem_xadv, stream>>>(g, tw, bufA, zeta, uk_dc, KCX);
+    mark();
     k_y_pass<R, true><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB, KCY);
+    mark();
     k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, npts(), g.NZ);
+    mark();
     if (Np > 0) {
       k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
+      mark();
       k_particles_hydro_velocity<R><<<Np, 256, 0, stream>>>(pp, parts, ustar, cells, noise, euler, status);
+      mark();
       k_particles_scatter<R><<<Np, 256, 0, stream>>>(pp, parts, cells, phiup);
-      launch_force_to_zeta();
+      mark();
+      k_z_force<R><<<gz(), 256, smem_zf, stream>>>(g, tw, phiup, ustar, bufB);
+      mark();
+      k_y_pass<R, false><<<gy(3), 256, smem_y, stream>>>(g, tw, bufB, bufA, KCY);
+      mark();
+      k_x_force_to_zeta<R><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc, KCX);
+      mark();
     }
   }
 
@@ -512,7 +532,7 @@ int Box<R>::fft_fwd_host(double *a) {
   Cx<R> *dout = nullptr;
   KCHECK(cudaMalloc(&din, sizeof(R) * npt));
   KCHECK(cudaMalloc(&dout, sizeof(Cx<R>) * (size_t)g.NX * g.NY * M1));
-  KCHECK(cudaMemcpy(din, h.data(), sizeof(R) * npt, cudaMemcpyHostToDevice));
+  KCHECK(cudaMemcpyAsync(din, h.data(), sizeof(R) * npt, cudaMemcpyHostToDevice, stream));
   int rc = FullFFT<R>::forward(*this, din, dout);
   std::vector<Cx<R>> o((size_t)g.NX * g.NY * M1);
   KCHECK(cudaMemcpyAsync(o.data(), dout, sizeof(Cx<R>) * o.size(), cudaMemcpyDeviceToHost, stream));
@@ -540,7 +560,7 @@ int Box<R>::fft_inv_host(double *a) {
   R *dout = nullptr;
   KCHECK(cudaMalloc(&din, sizeof(Cx<R>) * h.size()));
   KCHECK(cudaMalloc(&dout, sizeof(R) * npt));
-  KCHECK(cudaMemcpy(din, h.data(), sizeof(Cx<R>) * h.size(), cudaMemcpyHostToDevice));
+  KCHECK(cudaMemcpyAsync(din, h.data(), sizeof(Cx<R>) * h.size(), cudaMemcpyHostToDevice, stream));
   int rc = FullFFT<R>::inverse(*this, din, dout);
   std::vector<R> o(npt);
   KCHECK(cudaMemcpyAsync(o.data(), dout, sizeof(R) * npt, cudaMemcpyDeviceToHost, stream));
@@ -594,7 +614,8 @@ int Box<R>::solenoidal_host(double *u0, double *u1, double *u2) {
   KCHECK(cudaMalloc(&dk, sizeof(Cx<R>) * 3 * nk));
   for (int c = 0; c < 3; ++c) {
     std::vector<R> h = pack_real<R>(hu[c], g);
-    KCHECK(cudaMemcpy(din + c * npt, h.data(), sizeof(R) * npt, cudaMemcpyHostToDevice));
+    KCHECK(cudaMemcpyAsync(din + c * npt, h.data(), sizeof(R) * npt, cudaMemcpyHostToDevice, stream));
+    KCHECK(cudaStreamSynchronize(stream));
     FullFFT<R>::forward(*this, din + c * npt, dk + c * nk);
   }
   k_solenoidal_full<R><<<592, 256, 0, stream>>>(g, dk, dk + nk, dk + 2 * nk);
@@ -678,7 +699,8 @@ int Box<R>::fhydro_host(const double *u0, const double *u1, const double *u2, do
   const double *hu[3] = {u0, u1, u2};
   for (int c = 0; c < 3; ++c) {
     std::vector<R> h = pack_real<R>(hu[c], g);
-    KCHECK(cudaMemcpy(d + c * npt, h.data(), sizeof(R) * npt, cudaMemcpyHostToDevice));
+    KCHECK(cudaMemcpyAsync(d + c * npt, h.data(), sizeof(R) * npt, cudaMemcpyHostToDevice, stream));
+    KCHECK(cudaStreamSynchronize(stream));
   }
   if (Np > 0) k_gather_only<R><<<Np, 256, 0, stream>>>(pp, parts, d, cells, o);
   KCHECK(cudaGetLastError());
@@ -903,7 +925,9 @@ int kapsel_gpu_set_particles(kapsel_ctx *ctx, const double *x, const double *q) 
     }
     for (int i = 0; i < 4; ++i) h[n].q[i] = h[n].q_old[i] = qq[i];
   }
-  if (cudaMemcpy(b->parts, h.data(), sizeof(DPart) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+  if (cudaMemcpyAsync(b->parts, h.data(), sizeof(DPart) * h.size(), cudaMemcpyHostToDevice, b->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(b->stream) != cudaSuccess)
     return KAPSEL_ECUDA;
   b->particles_set = true;
   return 0;
@@ -968,7 +992,9 @@ int kapsel_gpu_get_zeta(kapsel_ctx *ctx, double *zeta, double *uk_dc) {
   int rc = b->zeta_to_host(zeta);
   if (rc) return rc;
   if (uk_dc) {
-    if (cudaMemcpy(uk_dc, b->uk_dc, sizeof(double) * 3, cudaMemcpyDeviceToHost) != cudaSuccess) return KAPSEL_ECUDA;
+    if (cudaMemcpyAsync(uk_dc, b->uk_dc, sizeof(double) * 3, cudaMemcpyDeviceToHost, b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+      return KAPSEL_ECUDA;
   }
   return 0;
 }
@@ -978,7 +1004,9 @@ int kapsel_gpu_set_zeta(kapsel_ctx *ctx, const double *zeta, const double *uk_dc
   BoxBase *b = ctx->box.get();
   int rc = b->zeta_from_host(zeta);
   if (rc) return rc;
-  if (cudaMemcpy(b->uk_dc, uk_dc, sizeof(double) * 3, cudaMemcpyHostToDevice) != cudaSuccess) return KAPSEL_ECUDA;
+  if (cudaMemcpyAsync(b->uk_dc, uk_dc, sizeof(double) * 3, cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+      cudaStreamSynchronize(b->stream) != cudaSuccess)
+    return KAPSEL_ECUDA;
   b->initialised = true;
   return 0;
 }
@@ -1043,7 +1071,9 @@ int kapsel_gpu_set_particle_state(kapsel_ctx *ctx, const double *in) {
       a.q_old[i] = o[KAPSEL_P_QOLD + i];
     }
   }
-  if (cudaMemcpy(b->parts, h.data(), sizeof(DPart) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+  if (cudaMemcpyAsync(b->parts, h.data(), sizeof(DPart) * h.size(), cudaMemcpyHostToDevice, b->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(b->stream) != cudaSuccess)
     return KAPSEL_ECUDA;
   b->particles_set = true;
   return 0;
@@ -1123,6 +1153,48 @@ int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr) {
   for (int n = 0; n < b->Np; ++n)
     for (int d = 0; d < 3; ++d) fr[3 * n + d] = h[n].fr_prev[d];
   return 0;
+}
+
+static const char *kKernelNames[KAPSEL_N_STEP_KERNELS] = {
+    "k_x_zeta_to_u",        "k_y_pass<inv>",        "k_z_products",       "k_y_pass<fwd>",
+    "k_x_advect_update",    "k_y_pass<inv>",        "k_z_c2r",            "k_particles_position",
+    "k_particles_hydro_velocity", "k_particles_scatter", "k_z_force",       "k_y_pass<fwd>",
+    "k_x_force_to_zeta"};
+
+int kapsel_gpu_get_stream(kapsel_ctx *ctx, void **stream) {
+  if (!ctx || !stream) return KAPSEL_EINVAL;
+  *stream = (void *)ctx->box->stream;
+  return 0;
+}
+
+int kapsel_gpu_launches_per_step(kapsel_ctx *ctx) {
+  if (!ctx) return KAPSEL_EINVAL;
+  return ctx->box->Np > 0 ? KAPSEL_N_STEP_KERNELS : 7;
+}
+
+const char *kapsel_gpu_kernel_name(int i) {
+  return (i >= 0 && i < KAPSEL_N_STEP_KERNELS) ? kKernelNames[i] : "";
+}
+
+int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms) {
+  if (!ctx || !ms) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (!b->initialised) return KAPSEL_ESTATE;
+  const int slot = b->ts & 1;
+  int rc = b->fill_noise(slot);
+  if (rc) return rc;
+  cudaEvent_t ev[KAPSEL_N_STEP_KERNELS + 1];
+  for (int i = 0; i <= KAPSEL_N_STEP_KERNELS; ++i)
+    if (cudaEventCreate(&ev[i]) != cudaSuccess) return KAPSEL_ECUDA;
+  b->launch_step(b->noise_dev[slot], b->ts == 0 ? 1 : 0, ev);
+  b->ts += 1;
+  b->time += b->prm.dt;
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
+  const int nk = b->Np > 0 ? KAPSEL_N_STEP_KERNELS : 7;
+  for (int i = 0; i < KAPSEL_N_STEP_KERNELS; ++i) ms[i] = 0.f;
+  for (int i = 0; i < nk; ++i) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+  for (int i = 0; i <= KAPSEL_N_STEP_KERNELS; ++i) cudaEventDestroy(ev[i]);
+  return check_status(b);
 }
 
 }  // extern "C"

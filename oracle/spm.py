@@ -110,7 +110,7 @@ class Spectral:
 
     def inv(self, A):
         """A_k2a (fft_wrapper.h:534-631)."""
-        return np.fft.irfftn(np.conj(A), s=self.P.N)
+        return np.fft.irfftn(np.conj(A), s=self.P.N, axes=(0, 1, 2))
 
     def truncate(self, A):
         """Truncate_two_third_rule_ooura (fft_wrapper.h:723-766)."""
