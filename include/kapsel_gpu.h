@@ -150,6 +150,17 @@ int kapsel_gpu_calc_f_hydro(kapsel_ctx *ctx, const double *u0, const double *u1,
    context's particles; writes fr[n*3]. */
 int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr);
 
+/* ---- Host-only helpers (no GPU needed). ---- */
+
+/* n normals (n even) of the thermostat stream Add_random_force_thermostat
+   draws (fluct.cxx:21-35): Gauss2 pairs (fluct.h:48-60) from MT19937 seeded by
+   init_genrand(seed) (mt19937ar.c), after skipping `skip` normals. */
+int kapsel_thermostat_normals(unsigned int seed, long long skip, long long n, double *out);
+
+/* Sekibun stencil offsets of Particle_domain (profile.cxx:25-74): returns the
+   point count; writes 3 ints per point when out != NULL (cap = points room). */
+int kapsel_sekibun_cells(double a, double a_xi, double dx, int *out, int cap);
+
 /* ---- Measurement hooks. ---- */
 
 /* Number of kernel launches of one step (and its upper bound). */

@@ -1161,6 +1161,28 @@ static const char *kKernelNames[KAPSEL_N_STEP_KERNELS] = {
     "k_particles_hydro_velocity", "k_particles_scatter", "k_z_force",       "k_y_pass<fwd>",
     "k_x_force_to_zeta"};
 
+int kapsel_thermostat_normals(unsigned int seed, long long skip, long long n, double *out) {
+  // n normals of the reference thermostat stream: Gauss2 pairs from MT19937
+  // seeded with init_genrand(seed), after `skip` normals (skip even).
+  if (!out || n < 0 || skip < 0 || (skip & 1) || (n & 1)) return KAPSEL_EINVAL;
+  MT19937 mt(seed);
+  double pair[2];
+  for (long long i = 0; i < skip; i += 2) mt.gauss2(pair);
+  for (long long i = 0; i < n; i += 2) mt.gauss2(out + i);
+  return 0;
+}
+
+int kapsel_sekibun_cells(double a, double a_xi, double dx, int *out, int cap) {
+  if (!(a > 0.0) || !(a_xi > 0.0) || !(dx > 0.0)) return KAPSEL_EINVAL;
+  std::vector<int> c = sekibun(a, a_xi, dx);
+  const int n = (int)c.size() / 3;
+  if (out) {
+    if (cap < n) return KAPSEL_ERANGE;
+    memcpy(out, c.data(), sizeof(int) * c.size());
+  }
+  return n;
+}
+
 int kapsel_gpu_get_stream(kapsel_ctx *ctx, void **stream) {
   if (!ctx || !stream) return KAPSEL_EINVAL;
   *stream = (void *)ctx->box->stream;

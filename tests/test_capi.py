@@ -1,0 +1,91 @@
+"""The C ABI library loads without a GPU and exports every symbol that
+include/kapsel_gpu.h declares; host-only helpers are checked against the
+oracle (no device calls)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "kapsel_gpu.h")
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(kapsel_\w+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import kapsel_old_b200 as kg
+
+    if not os.path.exists(kg.LIB_PATH):
+        from kapsel_old_b200 import build
+
+        build.build()
+    return ctypes.CDLL(kg.LIB_PATH)
+
+
+def test_exports_every_declared_symbol(lib):
+    syms = declared_symbols()
+    assert len(syms) >= 25
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_strerror_and_params_default(lib):
+    import kapsel_old_b200 as kg
+
+    L = kg.load_library()
+    assert L.kapsel_gpu_strerror(0) == b"ok"
+    assert b"invalid" in L.kapsel_gpu_strerror(-1)
+    p = kg._Params()
+    L.kapsel_params_default(ctypes.byref(p))
+    assert list(p.np_xyz) == [6, 6, 6] and p.dt == 0.01 and p.a == 5.0 and p.rotation == 1
+
+
+def test_thermostat_stream_matches_reference_mt19937(lib):
+    from oracle import spm
+
+    L = lib
+    L.kapsel_thermostat_normals.argtypes = [ctypes.c_uint, ctypes.c_longlong, ctypes.c_longlong,
+                                            ctypes.POINTER(ctypes.c_double)]
+    out = np.zeros(600)
+    assert L.kapsel_thermostat_normals(0, 0, 600, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 0
+    g = spm.MT19937Gauss(0)
+    ref = g.normals6(100).reshape(-1)
+    assert np.array_equal(out, ref)
+    skip = np.zeros(12)
+    assert L.kapsel_thermostat_normals(0, 588, 12, skip.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 0
+    assert np.array_equal(skip, ref[588:])
+
+
+def test_sekibun_matches_oracle(lib):
+    from oracle import spm
+
+    L = lib
+    L.kapsel_sekibun_cells.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    for a, counts in ((5.0, 1935), (4.0, 1309), (6.0, 2801), (10.0, 8709)):
+        n = L.kapsel_sekibun_cells(a, 2.0, 1.0, None, 0)
+        assert n == counts
+        buf = (ctypes.c_int * (3 * n))()
+        assert L.kapsel_sekibun_cells(a, 2.0, 1.0, buf, n) == n
+        mine = np.frombuffer(buf, dtype=np.int32).reshape(n, 3)
+        cfg = {"np_xyz": (6, 6, 6), "particles": [], "a": a, "a_xi": 2.0}
+        assert np.array_equal(mine, spm.sekibun_cells(spm.Params(cfg)))
+
+
+def test_invalid_arguments_rejected_without_gpu(lib):
+    import kapsel_old_b200 as kg
+
+    L = kg.load_library()
+    assert L.kapsel_gpu_create(None, None) == -1
+    p = kg._Params()
+    L.kapsel_params_default(ctypes.byref(p))
+    p.np_xyz[0] = 3  # grids are 16..512 per axis
+    h = ctypes.c_void_p()
+    assert L.kapsel_gpu_create(ctypes.byref(p), ctypes.byref(h)) == -1
