@@ -150,6 +150,26 @@ int kapsel_gpu_calc_f_hydro(kapsel_ctx *ctx, const double *u0, const double *u1,
    context's particles; writes fr[n*3]. */
 int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr);
 
+/* Solenoidal_u on three real fields that are already in device memory,
+   packed as NX*NY*NZ doubles each (no NZ_ padding), written to three device
+   output fields of the same shape, on `stream` (a cudaStream_t; NULL for the
+   default stream).  Unlike every other entry point it allocates nothing:
+   its spectra and twiddle tables live in one static device array of about
+   6.2 MiB (64*64*33 complex values per component plus tables) that each GPU
+   loading this library keeps until exit.  It is meant for callers that
+   cannot call cudaMalloc (a caller whose device memory is owned by another
+   allocator, or one that must not synchronise or fail on allocation in the
+   middle of a step).  Grids are powers of two, 16..128 per axis, with
+   NX*NY*(NZ/2+1) <= 64*64*33; larger grids return KAPSEL_ERANGE.  The first
+   call on a device looks up the array's device address (once per device,
+   with that device current); make that first call before any stream
+   capture.  All calls share the one array, so calls that overlap on the GPU
+   (different streams or threads at the same time) race; serialise them.
+   The call is asynchronous on `stream`.  No counterpart in the reference:
+   it is an addition of this library. */
+int kapsel_gpu_solenoidal_u_noalloc(const int *np_xyz, double dx, const double *u0, const double *u1,
+                                    const double *u2, double *o0, double *o1, double *o2, void *stream);
+
 /* ---- Host-only helpers (no GPU needed). ---- */
 
 /* n normals (n even) of the thermostat stream Add_random_force_thermostat

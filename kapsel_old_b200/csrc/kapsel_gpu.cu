@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -1220,3 +1221,145 @@ int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free Solenoidal_u on device arrays.
+//
+// Some callers cannot allocate device memory: code that runs while another
+// component owns every allocation (a fixed memory pool or a host program
+// whose allocator is not CUDA-aware), or code that must not call cudaMalloc
+// because that call can synchronise the device or fail under memory
+// pressure in the middle of a time step.  For them this entry point does the
+// 2/3-truncated solenoidal projection of three real fields without
+// allocating: its three spectra and its twiddle tables live in one
+// file-scope device array of fixed size, which every GPU that loads this
+// library holds until the process exits.
+namespace {
+
+// Largest grid the static scratch holds: NX*NY*(NZ/2+1) <= 64*64*33 complex
+// values per component (any axis 16..128), i.e. 64^3 or an equal-size box.
+constexpr size_t kNoAllocMaxModes = 64 * 64 * 33;
+constexpr size_t kNoAllocMaxTwiddles = 128 + 128 + 64 + 128;
+constexpr size_t kNoAllocScratchDoubles = 2 * (3 * kNoAllocMaxModes + kNoAllocMaxTwiddles);
+
+static __device__ __align__(256) double kNoAllocScratch[kNoAllocScratchDoubles];
+
+// The host-side name of kNoAllocScratch is only a stand-in for the device
+// array; its device address comes from cudaGetSymbolAddress, looked up once
+// per device with that device current and then reused.
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+int noalloc_scratch(void **out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return KAPSEL_ECUDA;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, kNoAllocScratch) != cudaSuccess || !p) return KAPSEL_ECUDA;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+
+__global__ void k_noalloc_twiddles(Cx<double> *tw, int nx, int ny, int m, int nz) {
+  const int n[4] = {nx, ny, m, nz};
+  int off = 0;
+  for (int t = 0; t < 4; ++t) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n[t]; j += gridDim.x * blockDim.x) {
+      double s, c;
+      sincospi(2.0 * (double)j / (double)n[t], &s, &c);
+      tw[off + j] = {c, s};
+    }
+    off += n[t];
+  }
+}
+
+}  // namespace
+
+extern "C" int kapsel_gpu_solenoidal_u_noalloc(const int *np_xyz, double dx, const double *u0, const double *u1,
+                                               const double *u2, double *o0, double *o1, double *o2, void *stream) {
+  if (!np_xyz || !u0 || !u1 || !u2 || !o0 || !o1 || !o2 || !(dx > 0.0)) return KAPSEL_EINVAL;
+  for (int d = 0; d < 3; ++d)
+    if (np_xyz[d] < 4 || np_xyz[d] > 7) return KAPSEL_ERANGE;  // each axis 16..128
+  Geo g;
+  memset(&g, 0, sizeof(g));
+  g.NX = 1 << np_xyz[0];
+  g.NY = 1 << np_xyz[1];
+  g.NZ = 1 << np_xyz[2];
+  g.M = g.NZ / 2;
+  const size_t modes = (size_t)g.NX * g.NY * (g.M + 1);
+  if (modes > kNoAllocMaxModes) return KAPSEL_ERANGE;
+  g.lx = ilog2(g.NX);
+  g.ly = ilog2(g.NY);
+  g.lm = ilog2(g.M);
+  g.TX = (g.NX + 2) / 3;
+  g.TY = (g.NY + 2) / 3;
+  g.TZ = (g.NZ + 2) / 3;
+  g.KXc = 2 * g.TX - 1;
+  g.KYc = 2 * g.TY - 1;
+  g.wave[0] = 2.0 * M_PI / (g.NX * dx);
+  g.wave[1] = 2.0 * M_PI / (g.NY * dx);
+  g.wave[2] = 2.0 * M_PI / (g.NZ * dx);
+  g.inv_n = 1.0 / ((double)g.NX * g.NY * g.NZ);
+  void *base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  Cx<double> *spec = reinterpret_cast<Cx<double> *>(base);
+  Cx<double> *twb = spec + 3 * kNoAllocMaxModes;
+  // the tables are rewritten on every call (the previous call may have used
+  // another grid); the spectra need no clearing: the forward transform
+  // writes every entry before anything reads it
+  k_noalloc_twiddles<<<2, 128, 0, s>>>(twb, g.NX, g.NY, g.M, g.NZ);
+  Twiddles<double> tw;
+  tw.x = twb;
+  tw.y = twb + g.NX;
+  tw.m = twb + g.NX + g.NY;
+  tw.z = twb + g.NX + g.NY + g.M;
+  const int M1 = g.M + 1;
+  const int gz = (g.NX * g.NY) / ZROWS;
+  const size_t sm_z = sizeof(Cx<double>) * (g.M + g.NZ + (size_t)ZROWS * (g.M + 1));
+  auto col = [&](Cx<double> *data, bool inv, int axis) {
+    const int n = axis == 0 ? g.NX : g.NY;
+    const int logn = axis == 0 ? g.lx : g.ly;
+    const Cx<double> *twn = axis == 0 ? tw.x : tw.y;
+    const size_t sm = sizeof(Cx<double>) * (n + (size_t)n * 16);
+    if (axis == 0) {
+      const int nl = g.NY * M1;
+      if (inv)
+        k_col_pass<double, true><<<(nl + 15) / 16, 256, sm, s>>>(g, twn, logn, n, data, data, 1,
+                                                                  (long long)g.NY * M1, nl);
+      else
+        k_col_pass<double, false><<<(nl + 15) / 16, 256, sm, s>>>(g, twn, logn, n, data, data, 1,
+                                                                   (long long)g.NY * M1, nl);
+    } else {
+      for (int x = 0; x < g.NX; ++x) {
+        Cx<double> *b = data + (size_t)x * g.NY * M1;
+        if (inv)
+          k_col_pass<double, true><<<(M1 + 15) / 16, 256, sm, s>>>(g, twn, logn, n, b, b, 1, M1, M1);
+        else
+          k_col_pass<double, false><<<(M1 + 15) / 16, 256, sm, s>>>(g, twn, logn, n, b, b, 1, M1, M1);
+      }
+    }
+  };
+  const double *in[3] = {u0, u1, u2};
+  double *out[3] = {o0, o1, o2};
+  for (int c = 0; c < 3; ++c) {
+    Cx<double> *sc = spec + c * modes;
+    k_z_r2c_full<double><<<gz, 256, sm_z, s>>>(g, tw, in[c], g.NZ, sc);
+    col(sc, false, 1);
+    col(sc, false, 0);
+  }
+  k_solenoidal_full<double><<<592, 256, 0, s>>>(g, spec, spec + modes, spec + 2 * modes);
+  for (int c = 0; c < 3; ++c) {
+    Cx<double> *sc = spec + c * modes;
+    col(sc, true, 0);
+    col(sc, true, 1);
+    k_z_c2r_full<double><<<gz, 256, sm_z, s>>>(g, tw, sc, out[c], g.inv_n);
+  }
+  if (cudaGetLastError() != cudaSuccess) return KAPSEL_ECUDA;
+  return 0;
+}
