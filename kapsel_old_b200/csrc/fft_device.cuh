@@ -16,7 +16,7 @@
 namespace kapsel {
 
 template <typename R>
-struct Cx {
+struct alignas(2 * sizeof(R)) Cx {
   R x, y;
 };
 
@@ -53,9 +53,10 @@ __device__ __forceinline__ Cx<R> twid(const Cx<R> *tw, int j, int sign) {
 // memory in bit-reversed order.  Element e of sequence c is at
 // buf[c*cstride + e*estride].  tw holds exp(+2 pi i j/N), j < N.  All
 // threads of the block must call it; it ends with a barrier.
-template <typename R>
-__device__ void fft_inplace(Cx<R> *buf, int logn, int ncols, int cstride, int estride, const Cx<R> *tw,
+template <typename R, int NCOLS = 0>
+__device__ void fft_inplace(Cx<R> *buf, int logn, int ncols_rt, int cstride, int estride, const Cx<R> *tw,
                             int sign) {
+  const int ncols = NCOLS > 0 ? NCOLS : ncols_rt;
   const int N = 1 << logn;
   int s = 0;
   if (logn & 1) {
@@ -96,6 +97,25 @@ __device__ void fft_inplace(Cx<R> *buf, int logn, int ncols, int cstride, int es
     }
     __syncthreads();
   }
+}
+
+// Asynchronous global -> shared copies (cp.async): every thread queues all of
+// its copies before waiting once, so a tile load keeps many requests in flight.
+__device__ __forceinline__ void cp_async_8(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+template <typename R>
+__device__ __forceinline__ void cp_async_cx(Cx<R> *smem, const Cx<R> *gmem) {
+  if (sizeof(Cx<R>) == 16)
+    cp_async_16(smem, gmem);
+  else
+    cp_async_8(smem, gmem);
 }
 
 // Cooperative copy of a twiddle table (n entries) into shared memory.

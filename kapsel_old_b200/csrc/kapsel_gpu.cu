@@ -187,14 +187,13 @@ struct Box : BoxBase {
   R *phiup = nullptr;     // [4][NX][NY][NZ]
   Cx<R> *twbuf = nullptr;
   Twiddles<R> tw;
-  int KCX = 16, KCY = 16;
+  static constexpr int KCX = sizeof(R) == 4 ? 16 : 8;  // x-pass kz tile
+  static constexpr int KCY = 16;                        // y-pass kz tile
   size_t smem_xu = 0, smem_xadv = 0, smem_xf = 0, smem_y = 0, smem_zp = 0, smem_zc = 0, smem_zf = 0;
 
   size_t npts() const { return (size_t)g.NX * g.NY * g.NZ; }
 
   int alloc() override {
-    KCX = sizeof(R) == 4 ? 16 : 8;
-    KCY = 16;
     const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
     const size_t nA = (size_t)g.NX * g.KYc * g.TZ;
     const size_t nB = (size_t)g.NX * g.NY * g.TZ;
@@ -225,20 +224,20 @@ struct Box : BoxBase {
     tw.z = twbuf + off[3];
     const size_t C = sizeof(Cx<R>);
     const int P = g.M + 1;
-    smem_xu = C * (g.NX + (size_t)g.NX * 3 * KCX);
-    smem_xadv = C * (g.NX + (size_t)g.KXc * 2 * KCX + (size_t)g.NX * 5 * KCX);
-    smem_xf = C * (g.NX + (size_t)g.NX * 3 * KCX);
+    smem_xu = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)g.NX * 3 * KCX);
+    smem_xadv = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)g.NX * 5 * KCX);
+    smem_xf = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)g.NX * 3 * KCX);
     smem_y = C * (g.NY + (size_t)g.NY * KCY);
     smem_zp = C * (g.M + g.NZ + (size_t)ZROWS * 8 * P);
-    smem_zc = C * (g.M + g.NZ + (size_t)ZROWS * P);
+    smem_zc = C * (g.M + g.NZ + (size_t)ZROWS * P + (size_t)ZROWS * g.TZ);
     smem_zf = C * (g.M + g.NZ + (size_t)ZROWS * 3 * P);
     const size_t mx = 227 * 1024;
     if (smem_xadv > mx || smem_xu > mx || smem_y > mx || smem_zp > mx) return KAPSEL_ERANGE;
-    KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
-    KCHECK(cudaFuncSetAttribute(k_x_advect_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xadv));
-    KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xf));
-    KCHECK(cudaFuncSetAttribute(k_y_pass<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
-    KCHECK(cudaFuncSetAttribute(k_y_pass<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
+    KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
+    KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xadv));
+    KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xf));
+    KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
+    KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
     KCHECK(cudaFuncSetAttribute(k_z_products<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zp));
     KCHECK(cudaFuncSetAttribute(k_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
     KCHECK(cudaFuncSetAttribute(k_z_r2c_full<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
@@ -257,16 +256,16 @@ struct Box : BoxBase {
 
   // zeta -> u* (real) through launches 1,2,(7); used by the velocity readout
   void launch_zeta_to_real(R *out, size_t cstride, int pitch) {
-    k_x_zeta_to_u<R><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA, KCX);
-    k_y_pass<R, true><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB, KCY);
+    k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
+    k_y_pass<R, true, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, out, cstride, pitch);
   }
 
   // f (from phi/up and u*) -> zeta update, launches 11-13
   void launch_force_to_zeta() {
     k_z_force<R><<<gz(), 256, smem_zf, stream>>>(g, tw, phiup, ustar, bufB);
-    k_y_pass<R, false><<<gy(3), 256, smem_y, stream>>>(g, tw, bufB, bufA, KCY);
-    k_x_force_to_zeta<R><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc, KCX);
+    k_y_pass<R, false, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufB, bufA);
+    k_x_force_to_zeta<R, KCX><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc);
   }
 
   void launch_step(const double *noise, int euler, cudaEvent_t *ev = nullptr) override {
@@ -275,17 +274,17 @@ struct Box : BoxBase {
       if (ev) cudaEventRecord(ev[e++], stream);
     };
     mark();
-    k_x_zeta_to_u<R><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA, KCX);
+    k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
     mark();
-    k_y_pass<R, true><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB, KCY);
+    k_y_pass<R, true, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB);
     mark();
     k_z_products<R><<<gz(), 256, smem_zp, stream>>>(g, tw, bufB);
     mark();
-    k_y_pass<R, false><<<gy(5), 256, smem_y, stream>>>(g, tw, bufB, bufA, KCY);
+    k_y_pass<R, false, KCY><<<gy(5), 256, smem_y, stream>>>(g, tw, bufB, bufA);
     mark();
-    k_x_advect_update<R><<<gx(), 256, smem_xadv, stream>>>(g, tw, bufA, zeta, uk_dc, KCX);
+    k_x_advect_update<R, KCX><<<gx(), 256, smem_xadv, stream>>>(g, tw, bufA, zeta, uk_dc);
     mark();
-    k_y_pass<R, true><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB, KCY);
+    k_y_pass<R, true, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB);
     mark();
     k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, npts(), g.NZ);
     mark();
@@ -298,9 +297,9 @@ struct Box : BoxBase {
       mark();
       k_z_force<R><<<gz(), 256, smem_zf, stream>>>(g, tw, phiup, ustar, bufB);
       mark();
-      k_y_pass<R, false><<<gy(3), 256, smem_y, stream>>>(g, tw, bufB, bufA, KCY);
+      k_y_pass<R, false, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufB, bufA);
       mark();
-      k_x_force_to_zeta<R><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc, KCX);
+      k_x_force_to_zeta<R, KCX><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc);
       mark();
     }
   }

@@ -210,10 +210,14 @@ __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart 
   KSum acc[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) acc[i] = {0.0, 0.0};
+#pragma unroll 4
   for (int m = threadIdx.x; m < p.S; m += blockDim.x) {
     int rm[3];
     double r[3], dist;
     stencil_point(b, cells + 3 * m, xp, p, rm, r, dist);
+    const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
+    // issue the field loads before the profile exps so they overlap
+    const double ug[3] = {(double)__ldg(u + im), (double)__ldg(u + npts + im), (double)__ldg(u + 2 * npts + im)};
     const double ph = prof_phi(dist, p);
     double vr[3] = {0.0, 0.0, 0.0};
     if (p.rotation) {
@@ -221,11 +225,10 @@ __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart 
       vr[1] = wp[2] * r[0] - wp[0] * r[2];
       vr[2] = wp[0] * r[1] - wp[1] * r[0];
     }
-    const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
     double fp[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      fp[d] = ((vp[d] + vr[d]) - (double)u[d * npts + im]) * ph;
+      fp[d] = ((vp[d] + vr[d]) - ug[d]) * ph;
       acc[d].add(fp[d]);
     }
     acc[3].add(r[1] * fp[2] - r[2] * fp[1]);
@@ -317,6 +320,7 @@ __global__ void __launch_bounds__(256) k_particles_scatter(PPar p, const DPart *
   const double wp[3] = {a.omega[0], a.omega[1], a.omega[2]};
   const StencilBase b = stencil_base(xp, p);
   const size_t npts = (size_t)p.N[0] * p.N[1] * p.N[2];
+#pragma unroll 4
   for (int m = threadIdx.x; m < p.S; m += blockDim.x) {
     int rm[3];
     double r[3], dist;

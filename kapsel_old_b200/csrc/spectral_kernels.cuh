@@ -88,21 +88,28 @@ __device__ __forceinline__ void select_zeta(int KXi, int KYi, const Cx<R> w[3], 
 // ---------------------------------------------------------------------------
 // x pass, inverse: zeta -> u_k (Zeta_k2u_k) -> inverse x transform.
 // grid (KYc, ceil(TZ/KC)), out I1[3][NX][KYc][TZ].
-template <typename R>
+template <typename R, int KC>
 __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ zeta,
-                                                     const double *__restrict__ uk_dc, Cx<R> *__restrict__ out,
-                                                     int KC) {
+                                                     const double *__restrict__ uk_dc, Cx<R> *__restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int W = 3 * KC;
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
-  Cx<R> *U = twx + g.NX;  // [NX rows][3*KC]
+  Cx<R> *Zt = twx + g.NX;          // [2][KXc][KC] staged zeta tile
+  Cx<R> *U = Zt + 2 * g.KXc * KC;  // [NX rows][3*KC]
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
-  const int W = 3 * KC;
+  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
+  for (int it = threadIdx.x; it < 2 * g.KXc * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
+    if (col < ncol)
+      cp_async_cx(Zt + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TZ + kz0 + col);
+  }
   load_twiddles(twx, tw.x, g.NX);
+  cp_async_wait_all();
+  __syncthreads();
   const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
   const R ky = R(g.wave[1] * KYi);
-  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
   for (int it = threadIdx.x; it < g.NX * KC; it += blockDim.x) {
     const int col = it % KC, i = it / KC;
     const int row = bitrev(i, g.lx);
@@ -111,8 +118,7 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
     if (col < ncol && abs(KXi) < g.TX) {
       const int ix = KXi >= 0 ? KXi : KXi + g.KXc;
       const int kz = kz0 + col;
-      const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
-      const Cx<R> z0 = zeta[o], z1 = zeta[zplane + o];
+      const Cx<R> z0 = Zt[ix * KC + col], z1 = Zt[(g.KXc + ix) * KC + col];
       const R kx = R(g.wave[0] * KXi), kzr = R(g.wave[2] * kz);
       const R k2 = kx * kx + ky * ky + kzr * kzr;
       const R ik2 = k2 > R(0) ? R(1) / k2 : R(0);
@@ -128,9 +134,9 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
     U[row * W + 2 * KC + col] = u[2];
   }
   __syncthreads();
-  fft_inplace(U, g.lx, W, 1, W, twx, -1);
+  fft_inplace<R, W>(U, g.lx, W, 1, W, twx, -1);
   for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest % g.NX, c = rest / g.NX;
+    const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
     if (col < ncol)
       out[(((size_t)c * g.NX + x) * g.KYc + iy) * g.TZ + kz0 + col] = U[x * W + c * KC + col];
   }
@@ -140,38 +146,42 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
 // y pass.  inverse: in [c][NX][KYc][TZ] -> out [c][NX][NY][TZ]
 //          forward: in [c][NX][NY][TZ] -> out [c][NX][KYc][TZ] (|ky| < TY kept)
 // grid (NX, ncomp, ceil(TZ/KC)).
-template <typename R, bool INVERSE>
+template <typename R, bool INVERSE, int KC>
 __global__ void __launch_bounds__(256) k_y_pass(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
-                                                Cx<R> *__restrict__ out, int KC) {
+                                                Cx<R> *__restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<R> *twy = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *Y = twy + g.NY;  // [NY rows][KC]
   const int x = blockIdx.x, c = blockIdx.y;
   const int kz0 = blockIdx.z * KC;
   const int ncol = min(KC, g.TZ - kz0);
-  load_twiddles(twy, tw.y, g.NY);
   const int rows_in = INVERSE ? g.KYc : g.NY;
   const int rows_out = INVERSE ? g.NY : g.KYc;
   const Cx<R> *src = in + ((size_t)c * g.NX + x) * rows_in * g.TZ + kz0;
   Cx<R> *dst = out + ((size_t)c * g.NX + x) * rows_out * g.TZ + kz0;
   for (int it = threadIdx.x; it < g.NY * KC; it += blockDim.x) {
     const int col = it % KC, j = it / KC;
-    Cx<R> v = {R(0), R(0)};
+    Cx<R> *d = Y + bitrev(j, g.ly) * KC + col;
+    bool loaded = false;
     if (col < ncol) {
       if (INVERSE) {
         const int KYi = signed_k(j, g.NY);
         if (abs(KYi) < g.TY) {
           const int iy = KYi >= 0 ? KYi : KYi + g.KYc;
-          v = src[(size_t)iy * g.TZ + col];
+          cp_async_cx(d, src + (size_t)iy * g.TZ + col);
+          loaded = true;
         }
       } else {
-        v = src[(size_t)j * g.TZ + col];
+        cp_async_cx(d, src + (size_t)j * g.TZ + col);
+        loaded = true;
       }
     }
-    Y[bitrev(j, g.ly) * KC + col] = v;
+    if (!loaded) *d = {R(0), R(0)};
   }
+  load_twiddles(twy, tw.y, g.NY);
+  cp_async_wait_all();
   __syncthreads();
-  fft_inplace(Y, g.ly, KC, 1, KC, twy, INVERSE ? -1 : 1);
+  fft_inplace<R, KC>(Y, g.ly, KC, 1, KC, twy, INVERSE ? -1 : 1);
   for (int it = threadIdx.x; it < rows_out * KC; it += blockDim.x) {
     const int col = it % KC, r = it / KC;
     if (col >= ncol) continue;
@@ -222,22 +232,27 @@ __global__ void __launch_bounds__(256) k_z_products(Geo g, Twiddles<R> tw, Cx<R>
   Cx<R> *twz = twm + M;
   Cx<R> *V = twz + g.NZ;      // [ZROWS*3][P] velocity lines, seq = rr*3 + c
   Cx<R> *Q = V + ZROWS * 3 * P;  // [ZROWS*5][P] product lines, seq = rr*5 + c
-  load_twiddles(twm, tw.m, M);
-  load_twiddles(twz, tw.z, g.NZ);
-  __syncthreads();
+  Cx<R> *A = Q;  // staging of the 3 input rows [ZROWS*3][TZ], reused by Q later
   const size_t rows = (size_t)g.NX * g.NY;
   const size_t row0 = (size_t)blockIdx.x * ZROWS;
   const size_t cstr = rows * g.TZ;
+  for (int it = threadIdx.x; it < ZROWS * 3 * g.TZ; it += blockDim.x) {
+    const int k = it % g.TZ, rest = it / g.TZ, c = rest % 3, rr = rest / 3;
+    cp_async_cx(A + it, io + c * cstr + (row0 + rr) * g.TZ + k);
+  }
+  load_twiddles(twm, tw.m, M);
+  load_twiddles(twz, tw.z, g.NZ);
+  cp_async_wait_all();
+  __syncthreads();
   for (int it = threadIdx.x; it < ZROWS * 3 * M; it += blockDim.x) {
-    const int k = it % M, rest = it / M, c = rest % 3, rr = rest / 3;
-    const Cx<R> *row = io + c * cstr + (row0 + rr) * g.TZ;
-    V[(rr * 3 + c) * P + bitrev(k, g.lm)] = c2r_pre(row, k, M, g.TZ, twz);
+    const int k = it & (M - 1), q = it >> g.lm;  // q = rr*3 + c
+    V[q * P + bitrev(k, g.lm)] = c2r_pre(A + q * g.TZ, k, M, g.TZ, twz);
   }
   __syncthreads();
-  fft_inplace(V, g.lm, ZROWS * 3, P, 1, twm, -1);
+  fft_inplace<R, ZROWS * 3>(V, g.lm, ZROWS * 3, P, 1, twm, -1);
   const R sc = R(g.inv_n);
   for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
-    const int n = it % M, rr = it / M;
+    const int n = it & (M - 1), rr = it >> g.lm;
     const Cx<R> U1 = V[(rr * 3) * P + n], U2 = V[(rr * 3 + 1) * P + n], U3 = V[(rr * 3 + 2) * P + n];
     const R u1a = U1.x * sc, u1b = U1.y * sc, u2a = U2.x * sc, u2b = U2.y * sc, u3a = U3.x * sc,
             u3b = U3.y * sc;
@@ -250,7 +265,7 @@ __global__ void __launch_bounds__(256) k_z_products(Geo g, Twiddles<R> tw, Cx<R>
     q[4 * P] = {(u3a - u1a) * (u3a + u1a), (u3b - u1b) * (u3b + u1b)};
   }
   __syncthreads();
-  fft_inplace(Q, g.lm, ZROWS * 5, P, 1, twm, 1);
+  fft_inplace<R, ZROWS * 5>(Q, g.lm, ZROWS * 5, P, 1, twm, 1);
   for (int it = threadIdx.x; it < ZROWS * 5 * g.TZ; it += blockDim.x) {
     const int k = it % g.TZ, rest = it / g.TZ, c = rest % 5, rr = rest / 5;
     io[c * cstr + (row0 + rr) * g.TZ + k] = r2c_post(Q + (rr * 5 + c) * P, k, M, twz);
@@ -267,23 +282,26 @@ __global__ void __launch_bounds__(256) k_z_c2r(Geo g, Twiddles<R> tw, const Cx<R
   Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *twz = twm + M;
   Cx<R> *S = twz + g.NZ;  // [ZROWS][P]
-  load_twiddles(twm, tw.m, M);
-  load_twiddles(twz, tw.z, g.NZ);
-  __syncthreads();
+  Cx<R> *A = S + ZROWS * P;  // staged input rows [ZROWS][TZ]
   const int c = blockIdx.y;
   const size_t rows = (size_t)g.NX * g.NY;
   const size_t row0 = (size_t)blockIdx.x * ZROWS;
-  const Cx<R> *src = in + c * rows * g.TZ;
+  const Cx<R> *src = in + c * rows * g.TZ + row0 * g.TZ;
+  for (int it = threadIdx.x; it < ZROWS * g.TZ; it += blockDim.x) cp_async_cx(A + it, src + it);
+  load_twiddles(twm, tw.m, M);
+  load_twiddles(twz, tw.z, g.NZ);
+  cp_async_wait_all();
+  __syncthreads();
   for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
-    const int k = it % M, rr = it / M;
-    S[rr * P + bitrev(k, g.lm)] = c2r_pre(src + (row0 + rr) * g.TZ, k, M, g.TZ, twz);
+    const int k = it & (M - 1), rr = it >> g.lm;
+    S[rr * P + bitrev(k, g.lm)] = c2r_pre(A + rr * g.TZ, k, M, g.TZ, twz);
   }
   __syncthreads();
-  fft_inplace(S, g.lm, ZROWS, P, 1, twm, -1);
+  fft_inplace<R, ZROWS>(S, g.lm, ZROWS, P, 1, twm, -1);
   const R sc = R(g.inv_n);
   R *dst = out + c * out_cstride;
   for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
-    const int n = it % M, rr = it / M;
+    const int n = it & (M - 1), rr = it >> g.lm;
     const Cx<R> v = S[rr * P + n];
     R *o = dst + (row0 + rr) * (size_t)out_pitch + 2 * n;
     o[0] = v.x * sc;
@@ -309,7 +327,7 @@ __global__ void __launch_bounds__(256) k_z_force(Geo g, Twiddles<R> tw, R *__res
   const size_t npts = (size_t)g.NX * g.NY * g.NZ;
   const size_t row0 = (size_t)blockIdx.x * ZROWS;
   for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
-    const int n = it % M, rr = it / M;
+    const int n = it & (M - 1), rr = it >> g.lm;
     const size_t o = (row0 + rr) * g.NZ + 2 * n;
     R ph[2], up[3][2], us[3][2];
 #pragma unroll
@@ -344,7 +362,7 @@ __global__ void __launch_bounds__(256) k_z_force(Geo g, Twiddles<R> tw, R *__res
     for (int d = 0; d < 3; ++d) S[(rr * 3 + d) * P + dst] = {f[d][0], f[d][1]};
   }
   __syncthreads();
-  fft_inplace(S, g.lm, ZROWS * 3, P, 1, twm, 1);
+  fft_inplace<R, ZROWS * 3>(S, g.lm, ZROWS * 3, P, 1, twm, 1);
   const size_t rows = (size_t)g.NX * g.NY;
   for (int it = threadIdx.x; it < ZROWS * 3 * g.TZ; it += blockDim.x) {
     const int k = it % g.TZ, rest = it / g.TZ, d = rest % 3, rr = rest / 3;
@@ -387,20 +405,33 @@ __global__ void __launch_bounds__(256) k_z_r2c_full(Geo g, Twiddles<R> tw, const
 //   zeta and the inverse x transform of u*.
 // In place on buf: reads [5][NX][KYc][TZ], writes [3][NX][KYc][TZ].
 // grid (KYc, ceil(TZ/KC)).
-template <typename R>
+template <typename R, int KC>
 __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ buf,
-                                                         Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc,
-                                                         int KC) {
+                                                         Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int W5 = 5 * KC, W3 = 3 * KC;
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
-  Cx<R> *Zs = twx + g.NX;          // [KXc][2*KC] updated zeta
-  Cx<R> *Pb = Zs + g.KXc * 2 * KC;  // [NX][5*KC], later [NX][3*KC]
+  Cx<R> *Zs = twx + g.NX;               // [2][KXc][KC] zeta tile (updated in place)
+  Cx<R> *Pb = Zs + 2 * g.KXc * KC;       // [NX][5*KC], later [NX][3*KC]
   __shared__ double ukd[3];
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
   const size_t cstr = (size_t)g.NX * g.KYc * g.TZ;
-  const int W5 = 5 * KC, W3 = 3 * KC;
+  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
+  // stage the five product spectra (bit-reversed rows) and the zeta tile
+  for (int it = threadIdx.x; it < 5 * g.NX * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
+    Cx<R> *d = Pb + bitrev(x, g.lx) * W5 + c * KC + col;
+    if (col < ncol)
+      cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col);
+    else
+      *d = {R(0), R(0)};
+  }
+  for (int it = threadIdx.x; it < 2 * g.KXc * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
+    if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TZ + kz0 + col);
+  }
   load_twiddles(twx, tw.x, g.NX);
   const bool has_k0 = (iy == 0 && blockIdx.y == 0);
   if (threadIdx.x < 3) {
@@ -411,17 +442,11 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
     }
     ukd[threadIdx.x] = v;
   }
-  for (int it = threadIdx.x; it < 5 * g.NX * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest % g.NX, c = rest / g.NX;
-    Cx<R> v = {R(0), R(0)};
-    if (col < ncol) v = buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col];
-    Pb[bitrev(x, g.lx) * W5 + c * KC + col] = v;
-  }
+  cp_async_wait_all();
   __syncthreads();
-  fft_inplace(Pb, g.lx, W5, 1, W5, twx, 1);
+  fft_inplace<R, W5>(Pb, g.lx, W5, 1, W5, twx, 1);
   const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
   const R ky = R(g.wave[1] * KYi);
-  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
   for (int it = threadIdx.x; it < g.KXc * KC; it += blockDim.x) {
     const int col = it % KC, ix = it / KC;
     if (col >= ncol) continue;
@@ -448,14 +473,14 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
     const double arg = -g.nu * g.dt * (double)K2;
     const R dmy = R(g.fp64_exp ? exp(arg) - 1.0 : expm1(arg));
     const R c1 = R(1.0 / g.nu) * IK2;
-    const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
-    Cx<R> z0 = zeta[o], z1 = zeta[zplane + o];
+    Cx<R> z0 = Zs[ix * KC + col], z1 = Zs[(g.KXc + ix) * KC + col];
     z0 = {z0.x + dmy * (z0.x - c1 * f0.x), z0.y + dmy * (z0.y - c1 * f0.y)};
     z1 = {z1.x + dmy * (z1.x - c1 * f1.x), z1.y + dmy * (z1.y - c1 * f1.y)};
+    const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
     zeta[o] = z0;
     zeta[zplane + o] = z1;
-    Zs[ix * 2 * KC + col] = z0;
-    Zs[ix * 2 * KC + KC + col] = z1;
+    Zs[ix * KC + col] = z0;
+    Zs[(g.KXc + ix) * KC + col] = z1;
   }
   __syncthreads();
   // u*_k = Zeta_k2u_k(zeta', uk_dc) on all NX rows (zero outside |kx| < TX)
@@ -469,7 +494,7 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
       const R kx = R(g.wave[0] * KXi), kzr = R(g.wave[2] * kz);
       const R k2 = kx * kx + ky * ky + kzr * kzr;
       const R ik2 = k2 > R(0) ? R(1) / k2 : R(0);
-      zeta_to_u(KXi, KYi, kx, ky, kzr, ik2, Zs[ix * 2 * KC + col], Zs[ix * 2 * KC + KC + col], u);
+      zeta_to_u(KXi, KYi, kx, ky, kzr, ik2, Zs[ix * KC + col], Zs[(g.KXc + ix) * KC + col], u);
       if (KXi == 0 && KYi == 0 && kz == 0) {
         u[0] = {R(ukd[0]), R(0)};
         u[1] = {R(ukd[1]), R(0)};
@@ -482,9 +507,9 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
     Pb[row * W3 + 2 * KC + col] = u[2];
   }
   __syncthreads();
-  fft_inplace(Pb, g.lx, W3, 1, W3, twx, -1);
+  fft_inplace<R, W3>(Pb, g.lx, W3, 1, W3, twx, -1);
   for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest % g.NX, c = rest / g.NX;
+    const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
     if (col < ncol) buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col] = Pb[x * W3 + c * KC + col];
   }
 }
@@ -497,30 +522,37 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
 // The velocity before the force is Zeta_k2u of the truncated zeta, so its
 // own U2zeta_k is that zeta again (linearity; parity up to roundoff).
 // in buf [3][NX][KYc][TZ].  grid (KYc, ceil(TZ/KC)).
-template <typename R>
+template <typename R, int KC>
 __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ buf,
-                                                         Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc,
-                                                         int KC) {
+                                                         Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int W3 = 3 * KC;
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
-  Cx<R> *Pb = twx + g.NX;  // [NX][3*KC]
+  Cx<R> *Zs = twx + g.NX;          // [2][KXc][KC]
+  Cx<R> *Pb = Zs + 2 * g.KXc * KC;  // [NX][3*KC]
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
   const size_t cstr = (size_t)g.NX * g.KYc * g.TZ;
-  const int W3 = 3 * KC;
-  load_twiddles(twx, tw.x, g.NX);
+  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
   for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest % g.NX, c = rest / g.NX;
-    Cx<R> v = {R(0), R(0)};
-    if (col < ncol) v = buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col];
-    Pb[bitrev(x, g.lx) * W3 + c * KC + col] = v;
+    const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
+    Cx<R> *d = Pb + bitrev(x, g.lx) * W3 + c * KC + col;
+    if (col < ncol)
+      cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col);
+    else
+      *d = {R(0), R(0)};
   }
+  for (int it = threadIdx.x; it < 2 * g.KXc * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
+    if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TZ + kz0 + col);
+  }
+  load_twiddles(twx, tw.x, g.NX);
+  cp_async_wait_all();
   __syncthreads();
-  fft_inplace(Pb, g.lx, W3, 1, W3, twx, 1);
+  fft_inplace<R, W3>(Pb, g.lx, W3, 1, W3, twx, 1);
   const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
   const R ky = R(g.wave[1] * KYi);
-  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
   for (int it = threadIdx.x; it < g.KXc * KC; it += blockDim.x) {
     const int col = it % KC, ix = it / KC;
     if (col >= ncol) continue;
@@ -550,8 +582,8 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
     Cx<R> z0, z1;
     select_zeta(KXi, KYi, w, z0, z1);
     const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
-    zeta[o] = cadd(zeta[o], z0);
-    zeta[zplane + o] = cadd(zeta[zplane + o], z1);
+    zeta[o] = cadd(Zs[ix * KC + col], z0);
+    zeta[zplane + o] = cadd(Zs[(g.KXc + ix) * KC + col], z1);
   }
 }
 
