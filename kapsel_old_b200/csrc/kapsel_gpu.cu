@@ -138,6 +138,8 @@ struct BoxBase {
   int *cells = nullptr;
   double *uk_dc = nullptr;
   int *status = nullptr;
+  double *partial = nullptr;  // [Np][PCL][18] partial force sums
+  int *arrivals = nullptr;    // [Np] blocks done per particle (0 between launches)
   double *noise_dev[2] = {nullptr, nullptr};
   double *noise_host[2] = {nullptr, nullptr};
   cudaEvent_t noise_ev[2] = {nullptr, nullptr};
@@ -187,9 +189,9 @@ struct Box : BoxBase {
   R *phiup = nullptr;     // [4][NX][NY][NZ]
   Cx<R> *twbuf = nullptr;
   Twiddles<R> tw;
-  static constexpr int KCX = sizeof(R) == 4 ? 16 : 8;  // x-pass kz tile
-  static constexpr int KCY = 16;                        // y-pass kz tile
-  size_t smem_xu = 0, smem_xadv = 0, smem_xf = 0, smem_y = 0, smem_zp = 0, smem_zc = 0, smem_zf = 0;
+  static constexpr int KCX = sizeof(R) == 4 ? 8 : 4;    // x-pass kz tile
+  static constexpr int KCY = sizeof(R) == 4 ? 32 : 16;  // y-pass kz tile
+  size_t smem_xu = 0, smem_xadv = 0, smem_xf = 0, smem_y = 0, smem_zp = 0, smem_zc = 0, smem_zf = 0, smem_zr = 0;
 
   size_t npts() const { return (size_t)g.NX * g.NY * g.NZ; }
 
@@ -224,13 +226,16 @@ struct Box : BoxBase {
     tw.z = twbuf + off[3];
     const size_t C = sizeof(Cx<R>);
     const int P = g.M + 1;
-    smem_xu = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)g.NX * 3 * KCX);
-    smem_xadv = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)g.NX * 5 * KCX);
-    smem_xf = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)g.NX * 3 * KCX);
-    smem_y = C * (g.NY + (size_t)g.NY * KCY);
-    smem_zp = C * (g.M + g.NZ + (size_t)ZROWS * 8 * P);
-    smem_zc = C * (g.M + g.NZ + (size_t)ZROWS * P + (size_t)ZROWS * g.TZ);
-    smem_zf = C * (g.M + g.NZ + (size_t)ZROWS * 3 * P);
+    smem_xu = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)2 * g.NX * 3 * KCX);
+    smem_xadv = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)2 * g.NX * 5 * KCX);
+    smem_xf = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)2 * g.NX * 3 * KCX);
+    smem_y = C * (g.NY + (size_t)2 * g.NY * KCY);
+    smem_zp = C * (g.M + g.NZ + (size_t)g.M * (ZROWS * 3 + 1) + (size_t)g.M * (ZROWS * 5 + 1) +
+                   std::max((size_t)g.M * ZROWS * 5, (size_t)ZROWS * 5 * (g.TZ + 1)));
+    smem_zc = C * (g.M + g.NZ + (size_t)g.M * (ZROWS + 1) + std::max((size_t)g.M * ZROWS, (size_t)ZROWS * (g.TZ + 1)));
+    smem_zf = C * (g.M + g.NZ + (size_t)g.M * (ZROWS * 3 + 1) +
+                   std::max((size_t)g.M * ZROWS * 3, (size_t)ZROWS * 3 * (g.TZ + 1)));
+    smem_zr = C * (g.M + g.NZ + (size_t)g.M * (2 * ZROWS + 1) + (size_t)ZROWS * P);
     const size_t mx = 227 * 1024;
     if (smem_xadv > mx || smem_xu > mx || smem_y > mx || smem_zp > mx) return KAPSEL_ERANGE;
     KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
@@ -240,13 +245,13 @@ struct Box : BoxBase {
     KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
     KCHECK(cudaFuncSetAttribute(k_z_products<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zp));
     KCHECK(cudaFuncSetAttribute(k_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
-    KCHECK(cudaFuncSetAttribute(k_z_r2c_full<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
+    KCHECK(cudaFuncSetAttribute(k_z_r2c_full<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zr));
     KCHECK(cudaFuncSetAttribute(k_z_force<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zf));
     const int nmax = std::max(g.NX, g.NY);
     const int smem_col = (int)(C * ((size_t)nmax + (size_t)nmax * 16));
     KCHECK(cudaFuncSetAttribute(k_col_pass<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_col));
     KCHECK(cudaFuncSetAttribute(k_col_pass<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_col));
-    KCHECK(cudaFuncSetAttribute(k_z_c2r_full<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
+    KCHECK(cudaFuncSetAttribute(k_z_c2r_full<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zr));
     return 0;
   }
 
@@ -291,9 +296,10 @@ struct Box : BoxBase {
     if (Np > 0) {
       k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
       mark();
-      k_particles_hydro_velocity<R><<<Np, 256, 0, stream>>>(pp, parts, ustar, cells, noise, euler, status);
+      k_particles_hydro_velocity<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, ustar, cells, noise, euler, status,
+                                                                    partial, arrivals);
       mark();
-      k_particles_scatter<R><<<Np, 256, 0, stream>>>(pp, parts, cells, phiup);
+      k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup);
       mark();
       k_z_force<R><<<gz(), 256, smem_zf, stream>>>(g, tw, phiup, ustar, bufB);
       mark();
@@ -312,7 +318,7 @@ struct Box : BoxBase {
     cudaMemsetAsync(ustar, 0, sizeof(R) * 3 * npts(), stream);
     cudaMemsetAsync(uk_dc, 0, sizeof(double) * 3, stream);
     if (Np > 0) {
-      k_particles_scatter<R><<<Np, 256, 0, stream>>>(pp, parts, cells, phiup);
+      k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup);
       launch_force_to_zeta();
     }
     cudaMemsetAsync(uk_dc, 0, sizeof(double) * 3, stream);
@@ -475,8 +481,7 @@ struct FullFFT {
   static int forward(Box<R> &b, const R *in, Cx<R> *out) {
     const Geo &g = b.g;
     const int M1 = g.M + 1;
-    const size_t sm_c = sizeof(Cx<R>) * (g.M + g.NZ + (size_t)ZROWS * (g.M + 1));
-    k_z_r2c_full<R><<<b.gz(), 256, sm_c, b.stream>>>(g, b.tw, in, g.NZ, out);
+    k_z_r2c_full<R><<<b.gz(), 256, b.smem_zr, b.stream>>>(g, b.tw, in, g.NZ, out);
     // y: lines (x, kz): line stride... lines indexed l = x*M1 + kz -> base x*NY*M1 + kz
     col_pass(b, out, g.NY, g.ly, b.tw.y, false, 1);
     col_pass(b, out, g.NX, g.lx, b.tw.x, false, 0);
@@ -488,8 +493,7 @@ struct FullFFT {
     const Geo &g = b.g;
     col_pass(b, in, g.NX, g.lx, b.tw.x, true, 0);
     col_pass(b, in, g.NY, g.ly, b.tw.y, true, 1);
-    const size_t sm_c = sizeof(Cx<R>) * (g.M + g.NZ + (size_t)ZROWS * (g.M + 1));
-    k_z_c2r_full<R><<<b.gz(), 256, sm_c, b.stream>>>(g, b.tw, in, out, g.inv_n);
+    k_z_c2r_full<R><<<b.gz(), 256, b.smem_zr, b.stream>>>(g, b.tw, in, out, g.inv_n);
     KCHECK(cudaGetLastError());
     return 0;
   }
@@ -637,7 +641,7 @@ int Box<R>::phi_up_host(double *phi, double *up0, double *up1, double *up2) {
   R *d = nullptr;
   KCHECK(cudaMalloc(&d, sizeof(R) * 4 * npt));
   KCHECK(cudaMemsetAsync(d, 0, sizeof(R) * 4 * npt, stream));
-  if (Np > 0) k_particles_scatter<R><<<Np, 256, 0, stream>>>(pp, parts, cells, d);
+  if (Np > 0) k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, d);
   k_clamp_phi<R><<<592, 256, 0, stream>>>(npt, d);
   KCHECK(cudaGetLastError());
   std::vector<R> h(4 * npt);
@@ -664,7 +668,7 @@ __global__ void k_gather_only(PPar p, const DPart *__restrict__ parts, const R *
     int rm[3];
     double r[3], dist;
     stencil_point(b, cells + 3 * m, xp, p, rm, r, dist);
-    const double ph = prof_phi(dist, p);
+    const double ph = (double)prof_phi<R>(dist, p);
     double vr[3] = {0.0, 0.0, 0.0};
     if (p.rotation) {
       vr[0] = a.omega[1] * r[2] - a.omega[2] * r[1];
@@ -718,6 +722,18 @@ int Box<R>::fhydro_host(const double *u0, const double *u1, const double *u2, do
 }
 
 }  // namespace
+
+// Holds its stream for `ns` nanoseconds of device time (bounded by the
+// global timer; no dependence on other work), used only by the profiler.
+__global__ void k_time_gate(unsigned long long ns) {
+  unsigned long long t0, t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (int i = 0; i < 1000000; ++i) {
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 >= ns) break;
+    __nanosleep(1000);
+  }
+}
 
 // ---------------------------------------------------------------------------
 struct kapsel_ctx {
@@ -810,7 +826,10 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   pp.N[0] = g.NX;
   pp.N[1] = g.NY;
   pp.N[2] = g.NZ;
-  for (int d = 0; d < 3; ++d) pp.L[d] = L[d];
+  for (int d = 0; d < 3; ++d) {
+    pp.L[d] = L[d];
+    pp.invL[d] = 1.0 / L[d];
+  }
   pp.DX = p->dx;
   pp.RADIUS = p->a * p->dx;
   const double XI = p->a_xi * p->dx;
@@ -865,6 +884,9 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   cudaMemset(b->uk_dc, 0, sizeof(double) * 3);
   if (cudaMalloc(&b->status, sizeof(int)) != cudaSuccess) return KAPSEL_ENOMEM;
   cudaMemset(b->status, 0, sizeof(int));
+  if (cudaMalloc(&b->partial, sizeof(double) * 18 * PCL * np1) != cudaSuccess) return KAPSEL_ENOMEM;
+  if (cudaMalloc(&b->arrivals, sizeof(int) * np1) != cudaSuccess) return KAPSEL_ENOMEM;
+  cudaMemset(b->arrivals, 0, sizeof(int) * np1);
   for (int s = 0; s < 2; ++s) {
     if (cudaMalloc(&b->noise_dev[s], sizeof(double) * 6 * np1) != cudaSuccess) return KAPSEL_ENOMEM;
     if (cudaMallocHost(&b->noise_host[s], sizeof(double) * 6 * np1) != cudaSuccess) return KAPSEL_ENOMEM;
@@ -895,6 +917,8 @@ int kapsel_gpu_destroy(kapsel_ctx *ctx) {
     cudaFree(b->cells);
     cudaFree(b->uk_dc);
     cudaFree(b->status);
+    cudaFree(b->partial);
+    cudaFree(b->arrivals);
     cudaStreamDestroy(b->stream);
   }
   delete ctx;
@@ -1141,11 +1165,11 @@ int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr) {
   p.thermostat = 0;  // no kick
   // u is never read with S == 0
   if (b->prm.precision == KAPSEL_FP64)
-    k_particles_hydro_velocity<double><<<b->Np, 256, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
-                                                                     b->status);
+    k_particles_hydro_velocity<double><<<b->Np * PCL, 256, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
+                                                                           b->status, b->partial, b->arrivals);
   else
-    k_particles_hydro_velocity<float><<<b->Np, 256, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
-                                                                    b->status);
+    k_particles_hydro_velocity<float><<<b->Np * PCL, 256, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
+                                                                          b->status, b->partial, b->arrivals);
   std::vector<DPart> h(b->Np);
   cudaMemcpyAsync(h.data(), scratch, sizeof(DPart) * b->Np, cudaMemcpyDeviceToHost, b->stream);
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
@@ -1199,6 +1223,10 @@ const char *kapsel_gpu_kernel_name(int i) {
 }
 
 int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms) {
+  // A short timed gate kernel holds the stream while the host enqueues the
+  // step with an event between consecutive launches, so on the device the
+  // launches run back to back and each event delta is one kernel's duration
+  // (not a host launch gap).
   if (!ctx || !ms) return KAPSEL_EINVAL;
   BoxBase *b = ctx->box.get();
   if (!b->initialised) return KAPSEL_ESTATE;
@@ -1208,13 +1236,15 @@ int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms) {
   cudaEvent_t ev[KAPSEL_N_STEP_KERNELS + 1];
   for (int i = 0; i <= KAPSEL_N_STEP_KERNELS; ++i)
     if (cudaEventCreate(&ev[i]) != cudaSuccess) return KAPSEL_ECUDA;
+  k_time_gate<<<1, 32, 0, b->stream>>>(2000000ull);  // 2 ms
   b->launch_step(b->noise_dev[slot], b->ts == 0 ? 1 : 0, ev);
   b->ts += 1;
   b->time += b->prm.dt;
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
   const int nk = b->Np > 0 ? KAPSEL_N_STEP_KERNELS : 7;
   for (int i = 0; i < KAPSEL_N_STEP_KERNELS; ++i) ms[i] = 0.f;
-  for (int i = 0; i < nk; ++i) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+  for (int i = 0; i < nk; ++i)
+    if (cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]) != cudaSuccess) return KAPSEL_ECUDA;
   for (int i = 0; i <= KAPSEL_N_STEP_KERNELS; ++i) cudaEventDestroy(ev[i]);
   return check_status(b);
 }
@@ -1320,7 +1350,7 @@ extern "C" int kapsel_gpu_solenoidal_u_noalloc(const int *np_xyz, double dx, con
   tw.z = twb + g.NX + g.NY + g.M;
   const int M1 = g.M + 1;
   const int gz = (g.NX * g.NY) / ZROWS;
-  const size_t sm_z = sizeof(Cx<double>) * (g.M + g.NZ + (size_t)ZROWS * (g.M + 1));
+  const size_t sm_z = sizeof(Cx<double>) * (g.M + g.NZ + (size_t)2 * g.M * ZROWS + (size_t)ZROWS * (g.M + 1));
   auto col = [&](Cx<double> *data, bool inv, int axis) {
     const int n = axis == 0 ? g.NX : g.NY;
     const int logn = axis == 0 ? g.lx : g.ly;

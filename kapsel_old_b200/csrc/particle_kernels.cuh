@@ -18,7 +18,7 @@ struct DPart {
 struct PPar {
   int Np, S;           // particles, Sekibun points per particle
   int N[3];
-  double L[3];
+  double L[3], invL[3];
   double DX, RADIUS, HXI;
   double dt;
   double IMASS, IMOI;
@@ -40,11 +40,22 @@ __device__ __forceinline__ double nint_d(double a) {
   return a >= 0.0 ? (double)(int)(a + 0.5) : (double)(int)(a - 0.5);
 }
 
-// H and Phi (profile.h:29-49)
-__device__ __forceinline__ double prof_H(double x, double dx) { return x > 0.0 ? exp(-((dx / x) * (dx / x))) : 0.0; }
-__device__ __forceinline__ double prof_phi(double x, const PPar &p) {
-  const double h = prof_H(p.RADIUS + p.HXI - x, p.DX);
-  return h / (h + prof_H(x - p.RADIUS + p.HXI, p.DX));
+// H and Phi (profile.h:29-49), evaluated in the field precision R: double
+// for the FP64 path, float (fast exp) for the mixed path, whose profile
+// stencils are single precision.
+template <typename R>
+__device__ __forceinline__ R prof_H(R x, R dx) {
+  if (sizeof(R) == 8) return x > R(0) ? R(exp(-((dx / x) * (dx / x)))) : R(0);
+  const float q = __fdividef((float)dx, (float)x);
+  return x > R(0) ? R(__expf(-q * q)) : R(0);
+}
+template <typename R>
+__device__ __forceinline__ R prof_phi(double x, const PPar &p) {
+  const R xr = R(x);
+  const R h = prof_H<R>(R(p.RADIUS + p.HXI) - xr, R(p.DX));
+  // (x - radius) + HXI as in profile.h:47 for the double path
+  const R h2 = prof_H<R>(sizeof(R) == 8 ? (xr - R(p.RADIUS)) + R(p.HXI) : xr - R(p.RADIUS - p.HXI), R(p.DX));
+  return sizeof(R) == 8 ? h / (h + h2) : R(__fdividef((float)h, (float)(h + h2)));
 }
 
 // Stencil geometry shared by the gather and the scatter: Particle_cell
@@ -73,10 +84,10 @@ __device__ __forceinline__ void stencil_point(const StencilBase &b, const int *c
   double s = 0.0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    rm[d] = (b.xi[d] + cell[d] + p.N[d]) % p.N[d];
+    rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);  // N is a power of two
     r[d] = (double)cell[d] * p.DX - b.res[d];
     double dd = xp[d] - (double)rm[d] * p.DX;
-    dd -= nint_d(dd / p.L[d]) * p.L[d];
+    dd -= nint_d(dd * p.invL[d]) * p.L[d];
     s += dd * dd;
   }
   dist = sqrt(s);
@@ -152,9 +163,10 @@ __global__ void k_particles_position(PPar p, DPart *__restrict__ parts, int eule
   }
 }
 
-// Block reduction of NV compensated sums; result valid in thread 0.
+// Block reduction of NV compensated sums; result valid in thread 0.  Warps
+// reduce with shuffles, then thread i < NV adds value i over the warps.
 template <int NV>
-__device__ void block_reduce(KSum (&v)[NV], double *sh /* [NV][blockDim/32] x2 */) {
+__device__ void block_reduce(KSum (&v)[NV], double *sh /* [2*NV][32] */) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
@@ -173,17 +185,23 @@ __device__ void block_reduce(KSum (&v)[NV], double *sh /* [NV][blockDim/32] x2 *
     }
   }
   __syncthreads();
+  if (threadIdx.x < NV) {
+    const int i = threadIdx.x;
+    KSum k{0.0, 0.0};
+    double cs = 0.0;
+    for (int w = 0; w < nw; ++w) {
+      k.add(sh[(2 * i) * 32 + w]);
+      cs += sh[(2 * i + 1) * 32 + w];
+    }
+    sh[(2 * i) * 32] = k.s;
+    sh[(2 * i + 1) * 32] = k.c + cs;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
-      KSum k{0.0, 0.0};
-      double cs = 0.0;
-      for (int w = 0; w < nw; ++w) {
-        k.add(sh[(2 * i) * 32 + w]);
-        cs += sh[(2 * i + 1) * 32 + w];
-      }
-      v[i].s = k.s;
-      v[i].c = k.c + cs;
+      v[i].s = sh[(2 * i) * 32];
+      v[i].c = sh[(2 * i + 1) * 32];
     }
   }
 }
@@ -193,14 +211,27 @@ __device__ void block_reduce(KSum (&v)[NV], double *sh /* [NV][blockDim/32] x2 *
 // MD_solver_velocity_Euler / _AB2_hydro with reset_Forces
 // (particle_solver.cxx:106-147, 247-289, 11-34) and, when kBT > 0, the
 // thermostat kick of Add_random_force_thermostat (fluct.cxx:10-36) from a
-// precomputed table of its normals.  One block per particle.
+// precomputed table of its normals.
+// PCL blocks per particle: each block sums a quarter of the Sekibun points
+// and of the LJ partners and stores its partial sums; the block that
+// finishes last (a per-particle arrival counter) adds the PCL partials in a
+// fixed order -- the result does not depend on block scheduling -- and
+// updates the particle.
+constexpr int PCL = 4;
+
 template <typename R>
 __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart *__restrict__ parts,
                                                                   const R *__restrict__ u, const int *__restrict__ cells,
                                                                   const double *__restrict__ noise, int euler,
-                                                                  int *__restrict__ status) {
+                                                                  int *__restrict__ status,
+                                                                  double *__restrict__ partial,
+                                                                  int *__restrict__ arrivals) {
   __shared__ double sh[2 * 9 * 32];
-  const int n = blockIdx.x;
+  __shared__ int last;
+  const int n = blockIdx.x / PCL;
+  const int rank = blockIdx.x % PCL;
+  const int stride = PCL * blockDim.x;
+  const int first = rank * blockDim.x + threadIdx.x;
   DPart &a = parts[n];
   const double xp[3] = {a.x[0], a.x[1], a.x[2]};
   const double vp[3] = {a.v[0], a.v[1], a.v[2]};
@@ -210,15 +241,14 @@ __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart 
   KSum acc[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) acc[i] = {0.0, 0.0};
-#pragma unroll 4
-  for (int m = threadIdx.x; m < p.S; m += blockDim.x) {
+  for (int m = first; m < p.S; m += stride) {
     int rm[3];
     double r[3], dist;
     stencil_point(b, cells + 3 * m, xp, p, rm, r, dist);
     const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
     // issue the field loads before the profile exps so they overlap
     const double ug[3] = {(double)__ldg(u + im), (double)__ldg(u + npts + im), (double)__ldg(u + 2 * npts + im)};
-    const double ph = prof_phi(dist, p);
+    const double ph = (double)prof_phi<R>(dist, p);
     double vr[3] = {0.0, 0.0, 0.0};
     if (p.rotation) {
       vr[0] = wp[1] * r[2] - wp[2] * r[1];
@@ -238,7 +268,7 @@ __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart 
   if (p.lj_on) {
     int mc[3];
     for (int d = 0; d < 3; ++d) mc[d] = (int)(xp[d] / p.lc_r);
-    for (int j = threadIdx.x; j < p.Np; j += blockDim.x) {
+    for (int j = first; j < p.Np; j += stride) {
       if (j == n) continue;
       const DPart &o = parts[j];
       int mult = 1;
@@ -255,7 +285,7 @@ __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart 
         }
         mult *= cnt;
         x12[d] = o.x[d] - xp[d];
-        x12[d] -= nint_d(x12[d] / p.L[d]) * p.L[d];
+        x12[d] -= nint_d(x12[d] * p.invL[d]) * p.L[d];
         r2 += x12[d] * x12[d];
       }
       const double rij = sqrt(r2);
@@ -271,12 +301,33 @@ __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart 
     }
   }
   block_reduce<9>(acc, sh);
-  if (threadIdx.x != 0) return;
+  if (threadIdx.x == 0) {
+    double *pp = partial + ((size_t)n * PCL + rank) * 18;
+    for (int i = 0; i < 9; ++i) {
+      pp[2 * i] = acc[i].s;
+      pp[2 * i + 1] = acc[i].c;
+    }
+    __threadfence();
+    last = (atomicAdd(arrivals + n, 1) == PCL - 1);
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  arrivals[n] = 0;
+  KSum tot[9];
+  for (int i = 0; i < 9; ++i) tot[i] = {0.0, 0.0};
+  for (int q = 0; q < PCL; ++q) {
+    const volatile double *pq = partial + ((size_t)n * PCL + q) * 18;
+    for (int i = 0; i < 9; ++i) {
+      tot[i].add(pq[2 * i]);
+      tot[i].c += pq[2 * i + 1];
+    }
+  }
   double fh[3], th[3], fr[3];
   for (int d = 0; d < 3; ++d) {
-    fh[d] = p.fh_coef * (acc[d].s + acc[d].c);
-    th[d] = p.rotation ? p.fh_coef * (acc[3 + d].s + acc[3 + d].c) : 0.0;
-    fr[d] = acc[6 + d].s + acc[6 + d].c;
+    fh[d] = p.fh_coef * (tot[d].s + tot[d].c);
+    th[d] = p.rotation ? p.fh_coef * (tot[3 + d].s + tot[3 + d].c) : 0.0;
+    fr[d] = tot[6 + d].s + tot[6 + d].c;
   }
   fr[p.gdir] -= p.grav;
   const double hdt = 0.5 * p.dt;
@@ -309,23 +360,25 @@ __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart 
 
 // Make_phi_u_primitive scatter (make_phi.cxx:221-277): phi += phi_i and
 // up += (v + omega x r) phi_i over the Sekibun points of each particle.
-// The phi > 1 clamp is applied by the consumer.  One block per particle.
+// The phi > 1 clamp is applied by the consumer.  PCL blocks per particle.
 template <typename R>
 __global__ void __launch_bounds__(256) k_particles_scatter(PPar p, const DPart *__restrict__ parts,
                                                            const int *__restrict__ cells, R *__restrict__ phiup) {
-  const int n = blockIdx.x;
+  const int n = blockIdx.x / PCL;
+  const int stride = PCL * blockDim.x;
+  const int first = (blockIdx.x % PCL) * blockDim.x + threadIdx.x;
   const DPart &a = parts[n];
   const double xp[3] = {a.x[0], a.x[1], a.x[2]};
   const double vp[3] = {a.v[0], a.v[1], a.v[2]};
   const double wp[3] = {a.omega[0], a.omega[1], a.omega[2]};
   const StencilBase b = stencil_base(xp, p);
   const size_t npts = (size_t)p.N[0] * p.N[1] * p.N[2];
-#pragma unroll 4
-  for (int m = threadIdx.x; m < p.S; m += blockDim.x) {
+#pragma unroll 2
+  for (int m = first; m < p.S; m += stride) {
     int rm[3];
     double r[3], dist;
     stencil_point(b, cells + 3 * m, xp, p, rm, r, dist);
-    const double ph = prof_phi(dist, p);
+    const double ph = (double)prof_phi<R>(dist, p);
     double vr[3] = {0.0, 0.0, 0.0};
     if (p.rotation) {
       vr[0] = wp[1] * r[2] - wp[2] * r[1];

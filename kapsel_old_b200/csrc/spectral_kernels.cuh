@@ -15,6 +15,7 @@
 #pragma once
 
 #include "fft_device.cuh"
+#include "rfft_device.cuh"
 
 namespace kapsel {
 
@@ -96,6 +97,7 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *Zt = twx + g.NX;          // [2][KXc][KC] staged zeta tile
   Cx<R> *U = Zt + 2 * g.KXc * KC;  // [NX rows][3*KC]
+  Cx<R> *scr = U + g.NX * W;       // FFT scratch, NX*3*KC
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
@@ -112,7 +114,6 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
   const R ky = R(g.wave[1] * KYi);
   for (int it = threadIdx.x; it < g.NX * KC; it += blockDim.x) {
     const int col = it % KC, i = it / KC;
-    const int row = bitrev(i, g.lx);
     Cx<R> u[3] = {{R(0), R(0)}, {R(0), R(0)}, {R(0), R(0)}};
     const int KXi = signed_k(i, g.NX);
     if (col < ncol && abs(KXi) < g.TX) {
@@ -129,12 +130,12 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
         u[2] = {R(uk_dc[2]), R(0)};
       }
     }
-    U[row * W + col] = u[0];
-    U[row * W + KC + col] = u[1];
-    U[row * W + 2 * KC + col] = u[2];
+    U[i * W + col] = u[0];
+    U[i * W + KC + col] = u[1];
+    U[i * W + 2 * KC + col] = u[2];
   }
   __syncthreads();
-  fft_inplace<R, W>(U, g.lx, W, 1, W, twx, -1);
+  fft2_smem<R, -1, W>(U, scr, g.lx, 1, W, twx);
   for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
     if (col < ncol)
@@ -147,11 +148,12 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
 //          forward: in [c][NX][NY][TZ] -> out [c][NX][KYc][TZ] (|ky| < TY kept)
 // grid (NX, ncomp, ceil(TZ/KC)).
 template <typename R, bool INVERSE, int KC>
-__global__ void __launch_bounds__(256) k_y_pass(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
+__global__ void __launch_bounds__(256, 3) k_y_pass(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
                                                 Cx<R> *__restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<R> *twy = reinterpret_cast<Cx<R> *>(smem_raw);
-  Cx<R> *Y = twy + g.NY;  // [NY rows][KC]
+  Cx<R> *Y = twy + g.NY;      // [NY rows][KC]
+  Cx<R> *scr = Y + g.NY * KC;  // FFT scratch
   const int x = blockIdx.x, c = blockIdx.y;
   const int kz0 = blockIdx.z * KC;
   const int ncol = min(KC, g.TZ - kz0);
@@ -159,35 +161,31 @@ __global__ void __launch_bounds__(256) k_y_pass(Geo g, Twiddles<R> tw, const Cx<
   const int rows_out = INVERSE ? g.NY : g.KYc;
   const Cx<R> *src = in + ((size_t)c * g.NX + x) * rows_in * g.TZ + kz0;
   Cx<R> *dst = out + ((size_t)c * g.NX + x) * rows_out * g.TZ + kz0;
-  for (int it = threadIdx.x; it < g.NY * KC; it += blockDim.x) {
-    const int col = it % KC, j = it / KC;
-    Cx<R> *d = Y + bitrev(j, g.ly) * KC + col;
-    bool loaded = false;
-    if (col < ncol) {
-      if (INVERSE) {
-        const int KYi = signed_k(j, g.NY);
-        if (abs(KYi) < g.TY) {
-          const int iy = KYi >= 0 ? KYi : KYi + g.KYc;
-          cp_async_cx(d, src + (size_t)iy * g.TZ + col);
-          loaded = true;
-        }
-      } else {
-        cp_async_cx(d, src + (size_t)j * g.TZ + col);
-        loaded = true;
-      }
+  // each thread keeps one column and walks rows (256/KC rows apart)
+  constexpr int RSTEP = 256 / KC;
+  const int col = threadIdx.x % KC, j0 = threadIdx.x / KC;
+  const bool colok = col < ncol;
+  for (int j = j0; j < g.NY; j += RSTEP) {
+    Cx<R> *d = Y + j * KC + col;
+    int srow = j;
+    if (INVERSE) {
+      const int KYi = j > g.NY / 2 ? j - g.NY : j;
+      srow = abs(KYi) < g.TY ? (KYi >= 0 ? KYi : KYi + g.KYc) : -1;
     }
-    if (!loaded) *d = {R(0), R(0)};
+    if (colok && srow >= 0)
+      cp_async_cx(d, src + (size_t)srow * g.TZ + col);
+    else
+      *d = {R(0), R(0)};
   }
   load_twiddles(twy, tw.y, g.NY);
   cp_async_wait_all();
   __syncthreads();
-  fft_inplace<R, KC>(Y, g.ly, KC, 1, KC, twy, INVERSE ? -1 : 1);
-  for (int it = threadIdx.x; it < rows_out * KC; it += blockDim.x) {
-    const int col = it % KC, r = it / KC;
-    if (col >= ncol) continue;
-    const int j = INVERSE ? r : full_from_compact(r, g.TY, g.KYc, g.NY);
-    dst[(size_t)r * g.TZ + col] = Y[j * KC + col];
-  }
+  fft2_smem<R, INVERSE ? -1 : 1, KC>(Y, scr, g.ly, 1, KC, twy);
+  if (colok)
+    for (int r = j0; r < rows_out; r += RSTEP) {
+      const int j = INVERSE ? r : full_from_compact(r, g.TY, g.KYc, g.NY);
+      dst[(size_t)r * g.TZ + col] = Y[j * KC + col];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -196,6 +194,8 @@ __global__ void __launch_bounds__(256) k_y_pass(Geo g, Twiddles<R> tw, const Cx<
 //      z = IFFT_M(Z), a[2n] = Re z[n], a[2n+1] = Im z[n].
 // r2c: z[n] = a[2n] + i a[2n+1], Z = FFT_M(z),
 //      A[k] = (Z[k] + conj Z[M-k])/2 - i/2 (Z[k] - conj Z[M-k]) w^{k}.
+// Lines are held element-major in shared memory (element e of line s at
+// [e*nseq + s]) so that consecutive threads touch consecutive words.
 template <typename R>
 __device__ __forceinline__ Cx<R> c2r_pre(const Cx<R> *row, int k, int M, int TZ, const Cx<R> *twz) {
   const Cx<R> zero = {R(0), R(0)};
@@ -205,19 +205,19 @@ __device__ __forceinline__ Cx<R> c2r_pre(const Cx<R> *row, int k, int M, int TZ,
   return cadd(cadd(a, b), cmul_pi(cmul(csub(a, b), w)));
 }
 
+// seq: natural-order FFT result, element e at seq[e*es]; Z[M] is Z[0]
 template <typename R>
-__device__ __forceinline__ Cx<R> r2c_post(const Cx<R> *seq, int k, int M, const Cx<R> *twz) {
-  // seq is in natural order after the FFT; Z[M] is Z[0]
-  const Cx<R> zk = seq[k & (M - 1)];
-  const Cx<R> zm = cconj(seq[(M - k) & (M - 1)]);
+__device__ __forceinline__ Cx<R> r2c_post(const Cx<R> *seq, int es, int k, int M, const Cx<R> *twz) {
+  const Cx<R> zk = seq[(k & (M - 1)) * es];
+  const Cx<R> zm = cconj(seq[((M - k) & (M - 1)) * es]);
   const Cx<R> e = cadd(zk, zm), d = csub(zk, zm);
   const Cx<R> w = twid(twz, k, 1);
   const Cx<R> t = cmul_mi(cmul(d, w));
   return cscale(cadd(e, t), R(0.5));
 }
 
-// Rows per block of the z kernels and the padded sequence pitch.
-constexpr int ZROWS = 4;
+// Rows per block of the z kernels.
+constexpr int ZROWS = 8;
 
 // z pass fused at the centre of the nonlinear term (operate_omega.cxx:14-58):
 // inverse z transform of the three velocity components of each row, the
@@ -227,82 +227,100 @@ constexpr int ZROWS = 4;
 template <typename R>
 __global__ void __launch_bounds__(256) k_z_products(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int M = g.M, P = M + 1;
+  const int M = g.M;
+  constexpr int NV = ZROWS * 3, NQ = ZROWS * 5;
+  constexpr int EV = NV + 1, EQ = NQ + 1;  // odd element strides: conflict-free columns
   Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *twz = twm + M;
-  Cx<R> *V = twz + g.NZ;      // [ZROWS*3][P] velocity lines, seq = rr*3 + c
-  Cx<R> *Q = V + ZROWS * 3 * P;  // [ZROWS*5][P] product lines, seq = rr*5 + c
-  Cx<R> *A = Q;  // staging of the 3 input rows [ZROWS*3][TZ], reused by Q later
+  Cx<R> *V = twz + g.NZ;     // [M][EV] velocity lines, line = rr*3 + c
+  Cx<R> *Q = V + M * EV;     // [M][EQ] product lines, line = rr*5 + c
+  Cx<R> *scr = Q + M * EQ;   // FFT scratch [M*NQ]; also the staged input and output rows
+  Cx<R> *A = scr;            // [NV][TZ + 1]
+  const int TA = g.TZ + 1;
   const size_t rows = (size_t)g.NX * g.NY;
   const size_t row0 = (size_t)blockIdx.x * ZROWS;
   const size_t cstr = rows * g.TZ;
-  for (int it = threadIdx.x; it < ZROWS * 3 * g.TZ; it += blockDim.x) {
-    const int k = it % g.TZ, rest = it / g.TZ, c = rest % 3, rr = rest / 3;
-    cp_async_cx(A + it, io + c * cstr + (row0 + rr) * g.TZ + k);
+  for (int it = threadIdx.x; it < NV * g.TZ; it += blockDim.x) {
+    const int k = it % g.TZ, q = it / g.TZ, c = q % 3, rr = q / 3;
+    cp_async_cx(A + q * TA + k, io + c * cstr + (row0 + rr) * g.TZ + k);
   }
   load_twiddles(twm, tw.m, M);
   load_twiddles(twz, tw.z, g.NZ);
   cp_async_wait_all();
   __syncthreads();
-  for (int it = threadIdx.x; it < ZROWS * 3 * M; it += blockDim.x) {
-    const int k = it & (M - 1), q = it >> g.lm;  // q = rr*3 + c
-    V[q * P + bitrev(k, g.lm)] = c2r_pre(A + q * g.TZ, k, M, g.TZ, twz);
+  for (int it = threadIdx.x; it < NV * M; it += blockDim.x) {
+    const int q = it % NV, k = it / NV;  // q = rr*3 + c
+    V[k * EV + q] = c2r_pre(A + q * TA, k, M, g.TZ, twz);
   }
   __syncthreads();
-  fft_inplace<R, ZROWS * 3>(V, g.lm, ZROWS * 3, P, 1, twm, -1);
+  fft2_smem<R, -1, NV>(V, scr, g.lm, 1, EV, twm);
   const R sc = R(g.inv_n);
   for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
-    const int n = it & (M - 1), rr = it >> g.lm;
-    const Cx<R> U1 = V[(rr * 3) * P + n], U2 = V[(rr * 3 + 1) * P + n], U3 = V[(rr * 3 + 2) * P + n];
+    const int rr = it % ZROWS, n = it / ZROWS;
+    const Cx<R> *v = V + n * EV + rr * 3;
+    const Cx<R> U1 = v[0], U2 = v[1], U3 = v[2];
     const R u1a = U1.x * sc, u1b = U1.y * sc, u2a = U2.x * sc, u2b = U2.y * sc, u3a = U3.x * sc,
             u3b = U3.y * sc;
-    const int dst = bitrev(n, g.lm);
-    Cx<R> *q = Q + rr * 5 * P + dst;
+    Cx<R> *q = Q + n * EQ + rr * 5;
     q[0] = {u2a * u3a, u2b * u3b};
-    q[P] = {u3a * u1a, u3b * u1b};
-    q[2 * P] = {u1a * u2a, u1b * u2b};
-    q[3 * P] = {(u2a - u3a) * (u2a + u3a), (u2b - u3b) * (u2b + u3b)};
-    q[4 * P] = {(u3a - u1a) * (u3a + u1a), (u3b - u1b) * (u3b + u1b)};
+    q[1] = {u3a * u1a, u3b * u1b};
+    q[2] = {u1a * u2a, u1b * u2b};
+    q[3] = {(u2a - u3a) * (u2a + u3a), (u2b - u3b) * (u2b + u3b)};
+    q[4] = {(u3a - u1a) * (u3a + u1a), (u3b - u1b) * (u3b + u1b)};
   }
   __syncthreads();
-  fft_inplace<R, ZROWS * 5>(Q, g.lm, ZROWS * 5, P, 1, twm, 1);
-  for (int it = threadIdx.x; it < ZROWS * 5 * g.TZ; it += blockDim.x) {
-    const int k = it % g.TZ, rest = it / g.TZ, c = rest % 5, rr = rest / 5;
-    io[c * cstr + (row0 + rr) * g.TZ + k] = r2c_post(Q + (rr * 5 + c) * P, k, M, twz);
+  fft2_smem<R, 1, NQ>(Q, scr, g.lm, 1, EQ, twm);
+  // post-process line by line (consecutive threads: consecutive lines), then
+  // copy the [line][TZ] tile out with consecutive threads on consecutive k
+  Cx<R> *O = scr;  // [NQ][TA]
+  for (int it = threadIdx.x; it < NQ * g.TZ; it += blockDim.x) {
+    const int q = it % NQ, k = it / NQ;
+    O[q * TA + k] = r2c_post(Q + q, EQ, k, M, twz);
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < NQ * g.TZ; it += blockDim.x) {
+    const int k = it % g.TZ, q = it / g.TZ, rr = q / 5, c = q % 5;
+    io[c * cstr + (row0 + rr) * g.TZ + k] = O[q * TA + k];
   }
 }
 
-// z pass, inverse to real space: in I2 [c][NX][NY][TZ], out real [c][NX][NY][NZ]
+// z pass, inverse to real space: in I2 [c][NX][NY][TZ], out real [c][rows][pitch]
 // scaled by 1/(NX NY NZ).  grid (NX*NY/ZROWS, ncomp).
 template <typename R>
 __global__ void __launch_bounds__(256) k_z_c2r(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
                                                R *__restrict__ out, size_t out_cstride, int out_pitch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int M = g.M, P = M + 1;
+  const int M = g.M;
+  constexpr int ES = ZROWS + 1;
   Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *twz = twm + M;
-  Cx<R> *S = twz + g.NZ;  // [ZROWS][P]
-  Cx<R> *A = S + ZROWS * P;  // staged input rows [ZROWS][TZ]
+  Cx<R> *S = twz + g.NZ;        // [M][ES]
+  Cx<R> *scr = S + M * ES;      // FFT scratch [M*ZROWS]; first the staged rows [ZROWS][TZ+1]
+  Cx<R> *A = scr;
+  const int TA = g.TZ + 1;
   const int c = blockIdx.y;
   const size_t rows = (size_t)g.NX * g.NY;
   const size_t row0 = (size_t)blockIdx.x * ZROWS;
   const Cx<R> *src = in + c * rows * g.TZ + row0 * g.TZ;
-  for (int it = threadIdx.x; it < ZROWS * g.TZ; it += blockDim.x) cp_async_cx(A + it, src + it);
+  for (int it = threadIdx.x; it < ZROWS * g.TZ; it += blockDim.x) {
+    const int k = it % g.TZ, rr = it / g.TZ;
+    cp_async_cx(A + rr * TA + k, src + it);
+  }
   load_twiddles(twm, tw.m, M);
   load_twiddles(twz, tw.z, g.NZ);
   cp_async_wait_all();
   __syncthreads();
   for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
-    const int k = it & (M - 1), rr = it >> g.lm;
-    S[rr * P + bitrev(k, g.lm)] = c2r_pre(A + rr * g.TZ, k, M, g.TZ, twz);
+    const int rr = it % ZROWS, k = it / ZROWS;
+    S[k * ES + rr] = c2r_pre(A + rr * TA, k, M, g.TZ, twz);
   }
   __syncthreads();
-  fft_inplace<R, ZROWS>(S, g.lm, ZROWS, P, 1, twm, -1);
+  fft2_smem<R, -1, ZROWS>(S, scr, g.lm, 1, ES, twm);
   const R sc = R(g.inv_n);
   R *dst = out + c * out_cstride;
   for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
     const int n = it & (M - 1), rr = it >> g.lm;
-    const Cx<R> v = S[rr * P + n];
+    const Cx<R> v = S[n * ES + rr];
     R *o = dst + (row0 + rr) * (size_t)out_pitch + 2 * n;
     o[0] = v.x * sc;
     o[1] = v.y * sc;
@@ -318,10 +336,12 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_z_force(Geo g, Twiddles<R> tw, R *__restrict__ phiup,
                                                  const R *__restrict__ ustar, Cx<R> *__restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int M = g.M, P = M + 1;
+  const int M = g.M;
+  constexpr int NS = ZROWS * 3, ES = NS + 1;
   Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *twz = twm + M;
-  Cx<R> *S = twz + g.NZ;  // [ZROWS*3][P]
+  Cx<R> *S = twz + g.NZ;     // [M][ES], line = rr*3 + d
+  Cx<R> *scr = S + M * ES;   // FFT scratch
   load_twiddles(twm, tw.m, M);
   load_twiddles(twz, tw.z, g.NZ);
   const size_t npts = (size_t)g.NX * g.NY * g.NZ;
@@ -357,16 +377,22 @@ __global__ void __launch_bounds__(256) k_z_force(Geo g, Twiddles<R> tw, R *__res
         for (int d = 0; d < 3; ++d) phiup[(1 + d) * npts + o + e] = R(0);
       }
     }
-    const int dst = bitrev(n, g.lm);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) S[(rr * 3 + d) * P + dst] = {f[d][0], f[d][1]};
+    for (int d = 0; d < 3; ++d) S[n * ES + rr * 3 + d] = {f[d][0], f[d][1]};
   }
   __syncthreads();
-  fft_inplace<R, ZROWS * 3>(S, g.lm, ZROWS * 3, P, 1, twm, 1);
+  fft2_smem<R, 1, NS>(S, scr, g.lm, 1, ES, twm);
   const size_t rows = (size_t)g.NX * g.NY;
-  for (int it = threadIdx.x; it < ZROWS * 3 * g.TZ; it += blockDim.x) {
-    const int k = it % g.TZ, rest = it / g.TZ, d = rest % 3, rr = rest / 3;
-    out[d * rows * g.TZ + (row0 + rr) * g.TZ + k] = r2c_post(S + (rr * 3 + d) * P, k, M, twz);
+  const int TA = g.TZ + 1;
+  Cx<R> *O = scr;  // [NS][TA]
+  for (int it = threadIdx.x; it < NS * g.TZ; it += blockDim.x) {
+    const int q = it % NS, k = it / NS;
+    O[q * TA + k] = r2c_post(S + q, ES, k, M, twz);
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < NS * g.TZ; it += blockDim.x) {
+    const int k = it % g.TZ, q = it / g.TZ, d = q % 3, rr = q / 3;
+    out[d * rows * g.TZ + (row0 + rr) * g.TZ + k] = O[q * TA + k];
   }
 }
 
@@ -376,23 +402,25 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_z_r2c_full(Geo g, Twiddles<R> tw, const R *__restrict__ in,
                                                     int in_pitch, Cx<R> *__restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int M = g.M, P = M + 1;
+  const int M = g.M;
   Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *twz = twm + M;
-  Cx<R> *S = twz + g.NZ;
+  constexpr int ES = ZROWS + 1;
+  Cx<R> *S = twz + g.NZ;        // [M][ES]
+  Cx<R> *scr = S + M * ES;
   load_twiddles(twm, tw.m, M);
   load_twiddles(twz, tw.z, g.NZ);
   const size_t row0 = (size_t)blockIdx.x * ZROWS;
   for (int it = threadIdx.x; it < ZROWS * M; it += blockDim.x) {
-    const int n = it % M, rr = it / M;
+    const int n = it & (M - 1), rr = it >> g.lm;
     const R *r = in + (row0 + rr) * (size_t)in_pitch + 2 * n;
-    S[rr * P + bitrev(n, g.lm)] = {r[0], r[1]};
+    S[n * ES + rr] = {r[0], r[1]};
   }
   __syncthreads();
-  fft_inplace(S, g.lm, ZROWS, P, 1, twm, 1);
+  fft2_smem<R, 1, ZROWS>(S, scr, g.lm, 1, ES, twm);
   for (int it = threadIdx.x; it < ZROWS * (M + 1); it += blockDim.x) {
     const int k = it % (M + 1), rr = it / (M + 1);
-    out[(row0 + rr) * (M + 1) + k] = r2c_post(S + rr * P, k, M, twz);
+    out[(row0 + rr) * (M + 1) + k] = r2c_post(S + rr, ES, k, M, twz);
   }
 }
 
@@ -413,6 +441,7 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *Zs = twx + g.NX;               // [2][KXc][KC] zeta tile (updated in place)
   Cx<R> *Pb = Zs + 2 * g.KXc * KC;       // [NX][5*KC], later [NX][3*KC]
+  Cx<R> *scr = Pb + g.NX * W5;            // FFT scratch
   __shared__ double ukd[3];
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
@@ -422,7 +451,7 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
   // stage the five product spectra (bit-reversed rows) and the zeta tile
   for (int it = threadIdx.x; it < 5 * g.NX * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
-    Cx<R> *d = Pb + bitrev(x, g.lx) * W5 + c * KC + col;
+    Cx<R> *d = Pb + x * W5 + c * KC + col;
     if (col < ncol)
       cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col);
     else
@@ -444,7 +473,7 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
   }
   cp_async_wait_all();
   __syncthreads();
-  fft_inplace<R, W5>(Pb, g.lx, W5, 1, W5, twx, 1);
+  fft2_smem<R, 1, W5>(Pb, scr, g.lx, 1, W5, twx);
   const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
   const R ky = R(g.wave[1] * KYi);
   for (int it = threadIdx.x; it < g.KXc * KC; it += blockDim.x) {
@@ -501,13 +530,12 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
         u[2] = {R(ukd[2]), R(0)};
       }
     }
-    const int row = bitrev(i, g.lx);
-    Pb[row * W3 + col] = u[0];
-    Pb[row * W3 + KC + col] = u[1];
-    Pb[row * W3 + 2 * KC + col] = u[2];
+    Pb[i * W3 + col] = u[0];
+    Pb[i * W3 + KC + col] = u[1];
+    Pb[i * W3 + 2 * KC + col] = u[2];
   }
   __syncthreads();
-  fft_inplace<R, W3>(Pb, g.lx, W3, 1, W3, twx, -1);
+  fft2_smem<R, -1, W3>(Pb, scr, g.lx, 1, W3, twx);
   for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
     if (col < ncol) buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col] = Pb[x * W3 + c * KC + col];
@@ -530,6 +558,7 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *Zs = twx + g.NX;          // [2][KXc][KC]
   Cx<R> *Pb = Zs + 2 * g.KXc * KC;  // [NX][3*KC]
+  Cx<R> *scr = Pb + g.NX * W3;       // FFT scratch
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
@@ -537,7 +566,7 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
   const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
   for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
-    Cx<R> *d = Pb + bitrev(x, g.lx) * W3 + c * KC + col;
+    Cx<R> *d = Pb + x * W3 + c * KC + col;
     if (col < ncol)
       cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col);
     else
@@ -550,7 +579,7 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
   load_twiddles(twx, tw.x, g.NX);
   cp_async_wait_all();
   __syncthreads();
-  fft_inplace<R, W3>(Pb, g.lx, W3, 1, W3, twx, 1);
+  fft2_smem<R, 1, W3>(Pb, scr, g.lx, 1, W3, twx);
   const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
   const R ky = R(g.wave[1] * KYi);
   for (int it = threadIdx.x; it < g.KXc * KC; it += blockDim.x) {
