@@ -73,6 +73,14 @@ class Params:
         self.IMASS = 1.0 / self.MASS
         self.MOI = 2.0 / 5.0 * self.MASS * self.RADIUS ** 2
         self.IMOI = 1.0 / self.MOI
+        el = cfg.get("electrolyte", {})
+        self.Dielectric_cst = float(el.get("dielectric", 1.0))
+        self.Surface_charge = float(el.get("surface_charge", 0.0))
+        self.Debye_length = float(el.get("debye", 1.0))
+        self.Valency = [float(el.get("val_p", 1.0)), float(el.get("val_n", -1.0))]
+        self.Onsager = [float(el.get("onsager_p", 1.0)), float(el.get("onsager_n", 1.0))]
+        self.E_ext = [float(e) for e in el.get("efield", (0.0, 0.0, 0.0))]
+        self.Elementary_charge = 1.0  # input.cxx:247
         self.TRN = [(n + 2) // 3 for n in self.N]
         self.L = [n * self.DX for n in self.N]
         self.WAVE = [2.0 * math.pi / l for l in self.L]
@@ -111,6 +119,34 @@ class Spectral:
     def inv(self, A):
         """A_k2a (fft_wrapper.h:534-631)."""
         return np.fft.irfftn(np.conj(A), s=self.P.N, axes=(0, 1, 2))
+
+    def inv_ooura(self, A):
+        """A_k2a on a spectrum that need not be Hermitian on the kz=0 and
+        kz=NZ/2 planes: rdft3dsort(isgn<0) (fftsg3d.c:645-668) reads only one
+        half of each of these planes (and the real part at the self-conjugate
+        points) and the inverse assumes the other half is its conjugate."""
+        X = A.copy()
+        n1, n2, m1 = X.shape
+        n1h, n2h = n1 // 2, n2 // 2
+        I, J = np.meshgrid(np.arange(n1), np.arange(n2), indexing="ij")
+        selfc = ((I == 0) | (I == n1h)) & ((J == 0) | (J == n2h))
+        for kz, hi in ((0, False), (m1 - 1, True)):
+            P = X[:, :, kz]
+            if hi:
+                keep = (J > n2h) | (((J == 0) | (J == n2h)) & (I >= n1h))
+            else:
+                keep = ((J > 0) & (J < n2h)) | (((J == 0) | (J == n2h)) & (I <= n1h))
+            Q = np.where(keep, P, np.conj(P[(-I) % n1, (-J) % n2]))
+            X[:, :, kz] = np.where(selfc, Q.real + 0j, Q)
+        return self.inv(X)
+
+    def grad_k(self, A):
+        """A_k2da_k (fft_wrapper.cxx:103-135): da = -i k a per component."""
+        return np.stack([-1j * self.kx * A, -1j * self.ky * A, -1j * self.kz * A])
+
+    def div_k(self, F):
+        """U_k2divergence_k (fft_wrapper.cxx:649-677): -i k.F."""
+        return -1j * (self.kx * F[0] + self.ky * F[1] + self.kz * F[2])
 
     def truncate(self, A):
         """Truncate_two_third_rule_ooura (fft_wrapper.h:723-766)."""
@@ -566,3 +602,160 @@ class SpmOracle:
     @staticmethod
     def from_ooura(a: np.ndarray) -> np.ndarray:
         return a[..., 0::2] + 1j * a[..., 1::2]
+
+
+def dphi_compact_sin(x, P: Params):
+    """DPhi_compact_sin (profile.h:168-181) with radius RADIUS and xi XI."""
+    hxi = 0.5 * P.XI
+    d = P.RADIUS - np.asarray(x, dtype=np.float64)
+    return np.where(np.abs(d) < hxi, math.pi * 0.5 * (1.0 / P.XI) * np.cos(math.pi * d * (1.0 / P.XI)), 0.0)
+
+
+class ElectrolyteOracle(SpmOracle):
+    """The Electrolyte branch (salt, two ion species, INIT_profile Uniform) of
+    Time_evolution_hydro (sp_3d_ns.cxx:61-212) with NSsolute_solver_Euler
+    (fluid_solver.cxx:306-326)."""
+
+    def __init__(self, cfg: dict):
+        super().__init__(cfg)
+        self.init_rho_ion()
+
+    # ---- particle-grid helpers
+    def _scatter(self, values_per_point):
+        P = self.P
+        r_mesh, r, dist = self.stencil(self.p.x)
+        flat = (r_mesh[..., 0] * P.NY + r_mesh[..., 1]) * P.NZ + r_mesh[..., 2]
+        n = P.NX * P.NY * P.NZ
+        return np.bincount(flat.ravel(), weights=values_per_point(r, dist).ravel(), minlength=n).reshape(P.N)
+
+    def phi_particle(self):
+        """Make_phi_particle (make_phi.cxx:388-400): scatter without the clamp."""
+        return self._scatter(lambda r, dist: phi_profile(dist, self.P.RADIUS, self.P))
+
+    def phi_qq(self):
+        """Make_phi_qq_particle (operate_electrolyte.cxx:179-242): phi and the
+        surface charge Z_e DPhi_compact_sin, rescaled so that its absolute
+        integral is sum |Z_e|."""
+        P = self.P
+        phi = self.phi_particle()
+        ze = P.Surface_charge * P.Elementary_charge
+        surf = self._scatter(lambda r, dist: ze * dphi_compact_sin(dist, P))
+        total = abs(ze) * self.p.n
+        surf = surf * (total / (np.sum(np.abs(surf)) * P.DX3))
+        return phi, surf
+
+    def surface_normal(self):
+        """Make_surface_normal (make_phi.cxx:17-58): sum of r/|r| over
+        interface points (| |r| - RADIUS | < HXI) of every particle."""
+        P = self.P
+        r_mesh, r, dist = self.stencil(self.p.x)
+        rr = np.sqrt(np.sum(r * r, axis=-1))
+        m = np.abs(rr - P.RADIUS) < P.HXI
+        flat = ((r_mesh[..., 0] * P.NY + r_mesh[..., 1]) * P.NZ + r_mesh[..., 2])[m]
+        n = P.NX * P.NY * P.NZ
+        out = np.stack([np.bincount(flat, weights=(r[..., d] / np.where(m, rr, 1.0))[m], minlength=n)
+                        for d in range(3)])
+        return out.reshape((3,) + tuple(P.N))
+
+    def charge_field(self):
+        """Conc_k2charge_field (operate_electrolyte.cxx:45-74)."""
+        P = self.P
+        phi, surf = self.phi_qq()
+        charge = surf.copy()
+        for n in range(2):
+            c = self.S.inv(self.conc_k[n])
+            charge += P.Valency[n] * P.Elementary_charge * c * (1.0 - phi)
+        return charge
+
+    def count_solute(self, conc_x, phi):
+        """Count_single_solute (solute_rhs.cxx:130-148)."""
+        return float(np.sum((1.0 - phi) * conc_x) * self.P.DX3)
+
+    def init_rho_ion(self):
+        """Init_rho_ion (operate_electrolyte.cxx:692-815), salt, Uniform:
+        Set_uniform_ion_charge_density_salt (:516-575) then Count_solute_each
+        (solute_rhs.h:143-157)."""
+        P = self.P
+        phi = self.phi_particle()
+        Z, Np = P.Surface_charge, self.p.n
+        pos = abs(Z * Np / P.Valency[0]) if Z < 0 else 0.0
+        neg = abs(Z * Np / P.Valency[1]) if Z > 0 else 0.0
+        vol = float(np.sum(1.0 - phi))
+        rho_inf = P.kBT * P.Dielectric_cst / (P.Elementary_charge * P.Debye_length) ** 2
+        v0, v1 = P.Valency
+        c0 = pos / (vol * P.DX3) + rho_inf / (v0 * (v0 - v1))
+        c1 = neg / (vol * P.DX3) - rho_inf / (v1 * (v0 - v1))
+        conc = [np.full(P.N, c0), np.full(P.N, c1)]
+        self.conc_k = np.stack([self.S.fwd(c) for c in conc])
+        phi = self.phi_particle()
+        self.total_solute = [self.count_solute(self.S.inv(self.conc_k[n]), phi) for n in range(2)]
+
+    def set_efield(self, e):
+        self.P.E_ext = [float(x) for x in e]
+
+    # ---- the step
+    def step(self):
+        P = self.P
+        S = self.S
+        N = P.NX * P.NY * P.NZ
+        ext_on = any(e != 0.0 for e in P.E_ext)
+        # Rhs_NS_Nernst_Planck (fluid_solver.cxx:243-280): potential gradient
+        charge = self.charge_field()
+        psi = S.truncate(S.fwd(charge) * S.IK2 * (1.0 / P.Dielectric_cst))
+        gk = S.grad_k(psi)
+        for d in range(3):  # Add_constant_field_k (fluid_solver.cxx:228-241)
+            gk[d][0, 0, 0] -= P.E_ext[d] * float(N)
+        grad = np.stack([S.inv(gk[d]) for d in range(3)])
+        # Rhs_NS_solute (fluid_solver.cxx:181-227)
+        zeta = np.stack([S.truncate(self.zeta[d]) for d in range(2)])
+        u = S.zeta_k2u(zeta, self.uk_dc)
+        normal = self.surface_normal()
+        n2 = np.sum(normal * normal, axis=0)
+        rhs_sol = []
+        for n in range(2):
+            self.conc_k[n] = S.truncate(self.conc_k[n])
+            L = P.Onsager[n]
+            flux = np.stack([S.inv(g) for g in S.grad_k(P.kBT * L * self.conc_k[n])])  # Diffusion_flux_single
+            c = S.inv(self.conc_k[n])
+            flux = flux + c * (L * (grad * (P.Valency[n] * P.Elementary_charge)))  # Solute_solver_rhs_nonlinear_x_single
+            # Solute_impermeability (solute_rhs.cxx:42-97): project out the normal part
+            dn = np.where(n2 > 0, np.sum(flux * normal, axis=0) / np.where(n2 > 0, n2, 1.0), 0.0)
+            flux = flux - normal * dn
+            flux = flux + c * -u  # Add_advection_flux
+            fk = np.stack([S.fwd(flux[d]) for d in range(3)])
+            rhs_sol.append(S.div_k(fk))
+        rhs_ns = S.advection_k(u)
+        rhs_ns = np.where(S.keep, rhs_ns - P.NU * S.K2 * zeta, rhs_ns)  # Add_zeta_viscous_term
+        # Field_solver_Euler on the retained modes
+        zeta = np.where(S.keep, zeta + P.DT * rhs_ns, zeta)
+        for n in range(2):
+            self.conc_k[n] = np.where(S.keep, self.conc_k[n] + P.DT * rhs_sol[n], self.conc_k[n])
+        for d in range(3):
+            if P.fix_cell[d]:
+                self.uk_dc[d] = 0.0
+        zeta = np.stack([S.truncate(zeta[d]) for d in range(2)])
+        u = S.zeta_k2u(zeta, self.uk_dc)
+        if self.p.n > 0:
+            self.position_update()
+        # Rescale_solute (solute_rhs.cxx:99-128)
+        phi = self.phi_particle()
+        for n in range(2):
+            fac = self.total_solute[n] / self.count_solute(S.inv(self.conc_k[n]), phi)
+            self.conc_k[n] = self.conc_k[n] * fac
+        # Make_Coulomb_force_x_on_fluid (operate_electrolyte.cxx:90-177): no truncation
+        charge = self.charge_field()
+        gk = S.grad_k(S.fwd(charge) * S.IK2 * (1.0 / P.Dielectric_cst))
+        grad = np.stack([S.inv_ooura(gk[d]) for d in range(3)])
+        f = np.stack([charge * (-grad[d] + (P.E_ext[d] if ext_on else 0.0)) for d in range(3)])
+        u = u + f * (P.DT * P.IRHO)
+        u = S.solenoidal_u(u)
+        if self.p.n > 0:
+            self.hydro_force(u)
+            self.velocity_update()
+            phi, up = self.phi_up(self.p.x, self.p.v, self.p.omega)
+            f = S.solenoidal_u(up - phi * u)
+            u = u + f
+        self.u = u
+        self.zeta, self.uk_dc = S.u2zeta_k(u)
+        self.ts += 1
+        self.time += P.DT

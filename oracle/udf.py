@@ -161,3 +161,20 @@ def ns_config(np_xyz, n_particles, seed, a=5.0, a_xi=2.0, kbt=0.0, dt=0.01, min_
         parts.append(p)
     return {"eq": "Navier_Stokes", "np_xyz": tuple(np_xyz), "particles": parts, "a": a, "a_xi": a_xi,
             "kbt": kbt, "dt": dt, "gravity_g": gravity_g, "mass_ratio": mass_ratio, "rotation": rotation}
+
+
+def electrolyte_config(np_xyz, n_particles, seed, surface_charge=-100.0, debye=4.0, bjerrum=0.7, kbt=1.0,
+                       efield=(0.0, 0.0, 0.0), a=5.0, a_xi=2.0, dt=0.01, min_gap=1.0):
+    """An Electrolyte configuration: two monovalent ion species (salt),
+    Onsager coefficients 1, uniform initial profile, Dielectric_cst chosen so
+    that e^2/(4 pi kBT eps) equals the Bjerrum length."""
+    import math
+
+    cfg = ns_config(np_xyz, n_particles, seed=seed, a=a, a_xi=a_xi, kbt=kbt, dt=dt, min_gap=min_gap)
+    cfg["eq"] = "Electrolyte"
+    cfg["alpha_v"] = 0.0
+    cfg["alpha_o"] = 0.0
+    cfg["electrolyte"] = dict(dielectric=1.0 / (4.0 * math.pi * kbt * bjerrum), surface_charge=float(surface_charge),
+                              debye=float(debye), val_p=1.0, val_n=-1.0, onsager_p=1.0, onsager_n=1.0,
+                              efield=tuple(float(e) for e in efield))
+    return cfg

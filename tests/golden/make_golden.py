@@ -29,6 +29,12 @@ CASES = {
 }
 
 
+EL_CASES = {
+    "el32_efield_x": (dict(np_xyz=(5, 5, 5), n=2, seed=3, surface_charge=-100.0, efield=(0.05, 0.0, 0.0)), 3),
+    "el_16x32x64_pos": (dict(np_xyz=(4, 5, 6), n=3, seed=5, surface_charge=50.0, min_gap=0.5), 3),
+}
+
+
 def make_cfg(spec):
     spec = dict(spec)
     fc = spec.pop("fix_cell", None)
@@ -46,6 +52,16 @@ def main():
         p = r.particles()
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), cfg=json.dumps(cfg), steps=steps, zeta=r.zeta(),
                             uk_dc=r.uk_dc(), **{f"p_{k}": v for k, v in p.items()})
+        print(name, "written")
+    for name, (spec, steps) in EL_CASES.items():
+        spec = dict(spec)
+        cfg = udf.electrolyte_config(spec.pop("np_xyz"), spec.pop("n"), **spec)
+        r = ref.RefSim(cfg)
+        r.step(steps)
+        p = r.particles()
+        conc = np.stack([r.field(20), r.field(21)])
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), cfg=json.dumps(cfg), steps=steps, zeta=r.zeta(),
+                            uk_dc=r.uk_dc(), conc=conc, **{f"p_{k}": v for k, v in p.items()})
         print(name, "written")
     cfg = udf.ns_config((4, 5, 3), 1, seed=1)
     r = ref.RefSim(cfg)

@@ -12,6 +12,7 @@ from oracle import spm
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
 STEP_CASES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLD, "ns*.npz")))
+EL_CASES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLD, "el*.npz")))
 
 
 def rel(a, b):
@@ -21,14 +22,19 @@ def rel(a, b):
 
 def test_fixtures_present():
     assert len(STEP_CASES) >= 3
+    assert len(EL_CASES) >= 2
 
 
-@pytest.mark.parametrize("name", STEP_CASES)
+@pytest.mark.parametrize("name", STEP_CASES + EL_CASES)
 def test_oracle_matches_reference_steps(name):
     g = np.load(os.path.join(GOLD, name + ".npz"))
     cfg = json.loads(str(g["cfg"]))
-    o = spm.SpmOracle(cfg)
+    o = spm.ElectrolyteOracle(cfg) if cfg.get("eq") == "Electrolyte" else spm.SpmOracle(cfg)
     o.run(int(g["steps"]))
+    if "conc" in g.files:
+        for n in range(2):
+            co = spm.SpmOracle.to_ooura(o.conc_k[n])
+            assert np.abs(co - g["conc"][n]).max() < 1e-11 * np.abs(g["conc"][n]).max(), n
     zt = spm.SpmOracle.to_ooura(np.stack([o.S.truncate(o.zeta[d]) for d in range(2)]))
     zr = g["zeta"].copy()
     keep = np.broadcast_to(np.repeat(o.S.keep, 2, axis=2), zr.shape[1:])
