@@ -124,8 +124,14 @@ int kapsel_gpu_get_time(kapsel_ctx *ctx, int *ts, double *time);
 /* Grid sizes: dims[0..5] = NX, NY, NZ, NZ_, n_particles, sekibun points. */
 int kapsel_gpu_get_dims(kapsel_ctx *ctx, int *dims);
 
-/* External electric field E_ext (operate_electrolyte.cxx:90-177). */
+/* External electric field E_ext (operate_electrolyte.cxx:90-177), Electrolyte
+   only: the reference reads it from the UDF (input.cxx:743-790); switching it
+   mid-run replaces a restart with a new Electric_field. */
 int kapsel_gpu_set_efield(kapsel_ctx *ctx, const double *e);
+
+/* Ion concentrations conc_k[2] in the Ooura layout (2*NX*NY*NZ_ doubles;
+   the Concentration array of solute_rhs.cxx:16), Electrolyte only. */
+int kapsel_gpu_get_concentration(kapsel_ctx *ctx, double *conc);
 
 /* ---- Routine-level entry points on host arrays (reference layouts). ---- */
 

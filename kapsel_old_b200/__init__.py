@@ -98,6 +98,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_get_time": (ctypes.c_int, [_VP, _IP, _DP]),
         "kapsel_gpu_get_dims": (ctypes.c_int, [_VP, _IP]),
         "kapsel_gpu_set_efield": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_get_concentration": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_A2a_k": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_A_k2a": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_solenoidal_u": (ctypes.c_int, [_VP, _DP, _DP, _DP]),
@@ -149,6 +150,17 @@ def params_from_config(cfg: dict, precision: int = FP64) -> _Params:
     for d in range(3):
         p.fix_cell[d] = 1 if fc[d] else 0
     p.mt_seed = int(cfg.get("mt_seed", 0))
+    el = cfg.get("electrolyte")
+    if el:
+        p.dielectric = float(el["dielectric"])
+        p.surface_charge = float(el["surface_charge"])
+        p.debye_length = float(el["debye"])
+        p.valency_p = float(el.get("val_p", 1.0))
+        p.valency_n = float(el.get("val_n", -1.0))
+        p.onsager_p = float(el.get("onsager_p", 1.0))
+        p.onsager_n = float(el.get("onsager_n", 1.0))
+        for d, e in enumerate(el.get("efield", (0.0, 0.0, 0.0))):
+            p.e_ext[d] = float(e)
     return p
 
 
@@ -246,6 +258,16 @@ class Simulation:
         a[: self.Np, 27:31] = st["q"]
         a[: self.Np, 31:35] = st["q_old"]
         self._check(self.L.kapsel_gpu_set_particle_state(self.h, _ptr(a)))
+
+    def concentration(self) -> np.ndarray:
+        """Ion concentrations (2, NX, NY, NZ_) in the Ooura layout (Electrolyte)."""
+        c = np.zeros((2, self.NX, self.NY, self.NZ_))
+        self._check(self.L.kapsel_gpu_get_concentration(self.h, _ptr(c)))
+        return c
+
+    def set_efield(self, e):
+        a = np.ascontiguousarray(e, dtype=np.float64)
+        self._check(self.L.kapsel_gpu_set_efield(self.h, _ptr(a)))
 
     # ---- routine-level entry points (reference layouts, NX*NY*NZ_ doubles)
     def _padded(self, a):

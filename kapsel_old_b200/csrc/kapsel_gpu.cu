@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "../../include/kapsel_gpu.h"
+#include "electrolyte_kernels.cuh"
 #include "particle_kernels.cuh"
 #include "spectral_kernels.cuh"
 
@@ -138,7 +139,7 @@ struct BoxBase {
   int *cells = nullptr;
   double *uk_dc = nullptr;
   int *status = nullptr;
-  double *partial = nullptr;  // [Np][PCL][18] partial force sums
+  double *partial_p = nullptr;  // [Np][PCL][18] partial force sums
   int *arrivals = nullptr;    // [Np] blocks done per particle (0 between launches)
   double *noise_dev[2] = {nullptr, nullptr};
   double *noise_host[2] = {nullptr, nullptr};
@@ -151,6 +152,9 @@ struct BoxBase {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
 
   virtual int alloc() = 0;
+  virtual int alloc_el() = 0;
+  virtual int init_el() = 0;
+  virtual int conc_to_host(double *c) = 0;
   virtual void launch_step(const double *noise, int euler, cudaEvent_t *ev = nullptr) = 0;
   virtual void launch_init() = 0;
   virtual int velocity_to_host(double *u) = 0;
@@ -274,6 +278,10 @@ struct Box : BoxBase {
   }
 
   void launch_step(const double *noise, int euler, cudaEvent_t *ev = nullptr) override {
+    if (prm.eq == KAPSEL_EQ_ELECTROLYTE) {
+      launch_step_el(euler);
+      return;
+    }
     int e = 0;
     auto mark = [&]() {
       if (ev) cudaEventRecord(ev[e++], stream);
@@ -297,7 +305,7 @@ struct Box : BoxBase {
       k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
       mark();
       k_particles_hydro_velocity<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, ustar, cells, noise, euler, status,
-                                                                    partial, arrivals);
+                                                                    partial_p, arrivals);
       mark();
       k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup);
       mark();
@@ -322,6 +330,228 @@ struct Box : BoxBase {
       launch_force_to_zeta();
     }
     cudaMemsetAsync(uk_dc, 0, sizeof(double) * 3, stream);
+  }
+
+  // ---- Electrolyte branch (two ion species) --------------------------------
+  Cx<R> *conc_k = nullptr;  // [2][KXc][KYc][TZ]
+  Cx<R> *rho_k = nullptr;   // [KXc][KYc][TZ]
+  R *phiq = nullptr;        // [5][N]: phi, surface charge, normal x/y/z
+  R *creal = nullptr;       // [2][N]
+  R *gradr = nullptr;       // [3][N]
+  R *ureal = nullptr;       // [3][N]
+  R *fluxr = nullptr;       // [3][N]
+  R *charge = nullptr;      // [N]
+  Cx<R> *F1 = nullptr, *F2 = nullptr;  // full spectra [3][NX][NY][M+1]
+  double *scal = nullptr;   // [0] surface-charge scale, [1..2] rescale factors, [3] free volume
+  double *partial = nullptr;
+  double *total_solute = nullptr;  // [2]
+  Geo gF;                    // geometry whose retained box is the whole half spectrum
+  size_t sm_el = 0;          // dynamic shared memory of the electrolyte launches
+
+  int alloc_el() override {
+    gF = g;
+    gF.TX = g.NX / 2 + 1;
+    gF.KXc = g.NX;
+    gF.TY = g.NY / 2 + 1;
+    gF.KYc = g.NY;
+    gF.TZ = g.M + 1;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ, N = npts();
+    const size_t nfull = (size_t)g.NX * g.NY * (g.M + 1);
+    KCHECK(cudaMalloc(&conc_k, sizeof(Cx<R>) * 2 * nz));
+    KCHECK(cudaMalloc(&rho_k, sizeof(Cx<R>) * nz));
+    KCHECK(cudaMalloc(&phiq, sizeof(R) * 5 * N));
+    KCHECK(cudaMalloc(&creal, sizeof(R) * 2 * N));
+    KCHECK(cudaMalloc(&gradr, sizeof(R) * 3 * N));
+    KCHECK(cudaMalloc(&ureal, sizeof(R) * 3 * N));
+    KCHECK(cudaMalloc(&fluxr, sizeof(R) * 3 * N));
+    KCHECK(cudaMalloc(&charge, sizeof(R) * N));
+    KCHECK(cudaMalloc(&F1, sizeof(Cx<R>) * 3 * nfull));
+    KCHECK(cudaMalloc(&F2, sizeof(Cx<R>) * 3 * nfull));
+    KCHECK(cudaMalloc(&scal, sizeof(double) * 8));
+    KCHECK(cudaMalloc(&partial, sizeof(double) * 2 * RED_BLOCKS));
+    KCHECK(cudaMalloc(&total_solute, sizeof(double) * 2));
+    KCHECK(cudaMemset(conc_k, 0, sizeof(Cx<R>) * 2 * nz));
+    KCHECK(cudaMemset(scal, 0, sizeof(double) * 8));
+    // one dynamic shared-memory size for every electrolyte launch: the
+    // largest of the x passes (full geometry, 3 components) and z passes
+    const size_t C = sizeof(Cx<R>);
+    const size_t xi = C * (g.NX + (size_t)3 * gF.KXc * KCX + (size_t)2 * g.NX * 3 * KCX);
+    const size_t xf = C * (g.NX + (size_t)2 * g.NX * 3 * KCX);
+    const size_t zr = C * (g.M + g.NZ + (size_t)g.M * (ZROWS + 1) + std::max((size_t)g.M * ZROWS, (size_t)ZROWS * (g.M + 2)));
+    sm_el = std::max(std::max(xi, xf), std::max(zr, smem_zc));
+    sm_el = std::max(sm_el, smem_y);
+    if (sm_el > 227 * 1024) return KAPSEL_ERANGE;
+    const int sm = (int)sm_el;
+    KCHECK(cudaFuncSetAttribute(k_x_inv_op<R, KCX, XI_IDENT, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_x_inv_op<R, KCX, XI_IDENT, 3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_x_inv_op<R, KCX, XI_GRADPSI, 1, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_x_inv_op<R, KCX, XI_GRADDIFF, 1, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_x_fwd_op<R, KCX, XF_STORE, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_x_fwd_op<R, KCX, XF_CONCUPD, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_x_fwd_op<R, KCX, XF_GRADPSI_FULL, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_z_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_xadv));
+    return 0;
+  }
+
+  dim3 gxF() const { return dim3(gF.KYc, (gF.TZ + KCX - 1) / KCX); }
+  dim3 gyF(int nc) const { return dim3(g.NX, nc, (gF.TZ + KCY - 1) / KCY); }
+  double ze() const { return prm.surface_charge * 1.0; }  // Surface_charge_e, Elementary_charge = 1
+  bool ext_on() const { return prm.e_ext[0] != 0.0 || prm.e_ext[1] != 0.0 || prm.e_ext[2] != 0.0; }
+
+  // real c_n = A_k2a_out(conc_k[n]) for both species
+  void el_conc_real() {
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    k_x_inv_op<R, KCX, XI_IDENT, 2, 2><<<gx(), 256, sm_el, stream>>>(g, tw, conc_k, nz, bufA, KOp{});
+    k_y_pass<R, true, KCY><<<gy(2), 256, sm_el, stream>>>(g, tw, bufA, bufB);
+    k_z_c2r<R><<<dim3(gz(), 2), 256, sm_el, stream>>>(g, tw, bufB, creal, npts(), g.NZ);
+  }
+  // surface-charge scale s0 = sum|Z_e| / (sum|surf| DX3) (operate_electrolyte.cxx:217-241)
+  void el_surface_scale() {
+    k_reduce_partial<R, RED_ABS><<<RED_BLOCKS, 256, 0, stream>>>(npts(), phiq + npts(), nullptr, 0, 1, partial);
+    const double dx3 = prm.dx * prm.dx * prm.dx;
+    k_reduce_final<<<1, 256, 0, stream>>>(partial, RED_BLOCKS, 1, 0, fabs(ze()) * Np, total_solute, dx3, scal);
+  }
+  void el_scatter(int with_normal) {
+    cudaMemsetAsync(phiq, 0, sizeof(R) * (with_normal ? 5 : 2) * npts(), stream);
+    if (Np > 0) k_particles_scatter_el<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiq, ze(), with_normal);
+  }
+  // forward transform of ncomp real fields, 2/3 modes kept, into bufA (I1 layout)
+  void el_forward_trunc(const R *real, int ncomp) {
+    k_z_r2c<R><<<dim3(gz(), ncomp), 256, sm_el, stream>>>(g, tw, real, g.NZ, npts(), bufB, g.TZ);
+    k_y_pass<R, false, KCY><<<gy(ncomp), 256, sm_el, stream>>>(g, tw, bufB, bufA);
+  }
+  // inverse of three I1-layout components in bufA into real fields
+  void el_inverse3(R *out) {
+    k_y_pass<R, true, KCY><<<gy(3), 256, sm_el, stream>>>(g, tw, bufA, bufB);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(g, tw, bufB, out, npts(), g.NZ);
+  }
+
+  void launch_step_el(int euler) {
+    const size_t N = npts(), nz = (size_t)g.KXc * g.KYc * g.TZ;
+    const double dx3 = prm.dx * prm.dx * prm.dx;
+    const double ve[2] = {prm.valency_p, prm.valency_n}, L[2] = {prm.onsager_p, prm.onsager_n};
+    const double ieps = 1.0 / prm.dielectric;
+    const int pb = 592;
+    // Rhs_NS_Nernst_Planck: charge from the current conc and positions
+    el_scatter(1);
+    el_surface_scale();
+    el_conc_real();
+    k_el_charge<R><<<pb, 256, 0, stream>>>(N, phiq, creal, scal, 0, ve[0], ve[1], charge);
+    el_forward_trunc(charge, 1);
+    k_x_fwd_op<R, KCX, XF_STORE, 1><<<gx(), 256, sm_el, stream>>>(g, tw, bufA, rho_k, 0, KOp{});
+    KOp gp{ieps, {prm.e_ext[0] * (double)N, prm.e_ext[1] * (double)N, prm.e_ext[2] * (double)N}};
+    k_x_inv_op<R, KCX, XI_GRADPSI, 1, 3><<<gx(), 256, sm_el, stream>>>(g, tw, rho_k, nz, bufA, gp);
+    el_inverse3(gradr);
+    // Rhs_NS_solute: u, the advection term and the explicit Euler update of zeta
+    k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
+    k_y_pass<R, true, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(g, tw, bufB, ureal, N, g.NZ);
+    k_z_products<R><<<gz(), 256, smem_zp, stream>>>(g, tw, bufB);
+    k_y_pass<R, false, KCY><<<gy(5), 256, smem_y, stream>>>(g, tw, bufB, bufA);
+    k_x_advect_update<R, KCX, 1><<<gx(), 256, smem_xadv, stream>>>(g, tw, bufA, zeta, uk_dc);
+    // ion fluxes and the Euler update of each concentration
+    for (int n = 0; n < 2; ++n) {
+      KOp dk{prm.kbt * L[n], {0, 0, 0}};
+      k_x_inv_op<R, KCX, XI_GRADDIFF, 1, 3><<<gx(), 256, sm_el, stream>>>(g, tw, conc_k + n * nz, nz, bufA, dk);
+      el_inverse3(fluxr);
+      k_el_flux<R><<<pb, 256, 0, stream>>>(N, fluxr, creal + n * N, gradr, phiq + 2 * N, ureal, N, L[n], ve[n]);
+      el_forward_trunc(fluxr, 3);
+      k_x_fwd_op<R, KCX, XF_CONCUPD, 3><<<gx(), 256, sm_el, stream>>>(g, tw, bufA, conc_k + n * nz, 0,
+                                                                         KOp{prm.dt, {0, 0, 0}});
+    }
+    if (Np > 0) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
+    // Rescale_solute at the new positions, then the Coulomb force
+    el_scatter(0);
+    el_surface_scale();
+    el_conc_real();
+    k_reduce_partial<R, RED_PHI_C><<<RED_BLOCKS, 256, 0, stream>>>(N, phiq, creal, N, 2, partial);
+    k_reduce_final<<<1, 256, 0, stream>>>(partial, RED_BLOCKS, 2, 1, 0.0, total_solute, dx3, scal);
+    k_scale_conc<R><<<pb, 256, 0, stream>>>(nz, conc_k, scal);
+    k_el_charge<R><<<pb, 256, 0, stream>>>(N, phiq, creal, scal, 1, ve[0], ve[1], charge);
+    // full (untruncated) potential gradient with the Ooura inverse semantics
+    const size_t nfull = (size_t)g.NX * g.NY * (g.M + 1);
+    k_z_r2c<R><<<dim3(gz(), 1), 256, sm_el, stream>>>(gF, tw, charge, g.NZ, N, F2, g.M + 1);
+    k_y_pass<R, false, KCY><<<gyF(1), 256, sm_el, stream>>>(gF, tw, F2, F1);
+    k_x_fwd_op<R, KCX, XF_GRADPSI_FULL, 1><<<gxF(), 256, sm_el, stream>>>(gF, tw, F1, F2, nfull,
+                                                                             KOp{ieps, {0, 0, 0}});
+    k_hermitian_planes<R><<<pb, 256, 0, stream>>>(gF, F2, 3);
+    k_x_inv_op<R, KCX, XI_IDENT, 3, 3><<<gxF(), 256, sm_el, stream>>>(gF, tw, F2, nfull, F1, KOp{});
+    k_y_pass<R, true, KCY><<<gyF(3), 256, sm_el, stream>>>(gF, tw, F1, F2);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(gF, tw, F2, gradr, N, g.NZ);
+    const bool ext = ext_on();
+    k_el_coulomb<R><<<pb, 256, 0, stream>>>(N, charge, gradr, ext ? prm.e_ext[0] : 0.0, ext ? prm.e_ext[1] : 0.0,
+                                            ext ? prm.e_ext[2] : 0.0, prm.dt / prm.rho, fluxr);
+    // u += f dt/rho; Solenoidal_u: in k-space zeta += zeta(sol f), uk_dc += f(0)
+    el_forward_trunc(fluxr, 3);
+    k_x_force_to_zeta<R, KCX><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc);
+    // u (real) of the updated zeta, then the particle part of the step
+    k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
+    k_y_pass<R, true, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, N, g.NZ);
+    if (Np > 0) {
+      k_particles_hydro_velocity<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, ustar, cells, nullptr, euler, status,
+                                                                  partial_p, arrivals);
+      k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup);
+      launch_force_to_zeta();
+    }
+  }
+
+  // Init_rho_ion, salt with a uniform initial profile (operate_electrolyte.cxx:
+  // 516-575, 692-815): densities from the free volume sum(1 - phi).
+  int init_el() override {
+    el_scatter(0);
+    k_reduce_partial<R, RED_1MPHI><<<RED_BLOCKS, 256, 0, stream>>>(npts(), phiq, nullptr, 0, 1, partial);
+    k_reduce_final<<<1, 256, 0, stream>>>(partial, RED_BLOCKS, 1, 2, 0.0, total_solute, 1.0, scal);
+    double h[8];
+    KCHECK(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    const double vol = h[3], dx3 = prm.dx * prm.dx * prm.dx;
+    const double Z = prm.surface_charge, v0 = prm.valency_p, v1 = prm.valency_n;
+    const double pos = Z < 0. ? fabs(Z * Np / v0) : 0.0, neg = Z > 0. ? fabs(Z * Np / v1) : 0.0;
+    const double e = 1.0;  // Elementary_charge
+    const double rho_inf = prm.kbt * prm.dielectric / ((e * prm.debye_length) * (e * prm.debye_length));
+    const double c0 = pos / (vol * dx3) + rho_inf / (v0 * (v0 - v1));
+    const double c1 = neg / (vol * dx3) + -rho_inf / (v1 * (v0 - v1));
+    const double tot[2] = {c0 * vol * dx3, c1 * vol * dx3};
+    const double Nn = (double)npts();
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    KCHECK(cudaMemsetAsync(conc_k, 0, sizeof(Cx<R>) * 2 * nz, stream));
+    const Cx<R> k0[2] = {{(R)(c0 * Nn), (R)0}, {(R)(c1 * Nn), (R)0}};
+    KCHECK(cudaMemcpyAsync(conc_k, &k0[0], sizeof(Cx<R>), cudaMemcpyHostToDevice, stream));
+    KCHECK(cudaMemcpyAsync(conc_k + nz, &k0[1], sizeof(Cx<R>), cudaMemcpyHostToDevice, stream));
+    KCHECK(cudaMemcpyAsync(total_solute, tot, sizeof(tot), cudaMemcpyHostToDevice, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    return 0;
+  }
+
+  int conc_to_host(double *c) override {
+    if (!conc_k) return KAPSEL_ESTATE;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    std::vector<Cx<R>> h(2 * nz);
+    KCHECK(cudaMemcpyAsync(h.data(), conc_k, sizeof(Cx<R>) * h.size(), cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    const int NZ_ = g.NZ + 2;
+    const size_t plane = (size_t)g.NX * g.NY * NZ_;
+    memset(c, 0, sizeof(double) * 2 * plane);
+    for (int q = 0; q < 2; ++q)
+      for (int ix = 0; ix < g.KXc; ++ix) {
+        const int i = ix < g.TX ? ix : g.NX + ix - g.KXc;
+        for (int iy = 0; iy < g.KYc; ++iy) {
+          const int j = iy < g.TY ? iy : g.NY + iy - g.KYc;
+          for (int k = 0; k < g.TZ; ++k) {
+            const Cx<R> v = h[q * nz + ((size_t)ix * g.KYc + iy) * g.TZ + k];
+            double *o = c + q * plane + ((size_t)i * g.NY + j) * NZ_ + 2 * k;
+            o[0] = (double)v.x;
+            o[1] = (double)v.y;
+          }
+        }
+      }
+    return 0;
   }
 
   // ---- host <-> device helpers in the reference layouts
@@ -393,6 +623,19 @@ struct Box : BoxBase {
   int fhydro_host(const double *u0, const double *u1, const double *u2, double *f, double *t) override;
 
   void free_all() override {
+    cudaFree(conc_k);
+    cudaFree(rho_k);
+    cudaFree(phiq);
+    cudaFree(creal);
+    cudaFree(gradr);
+    cudaFree(ureal);
+    cudaFree(fluxr);
+    cudaFree(charge);
+    cudaFree(F1);
+    cudaFree(F2);
+    cudaFree(scal);
+    cudaFree(partial);
+    cudaFree(total_solute);
     cudaFree(zeta);
     cudaFree(bufA);
     cudaFree(bufB);
@@ -783,7 +1026,10 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   *out = nullptr;
   for (int d = 0; d < 3; ++d)
     if (p->np_xyz[d] < 4 || p->np_xyz[d] > 9) return KAPSEL_EINVAL;  // 16..512 per axis
-  if (p->eq != KAPSEL_EQ_NAVIER_STOKES) return KAPSEL_EINVAL;
+  if (p->eq != KAPSEL_EQ_NAVIER_STOKES && p->eq != KAPSEL_EQ_ELECTROLYTE) return KAPSEL_EINVAL;
+  if (p->eq == KAPSEL_EQ_ELECTROLYTE && (!(p->dielectric > 0.0) || p->surface_charge == 0.0 || !(p->debye_length > 0.0) ||
+                                         !(p->valency_p > 0.0) || !(p->valency_n < 0.0)))
+    return KAPSEL_EINVAL;
   if (p->precision != KAPSEL_FP64 && p->precision != KAPSEL_MIXED) return KAPSEL_EINVAL;
   if (p->n_particles < 0 || p->dx <= 0 || p->rho <= 0 || p->eta <= 0 || p->dt <= 0 || p->a <= 0 || p->a_xi <= 0)
     return KAPSEL_EINVAL;
@@ -864,7 +1110,8 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   const double gravity_on_fluid = p->gravity_g * p->rho * 4. / 3. * M_PI * (pp.RADIUS * pp.RADIUS) * pp.RADIUS;
   pp.grav = p->gravity_g != 0.0 ? gravity_on_fluid * (p->mass_ratio - 1.0) : 0.0;
   pp.gdir = p->gravity_dir;
-  pp.thermostat = (p->kbt > 0.0 && b->Np > 0) ? 1 : 0;
+  // no thermostat in the Electrolyte branch (sp_3d_ns.cxx:183)
+  pp.thermostat = (p->kbt > 0.0 && b->Np > 0 && p->eq != KAPSEL_EQ_ELECTROLYTE) ? 1 : 0;
   const double zeta_drag = 6. * M_PI * p->eta * pp.RADIUS;
   const double zeta_drag_rot = 8. * M_PI * p->eta * (pp.RADIUS * pp.RADIUS * pp.RADIUS);
   pp.noise_v = 1.439 * std::sqrt(zeta_drag * p->dt * p->kbt * p->alpha_v);
@@ -874,6 +1121,10 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return KAPSEL_ECUDA;
   int rc = b->alloc();
   if (rc) return rc;
+  if (p->eq == KAPSEL_EQ_ELECTROLYTE) {
+    rc = b->alloc_el();
+    if (rc) return rc;
+  }
   const int np1 = b->Np > 0 ? b->Np : 1;
   if (cudaMalloc(&b->parts, sizeof(DPart) * np1) != cudaSuccess) return KAPSEL_ENOMEM;
   if (cudaMemset(b->parts, 0, sizeof(DPart) * np1) != cudaSuccess) return KAPSEL_ECUDA;
@@ -884,7 +1135,7 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   cudaMemset(b->uk_dc, 0, sizeof(double) * 3);
   if (cudaMalloc(&b->status, sizeof(int)) != cudaSuccess) return KAPSEL_ENOMEM;
   cudaMemset(b->status, 0, sizeof(int));
-  if (cudaMalloc(&b->partial, sizeof(double) * 18 * PCL * np1) != cudaSuccess) return KAPSEL_ENOMEM;
+  if (cudaMalloc(&b->partial_p, sizeof(double) * 18 * PCL * np1) != cudaSuccess) return KAPSEL_ENOMEM;
   if (cudaMalloc(&b->arrivals, sizeof(int) * np1) != cudaSuccess) return KAPSEL_ENOMEM;
   cudaMemset(b->arrivals, 0, sizeof(int) * np1);
   for (int s = 0; s < 2; ++s) {
@@ -917,7 +1168,7 @@ int kapsel_gpu_destroy(kapsel_ctx *ctx) {
     cudaFree(b->cells);
     cudaFree(b->uk_dc);
     cudaFree(b->status);
-    cudaFree(b->partial);
+    cudaFree(b->partial_p);
     cudaFree(b->arrivals);
     cudaStreamDestroy(b->stream);
   }
@@ -964,6 +1215,10 @@ int kapsel_gpu_init_state(kapsel_ctx *ctx) {
   b->launch_init();
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
   if (cudaGetLastError() != cudaSuccess) return KAPSEL_ECUDA;
+  if (b->prm.eq == KAPSEL_EQ_ELECTROLYTE) {
+    int rc = b->init_el();
+    if (rc) return rc;
+  }
   b->ts = 0;
   b->time = 0.0;
   b->initialised = true;
@@ -1124,8 +1379,23 @@ int kapsel_gpu_get_dims(kapsel_ctx *ctx, int *dims) {
 
 int kapsel_gpu_set_efield(kapsel_ctx *ctx, const double *e) {
   if (!ctx || !e) return KAPSEL_EINVAL;
-  for (int d = 0; d < 3; ++d) ctx->box->prm.e_ext[d] = e[d];
-  return ctx->box->prm.eq == KAPSEL_EQ_ELECTROLYTE ? 0 : KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (b->prm.eq != KAPSEL_EQ_ELECTROLYTE) return KAPSEL_EINVAL;
+  for (int d = 0; d < 3; ++d) b->prm.e_ext[d] = e[d];
+  // the field enters the step as launch arguments: re-capture the graphs
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
+  for (int s = 0; s < 2; ++s)
+    if (b->graph[s]) {
+      cudaGraphExecDestroy(b->graph[s]);
+      b->graph[s] = nullptr;
+    }
+  return 0;
+}
+
+int kapsel_gpu_get_concentration(kapsel_ctx *ctx, double *c) {
+  if (!ctx || !c) return KAPSEL_EINVAL;
+  if (ctx->box->prm.eq != KAPSEL_EQ_ELECTROLYTE) return KAPSEL_ESTATE;
+  return ctx->box->conc_to_host(c);
 }
 
 int kapsel_gpu_A2a_k(kapsel_ctx *ctx, double *a) {
@@ -1166,10 +1436,10 @@ int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr) {
   // u is never read with S == 0
   if (b->prm.precision == KAPSEL_FP64)
     k_particles_hydro_velocity<double><<<b->Np * PCL, 256, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
-                                                                           b->status, b->partial, b->arrivals);
+                                                                           b->status, b->partial_p, b->arrivals);
   else
     k_particles_hydro_velocity<float><<<b->Np * PCL, 256, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
-                                                                          b->status, b->partial, b->arrivals);
+                                                                          b->status, b->partial_p, b->arrivals);
   std::vector<DPart> h(b->Np);
   cudaMemcpyAsync(h.data(), scratch, sizeof(DPart) * b->Np, cudaMemcpyDeviceToHost, b->stream);
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;

@@ -433,7 +433,11 @@ __global__ void __launch_bounds__(256) k_z_r2c_full(Geo g, Twiddles<R> tw, const
 //   zeta and the inverse x transform of u*.
 // In place on buf: reads [5][NX][KYc][TZ], writes [3][NX][KYc][TZ].
 // grid (KYc, ceil(TZ/KC)).
-template <typename R, int KC>
+// EULER = 1 is the Electrolyte variant: explicit Euler of
+// NSsolute_solver_Euler (Add_zeta_viscous_term then Field_solver_Euler,
+// fluid_solver.cxx:122-135, operate_omega.cxx:172-184) instead of the slaved
+// step, and no u* output (the electrolyte rebuilds u after the Coulomb force).
+template <typename R, int KC, int EULER = 0>
 __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ buf,
                                                          Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -499,18 +503,27 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
     select_zeta(KXi, KYi, w, f0, f1);
     const R K2 = k1 * k1 + k2 * k2 + k3 * k3;
     const R IK2 = K2 > R(0) ? R(1) / K2 : R(0);
-    const double arg = -g.nu * g.dt * (double)K2;
-    const R dmy = R(g.fp64_exp ? exp(arg) - 1.0 : expm1(arg));
-    const R c1 = R(1.0 / g.nu) * IK2;
     Cx<R> z0 = Zs[ix * KC + col], z1 = Zs[(g.KXc + ix) * KC + col];
-    z0 = {z0.x + dmy * (z0.x - c1 * f0.x), z0.y + dmy * (z0.y - c1 * f0.y)};
-    z1 = {z1.x + dmy * (z1.x - c1 * f1.x), z1.y + dmy * (z1.y - c1 * f1.y)};
+    if (EULER) {
+      const R nk2 = R(g.nu) * K2, dt = R(g.dt);
+      const Cx<R> r0 = {f0.x + -(nk2 * z0.x), f0.y + -(nk2 * z0.y)};
+      const Cx<R> r1 = {f1.x + -(nk2 * z1.x), f1.y + -(nk2 * z1.y)};
+      z0 = {z0.x + dt * r0.x, z0.y + dt * r0.y};
+      z1 = {z1.x + dt * r1.x, z1.y + dt * r1.y};
+    } else {
+      const double arg = -g.nu * g.dt * (double)K2;
+      const R dmy = R(g.fp64_exp ? exp(arg) - 1.0 : expm1(arg));
+      const R c1 = R(1.0 / g.nu) * IK2;
+      z0 = {z0.x + dmy * (z0.x - c1 * f0.x), z0.y + dmy * (z0.y - c1 * f0.y)};
+      z1 = {z1.x + dmy * (z1.x - c1 * f1.x), z1.y + dmy * (z1.y - c1 * f1.y)};
+    }
     const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
     zeta[o] = z0;
     zeta[zplane + o] = z1;
     Zs[ix * KC + col] = z0;
     Zs[(g.KXc + ix) * KC + col] = z1;
   }
+  if (EULER) return;
   __syncthreads();
   // u*_k = Zeta_k2u_k(zeta', uk_dc) on all NX rows (zero outside |kx| < TX)
   for (int it = threadIdx.x; it < g.NX * KC; it += blockDim.x) {
