@@ -179,7 +179,7 @@ def run_ours(args, rank, world, local_rank):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     L = kg.load_library()
 
-    def timed(precision, steps, warmup):
+    def timed(precision, steps, warmup, cfg=cfg):
         sim = kg.Simulation(cfg, precision=precision)
         sp = ctypes.c_void_p()
         sim._check(L.kapsel_gpu_get_stream(sim.h, ctypes.byref(sp)))
@@ -250,6 +250,30 @@ def run_ours(args, rank, world, local_rank):
         e2e_s = float(t.item())
     sim_m.close()
 
+    # ---- the other workloads, same timing rules, fewer steps
+    extra = {}
+    if not args.no_extra:
+        k2 = max(10, min(args.steps, 50))
+        c1 = workload.plain_64_16()
+        s1, _, ms1 = timed(kg.FP64, k2, args.warmup, cfg=c1)
+        s1.close()
+        c3 = workload.electrolyte_128_64()
+        s3m, _, ms3m = timed(kg.MIXED, k2, args.warmup, cfg=c3)
+        s3m.close()
+        s3d, _, ms3d = timed(kg.FP64, k2, args.warmup, cfg=c3)
+        s3d.close()
+        extra = {
+            "plain_64cubed_16_fp64": {"value": round(k2 * world / (ms1 * 1e-3), 2), "unit": UNIT, "steps": k2,
+                                      "workload": "64^3, 16 spheres a=5, kBT=0, body force 1e-3 along -z, FP64"},
+            "electrolyte_128cubed_64": {"mixed": round(k2 * world / (ms3m * 1e-3), 2),
+                                        "fp64": round(k2 * world / (ms3d * 1e-3), 2), "unit": UNIT, "steps": k2,
+                                        "workload": "128^3, 64 spheres a=5 Z=-100, salt Debye 4, Bjerrum 0.7, "
+                                                    "E_x=0.05"},
+        }
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            extra["plain_64cubed_16_fp64"]["cpu_baseline"] = cpu_baseline(c1, warmup=1, steps=30)
+            extra["electrolyte_128cubed_64"]["cpu_baseline"] = cpu_baseline(c3, warmup=1, steps=4)
+
     steps_total = args.steps * world
     value = steps_total / (ms_m * 1e-3)
     fp64_value = steps_total / (ms_d * 1e-3)
@@ -290,6 +314,7 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": kg.P_STRIDE * 8 * Np + 4},
         "gpu_launches": nker * args.steps,
         "clocks": clocks,
+        "other_workloads": extra,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, warmup=1, steps=min(args.steps, 12))
@@ -311,7 +336,7 @@ def cpu_baseline(cfg, warmup: int, steps: int, threads: int | None = None):
                                  timeout=900)
             d = json.loads(out.stdout.strip().splitlines()[-1])
         return {"value": round(1.0 / d["s_per_step"], 4), "unit": UNIT, "cores": threads, "kind": "reference",
-                "sample": f"{steps} steps of the same 128^3/256-sphere workload after {warmup} warm-up, "
+                "sample": f"{steps} steps of the same workload after {warmup} warm-up, "
                           f"unmodified KAPSEL sources (OpenMP loops, Ooura FFT), wall clock"}
     from oracle import spm
 
@@ -359,6 +384,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the 64^3 FP64 and electrolyte workloads")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))

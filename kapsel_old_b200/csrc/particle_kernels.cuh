@@ -220,7 +220,7 @@ __device__ void block_reduce(KSum (&v)[NV], double *sh /* [2*NV][32] */) {
 constexpr int PCL = 4;
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart *__restrict__ parts,
+__global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPart *__restrict__ parts,
                                                                   const R *__restrict__ u, const int *__restrict__ cells,
                                                                   const double *__restrict__ noise, int euler,
                                                                   int *__restrict__ status,
@@ -238,9 +238,11 @@ __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart 
   const double wp[3] = {a.omega[0], a.omega[1], a.omega[2]};
   const StencilBase b = stencil_base(xp, p);
   const size_t npts = (size_t)p.N[0] * p.N[1] * p.N[2];
-  KSum acc[9];
+  // each thread adds only a few terms: plain sums here, compensated sums in
+  // the block and cross-block reductions
+  double a9[9];
 #pragma unroll
-  for (int i = 0; i < 9; ++i) acc[i] = {0.0, 0.0};
+  for (int i = 0; i < 9; ++i) a9[i] = 0.0;
   for (int m = first; m < p.S; m += stride) {
     int rm[3];
     double r[3], dist;
@@ -259,11 +261,11 @@ __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart 
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       fp[d] = ((vp[d] + vr[d]) - ug[d]) * ph;
-      acc[d].add(fp[d]);
+      a9[d] += fp[d];
     }
-    acc[3].add(r[1] * fp[2] - r[2] * fp[1]);
-    acc[4].add(r[2] * fp[0] - r[0] * fp[2]);
-    acc[5].add(r[0] * fp[1] - r[1] * fp[0]);
+    a9[3] += r[1] * fp[2] - r[2] * fp[1];
+    a9[4] += r[2] * fp[0] - r[0] * fp[2];
+    a9[5] += r[0] * fp[1] - r[1] * fp[0];
   }
   if (p.lj_on) {
     int mc[3];
@@ -296,10 +298,13 @@ __global__ void __launch_bounds__(256) k_particles_hydro_velocity(PPar p, DPart 
         if (p.lj_powers >= 1) dmy = dmy * dmy;
         if (p.lj_powers >= 2) dmy = dmy * (s * s) * (s * s) * (s * s);
         const double f = p.lj_coeff / (rij * rij) * (2.0 * dmy * dmy - dmy);
-        for (int d = 0; d < 3; ++d) acc[6 + d].add((double)mult * (f * -x12[d]));
+        for (int d = 0; d < 3; ++d) a9[6 + d] += (double)mult * (f * -x12[d]);
       }
     }
   }
+  KSum acc[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) acc[i] = {a9[i], 0.0};
   block_reduce<9>(acc, sh);
   if (threadIdx.x == 0) {
     double *pp = partial + ((size_t)n * PCL + rank) * 18;

@@ -58,3 +58,18 @@ def plain_64_16() -> dict:
     eps = 1e-3
     g = 1e-3 / (4.0 / 3.0 * math.pi * 5.0 ** 3 * eps)
     return spm_config((6, 6, 6), 16, seed=1, kbt=0.0, gravity_g=g, mass_ratio=1.0 + eps, gravity_dir="-Z")
+
+
+def electrolyte_128_64() -> dict:
+    """128^3, 64 spheres a=5 with surface charge -100 in a monovalent salt
+    (Debye length 4, Bjerrum length 0.7 at kBT=1), external field 0.05 along x,
+    dt=0.01, positions from PCG64 seed 3."""
+    import math
+
+    cfg = spm_config((7, 7, 7), 64, seed=3, kbt=1.0)
+    cfg["eq"] = "Electrolyte"
+    cfg["alpha_v"] = 0.0
+    cfg["alpha_o"] = 0.0
+    cfg["electrolyte"] = dict(dielectric=1.0 / (4.0 * math.pi * 0.7), surface_charge=-100.0, debye=4.0,
+                              val_p=1.0, val_n=-1.0, onsager_p=1.0, onsager_n=1.0, efield=(0.05, 0.0, 0.0))
+    return cfg
