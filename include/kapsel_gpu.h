@@ -133,6 +133,23 @@ int kapsel_gpu_set_efield(kapsel_ctx *ctx, const double *e);
    the Concentration array of solute_rhs.cxx:16), Electrolyte only. */
 int kapsel_gpu_get_concentration(kapsel_ctx *ctx, double *conc);
 
+/* ---- Batched ensemble of independent boxes. ---- */
+
+/* Many independent boxes of any sizes advanced together, one CUDA graph
+   launch per step.  The reference runs each box as its own process (one
+   main() per UDF); boxes keep their own parameters, particles and thermostat
+   streams.  `boxes` must be initialised contexts at the same time step; the
+   batch does not own them.  With autotune != 0 the y-pass tile width is
+   chosen per box shape by timing both variants. */
+typedef struct kapsel_batch kapsel_batch;
+int kapsel_batch_create(kapsel_ctx *const *boxes, int n, int autotune, kapsel_batch **out);
+int kapsel_batch_step(kapsel_batch *b, int nsteps);
+/* Per-box mean-square displacement of the unwrapped positions x_nopbc since
+   kapsel_batch_create (the R_raw records of Output_udf, avs_output.cxx:361-363). */
+int kapsel_batch_msd(kapsel_batch *b, double *msd);
+int kapsel_batch_get_stream(kapsel_batch *b, void **stream);
+int kapsel_batch_destroy(kapsel_batch *b);
+
 /* ---- Routine-level entry points on host arrays (reference layouts). ---- */
 
 /* A2a_k / A_k2a (fft_wrapper.h:432-631): in-place forward / inverse 3D real

@@ -106,6 +106,12 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_calc_f_hydro": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP, _DP]),
         "kapsel_gpu_calc_fr": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+        "kapsel_batch_create": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.c_int, ctypes.c_int,
+                                               ctypes.POINTER(_VP)]),
+        "kapsel_batch_step": (ctypes.c_int, [_VP, ctypes.c_int]),
+        "kapsel_batch_msd": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_batch_get_stream": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+        "kapsel_batch_destroy": (ctypes.c_int, [_VP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -308,4 +314,47 @@ class Simulation:
         return f[: self.Np]
 
 
-__all__ = ["Simulation", "KapselError", "load_library", "params_from_config", "FP64", "MIXED", "LIB_PATH"]
+class Batch:
+    """Independent boxes advanced together, one CUDA graph launch per step
+    (kapsel_batch_*).  The Simulation objects stay owned by the caller."""
+
+    def __init__(self, sims, autotune: bool = True):
+        self.L = load_library()
+        self.sims = list(sims)
+        arr = (_VP * len(self.sims))(*[s.h for s in self.sims])
+        h = _VP()
+        rc = self.L.kapsel_batch_create(arr, len(self.sims), 1 if autotune else 0, ctypes.byref(h))
+        if rc != 0:
+            raise KapselError(f"kapsel_batch_create status {rc}: {self.L.kapsel_gpu_strerror(rc).decode()}")
+        self.h = h
+
+    def step(self, n: int = 1):
+        rc = self.L.kapsel_batch_step(self.h, int(n))
+        if rc != 0:
+            raise KapselError(f"kapsel_batch_step status {rc}: {self.L.kapsel_gpu_strerror(rc).decode()}")
+
+    def msd(self) -> np.ndarray:
+        out = np.zeros(len(self.sims))
+        rc = self.L.kapsel_batch_msd(self.h, _ptr(out))
+        if rc != 0:
+            raise KapselError(f"kapsel_batch_msd status {rc}")
+        return out
+
+    def stream(self) -> int:
+        sp = _VP()
+        self.L.kapsel_batch_get_stream(self.h, ctypes.byref(sp))
+        return sp.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.kapsel_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ = ["Batch", "Simulation", "KapselError", "load_library", "params_from_config", "FP64", "MIXED", "LIB_PATH"]

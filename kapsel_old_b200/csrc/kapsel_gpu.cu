@@ -152,6 +152,8 @@ struct BoxBase {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
 
   virtual int alloc() = 0;
+  virtual float time_ypass(int small, int reps) = 0;
+  virtual void set_ytile(int small) = 0;
   virtual int alloc_el() = 0;
   virtual int init_el() = 0;
   virtual int conc_to_host(double *c) = 0;
@@ -247,6 +249,8 @@ struct Box : BoxBase {
     KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xf));
     KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
     KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
+    KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
+    KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
     KCHECK(cudaFuncSetAttribute(k_z_products<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zp));
     KCHECK(cudaFuncSetAttribute(k_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
     KCHECK(cudaFuncSetAttribute(k_z_r2c_full<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zr));
@@ -261,19 +265,51 @@ struct Box : BoxBase {
 
   dim3 gx() const { return dim3(g.KYc, (g.TZ + KCX - 1) / KCX); }
   dim3 gy(int nc) const { return dim3(g.NX, nc, (g.TZ + KCY - 1) / KCY); }
+  // y-pass tile width: KCY, or KCY/2 when the autotuner found it faster for
+  // this box shape (kapsel_batch_create)
+  int ytile_small = 0;
+  template <bool INV>
+  void launch_y(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out) {
+    constexpr int K2 = KCY / 2;
+    const size_t sm = std::max(smem_y, sm_y_any);
+    if (ytile_small)
+      k_y_pass<R, INV, K2><<<dim3(g.NX, nc, (gg.TZ + K2 - 1) / K2), 256, sm, stream>>>(gg, tw, in, out);
+    else
+      k_y_pass<R, INV, KCY><<<dim3(g.NX, nc, (gg.TZ + KCY - 1) / KCY), 256, sm, stream>>>(gg, tw, in, out);
+  }
+  size_t sm_y_any = 0;
+  float time_ypass(int small, int reps) override {
+    const int keep = ytile_small;
+    ytile_small = small;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    launch_y<false>(g, 5, bufB, bufA);  // warm
+    cudaEventRecord(a, stream);
+    for (int r = 0; r < reps; ++r) launch_y<false>(g, 5, bufB, bufA);
+    cudaEventRecord(b, stream);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    ytile_small = keep;
+    return ms / reps;
+  }
+  void set_ytile(int small) override { ytile_small = small; }
   int gz() const { return (g.NX * g.NY) / ZROWS; }
 
   // zeta -> u* (real) through launches 1,2,(7); used by the velocity readout
   void launch_zeta_to_real(R *out, size_t cstride, int pitch) {
     k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
-    k_y_pass<R, true, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB);
+    launch_y<true>(g, 3, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, out, cstride, pitch);
   }
 
   // f (from phi/up and u*) -> zeta update, launches 11-13
   void launch_force_to_zeta() {
     k_z_force<R><<<gz(), 256, smem_zf, stream>>>(g, tw, phiup, ustar, bufB);
-    k_y_pass<R, false, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufB, bufA);
+    launch_y<false>(g, 3, bufB, bufA);
     k_x_force_to_zeta<R, KCX><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc);
   }
 
@@ -289,15 +325,15 @@ struct Box : BoxBase {
     mark();
     k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
     mark();
-    k_y_pass<R, true, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB);
+    launch_y<true>(g, 3, bufA, bufB);
     mark();
     k_z_products<R><<<gz(), 256, smem_zp, stream>>>(g, tw, bufB);
     mark();
-    k_y_pass<R, false, KCY><<<gy(5), 256, smem_y, stream>>>(g, tw, bufB, bufA);
+    launch_y<false>(g, 5, bufB, bufA);
     mark();
     k_x_advect_update<R, KCX><<<gx(), 256, smem_xadv, stream>>>(g, tw, bufA, zeta, uk_dc);
     mark();
-    k_y_pass<R, true, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB);
+    launch_y<true>(g, 3, bufA, bufB);
     mark();
     k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, npts(), g.NZ);
     mark();
@@ -311,7 +347,7 @@ struct Box : BoxBase {
       mark();
       k_z_force<R><<<gz(), 256, smem_zf, stream>>>(g, tw, phiup, ustar, bufB);
       mark();
-      k_y_pass<R, false, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufB, bufA);
+      launch_y<false>(g, 3, bufB, bufA);
       mark();
       k_x_force_to_zeta<R, KCX><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc);
       mark();
@@ -380,6 +416,7 @@ struct Box : BoxBase {
     const size_t zr = C * (g.M + g.NZ + (size_t)g.M * (ZROWS + 1) + std::max((size_t)g.M * ZROWS, (size_t)ZROWS * (g.M + 2)));
     sm_el = std::max(std::max(xi, xf), std::max(zr, smem_zc));
     sm_el = std::max(sm_el, smem_y);
+    sm_y_any = sm_el;
     if (sm_el > 227 * 1024) return KAPSEL_ERANGE;
     const int sm = (int)sm_el;
     KCHECK(cudaFuncSetAttribute(k_x_inv_op<R, KCX, XI_IDENT, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
@@ -393,6 +430,8 @@ struct Box : BoxBase {
     KCHECK(cudaFuncSetAttribute(k_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_xadv));
     return 0;
@@ -407,7 +446,7 @@ struct Box : BoxBase {
   void el_conc_real() {
     const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
     k_x_inv_op<R, KCX, XI_IDENT, 2, 2><<<gx(), 256, sm_el, stream>>>(g, tw, conc_k, nz, bufA, KOp{});
-    k_y_pass<R, true, KCY><<<gy(2), 256, sm_el, stream>>>(g, tw, bufA, bufB);
+    launch_y<true>(g, 2, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 2), 256, sm_el, stream>>>(g, tw, bufB, creal, npts(), g.NZ);
   }
   // surface-charge scale s0 = sum|Z_e| / (sum|surf| DX3) (operate_electrolyte.cxx:217-241)
@@ -423,11 +462,11 @@ struct Box : BoxBase {
   // forward transform of ncomp real fields, 2/3 modes kept, into bufA (I1 layout)
   void el_forward_trunc(const R *real, int ncomp) {
     k_z_r2c<R><<<dim3(gz(), ncomp), 256, sm_el, stream>>>(g, tw, real, g.NZ, npts(), bufB, g.TZ);
-    k_y_pass<R, false, KCY><<<gy(ncomp), 256, sm_el, stream>>>(g, tw, bufB, bufA);
+    launch_y<false>(g, ncomp, bufB, bufA);
   }
   // inverse of three I1-layout components in bufA into real fields
   void el_inverse3(R *out) {
-    k_y_pass<R, true, KCY><<<gy(3), 256, sm_el, stream>>>(g, tw, bufA, bufB);
+    launch_y<true>(g, 3, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(g, tw, bufB, out, npts(), g.NZ);
   }
 
@@ -449,10 +488,10 @@ struct Box : BoxBase {
     el_inverse3(gradr);
     // Rhs_NS_solute: u, the advection term and the explicit Euler update of zeta
     k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
-    k_y_pass<R, true, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB);
+    launch_y<true>(g, 3, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(g, tw, bufB, ureal, N, g.NZ);
     k_z_products<R><<<gz(), 256, smem_zp, stream>>>(g, tw, bufB);
-    k_y_pass<R, false, KCY><<<gy(5), 256, smem_y, stream>>>(g, tw, bufB, bufA);
+    launch_y<false>(g, 5, bufB, bufA);
     k_x_advect_update<R, KCX, 1><<<gx(), 256, smem_xadv, stream>>>(g, tw, bufA, zeta, uk_dc);
     // ion fluxes and the Euler update of each concentration
     for (int n = 0; n < 2; ++n) {
@@ -476,12 +515,12 @@ struct Box : BoxBase {
     // full (untruncated) potential gradient with the Ooura inverse semantics
     const size_t nfull = (size_t)g.NX * g.NY * (g.M + 1);
     k_z_r2c<R><<<dim3(gz(), 1), 256, sm_el, stream>>>(gF, tw, charge, g.NZ, N, F2, g.M + 1);
-    k_y_pass<R, false, KCY><<<gyF(1), 256, sm_el, stream>>>(gF, tw, F2, F1);
+    launch_y<false>(gF, 1, F2, F1);
     k_x_fwd_op<R, KCX, XF_GRADPSI_FULL, 1><<<gxF(), 256, sm_el, stream>>>(gF, tw, F1, F2, nfull,
                                                                              KOp{ieps, {0, 0, 0}});
     k_hermitian_planes<R><<<pb, 256, 0, stream>>>(gF, F2, 3);
     k_x_inv_op<R, KCX, XI_IDENT, 3, 3><<<gxF(), 256, sm_el, stream>>>(gF, tw, F2, nfull, F1, KOp{});
-    k_y_pass<R, true, KCY><<<gyF(3), 256, sm_el, stream>>>(gF, tw, F1, F2);
+    launch_y<true>(gF, 3, F1, F2);
     k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(gF, tw, F2, gradr, N, g.NZ);
     const bool ext = ext_on();
     k_el_coulomb<R><<<pb, 256, 0, stream>>>(N, charge, gradr, ext ? prm.e_ext[0] : 0.0, ext ? prm.e_ext[1] : 0.0,
@@ -491,7 +530,7 @@ struct Box : BoxBase {
     k_x_force_to_zeta<R, KCX><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc);
     // u (real) of the updated zeta, then the particle part of the step
     k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
-    k_y_pass<R, true, KCY><<<gy(3), 256, smem_y, stream>>>(g, tw, bufA, bufB);
+    launch_y<true>(g, 3, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, N, g.NZ);
     if (Np > 0) {
       k_particles_hydro_velocity<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, ustar, cells, nullptr, euler, status,
@@ -1517,6 +1556,173 @@ int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms) {
     if (cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]) != cudaSuccess) return KAPSEL_ECUDA;
   for (int i = 0; i <= KAPSEL_N_STEP_KERNELS; ++i) cudaEventDestroy(ev[i]);
   return check_status(b);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched ensemble: independent boxes advanced together, one CUDA graph
+// launch per step.  The graph forks from a root stream to every box's stream,
+// runs each box's step sequence as a parallel branch, and joins back.
+struct kapsel_batch {
+  std::vector<kapsel_ctx *> boxes;
+  cudaStream_t root = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaEvent_t fork = nullptr, done = nullptr;
+  std::vector<cudaEvent_t> ready, join;
+  std::vector<std::vector<double>> x0;
+};
+
+extern "C" {
+
+int kapsel_batch_create(kapsel_ctx *const *boxes, int n, int autotune, kapsel_batch **out) {
+  if (!boxes || n <= 0 || !out) return KAPSEL_EINVAL;
+  *out = nullptr;
+  std::unique_ptr<kapsel_batch> b(new (std::nothrow) kapsel_batch);
+  if (!b) return KAPSEL_ENOMEM;
+  const int ts0 = boxes[0]->box->ts;
+  for (int i = 0; i < n; ++i) {
+    if (!boxes[i] || !boxes[i]->box->initialised || boxes[i]->box->ts != ts0) return KAPSEL_ESTATE;
+    b->boxes.push_back(boxes[i]);
+  }
+  if (cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking) != cudaSuccess) return KAPSEL_ECUDA;
+  if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) return KAPSEL_ECUDA;
+  if (cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) return KAPSEL_ECUDA;
+  b->ready.resize(n);
+  b->join.resize(n);
+  for (int i = 0; i < n; ++i) {
+    if (cudaEventCreateWithFlags(&b->ready[i], cudaEventDisableTiming) != cudaSuccess) return KAPSEL_ECUDA;
+    if (cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) != cudaSuccess) return KAPSEL_ECUDA;
+  }
+  // autotune: the y-pass tile width per box shape, by timing both variants
+  if (autotune) {
+    std::vector<std::pair<std::vector<int>, int>> chosen;
+    for (int i = 0; i < n; ++i) {
+      BoxBase *x = b->boxes[i]->box.get();
+      std::vector<int> key = {x->g.NX, x->g.NY, x->g.NZ, x->prm.precision};
+      int pick = -1;
+      for (auto &c : chosen)
+        if (c.first == key) pick = c.second;
+      if (pick < 0) {
+        const float t0 = x->time_ypass(0, 10), t1 = x->time_ypass(1, 10);
+        pick = t1 < t0 ? 1 : 0;
+        chosen.push_back({key, pick});
+      }
+      x->set_ytile(pick);
+    }
+  }
+  // initial unwrapped positions for the mean-square displacement
+  for (int i = 0; i < n; ++i) {
+    BoxBase *x = b->boxes[i]->box.get();
+    std::vector<double> rec((size_t)KAPSEL_P_STRIDE * std::max(x->Np, 1));
+    int rc = kapsel_gpu_get_particles(b->boxes[i], rec.data());
+    if (rc) return rc;
+    std::vector<double> p0(3 * (size_t)x->Np);
+    for (int m = 0; m < x->Np; ++m)
+      for (int d = 0; d < 3; ++d) p0[3 * m + d] = rec[(size_t)KAPSEL_P_STRIDE * m + KAPSEL_P_XNOPBC + d];
+    b->x0.push_back(p0);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return KAPSEL_ECUDA;
+  *out = b.release();
+  return 0;
+}
+
+int kapsel_batch_step(kapsel_batch *b, int nsteps) {
+  if (!b || nsteps < 0) return KAPSEL_EINVAL;
+  const int n = (int)b->boxes.size();
+  for (int s = 0; s < nsteps; ++s) {
+    BoxBase *first = b->boxes[0]->box.get();
+    const int slot = first->ts & 1;
+    const int euler = first->ts == 0 ? 1 : 0;
+    for (int i = 0; i < n; ++i) {
+      BoxBase *x = b->boxes[i]->box.get();
+      int rc = x->fill_noise(slot);
+      if (rc) return rc;
+    }
+    if (euler) {
+      for (int i = 0; i < n; ++i) {
+        BoxBase *x = b->boxes[i]->box.get();
+        x->launch_step(x->noise_dev[slot], 1);
+      }
+    } else {
+      if (!b->graph[slot]) {
+        cudaGraph_t gr;
+        if (cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return KAPSEL_ECUDA;
+        cudaEventRecord(b->fork, b->root);
+        for (int i = 0; i < n; ++i) {
+          BoxBase *x = b->boxes[i]->box.get();
+          cudaStreamWaitEvent(x->stream, b->fork, 0);
+          x->launch_step(x->noise_dev[slot], 0);
+          cudaEventRecord(b->join[i], x->stream);
+          cudaStreamWaitEvent(b->root, b->join[i], 0);
+        }
+        if (cudaStreamEndCapture(b->root, &gr) != cudaSuccess) return KAPSEL_ECUDA;
+        if (cudaGraphInstantiate(&b->graph[slot], gr, 0) != cudaSuccess) return KAPSEL_ECUDA;
+        cudaGraphDestroy(gr);
+      }
+      // the graph reads each box's freshly copied noise: wait for the copies
+      for (int i = 0; i < n; ++i) {
+        BoxBase *x = b->boxes[i]->box.get();
+        cudaEventRecord(b->ready[i], x->stream);
+        cudaStreamWaitEvent(b->root, b->ready[i], 0);
+      }
+      if (cudaGraphLaunch(b->graph[slot], b->root) != cudaSuccess) return KAPSEL_ECUDA;
+      // later work on the box streams (the next noise copies) follows the graph
+      cudaEventRecord(b->done, b->root);
+      for (int i = 0; i < n; ++i) cudaStreamWaitEvent(b->boxes[i]->box->stream, b->done, 0);
+    }
+    for (int i = 0; i < n; ++i) {
+      BoxBase *x = b->boxes[i]->box.get();
+      x->ts += 1;
+      x->time += x->prm.dt;
+    }
+  }
+  if (cudaStreamSynchronize(b->root) != cudaSuccess) return KAPSEL_ECUDA;
+  for (int i = 0; i < n; ++i) {
+    int rc = check_status(b->boxes[i]->box.get());
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int kapsel_batch_msd(kapsel_batch *b, double *msd) {
+  // mean over the particles of each box of |x_nopbc(t) - x_nopbc(t0)|^2
+  // (the unwrapped R_raw of Output_udf, avs_output.cxx:361-363)
+  if (!b || !msd) return KAPSEL_EINVAL;
+  for (size_t i = 0; i < b->boxes.size(); ++i) {
+    BoxBase *x = b->boxes[i]->box.get();
+    std::vector<double> rec((size_t)KAPSEL_P_STRIDE * std::max(x->Np, 1));
+    int rc = kapsel_gpu_get_particles(b->boxes[i], rec.data());
+    if (rc) return rc;
+    double acc = 0.0;
+    for (int m = 0; m < x->Np; ++m)
+      for (int d = 0; d < 3; ++d) {
+        const double dd = rec[(size_t)KAPSEL_P_STRIDE * m + KAPSEL_P_XNOPBC + d] - b->x0[i][3 * m + d];
+        acc += dd * dd;
+      }
+    msd[i] = x->Np > 0 ? acc / x->Np : 0.0;
+  }
+  return 0;
+}
+
+int kapsel_batch_get_stream(kapsel_batch *b, void **stream) {
+  if (!b || !stream) return KAPSEL_EINVAL;
+  *stream = (void *)b->root;
+  return 0;
+}
+
+int kapsel_batch_destroy(kapsel_batch *b) {
+  if (!b) return KAPSEL_EINVAL;
+  cudaStreamSynchronize(b->root);
+  for (int s = 0; s < 2; ++s)
+    if (b->graph[s]) cudaGraphExecDestroy(b->graph[s]);
+  for (auto e : b->ready) cudaEventDestroy(e);
+  for (auto e : b->join) cudaEventDestroy(e);
+  cudaEventDestroy(b->fork);
+  cudaEventDestroy(b->done);
+  cudaStreamDestroy(b->root);
+  delete b;
+  return 0;
 }
 
 }  // extern "C"

@@ -73,3 +73,26 @@ def electrolyte_128_64() -> dict:
     cfg["electrolyte"] = dict(dielectric=1.0 / (4.0 * math.pi * 0.7), surface_charge=-100.0, debye=4.0,
                               val_p=1.0, val_n=-1.0, onsager_p=1.0, onsager_n=1.0, efield=(0.05, 0.0, 0.0))
     return cfg
+
+
+BATCH_SHAPES = [(5, 5, 5), (6, 6, 6), (6, 6, 7), (7, 7, 7)]  # 32^3, 64^3, 64x64x128, 128^3
+
+
+def batched(n_boxes: int = 48, seed: int = 4, max_fill: float = 0.2) -> list:
+    """n_boxes independent boxes with shapes drawn from 32^3, 64^3, 64x64x128
+    and 128^3, 1-64 spheres each (capped so that the solid volume fraction
+    stays below max_fill; a small box cannot hold 64 spheres), radius a drawn
+    from [4, 6], xi=2, kBT=1e-3, all from one PCG64(seed) stream."""
+    import math
+
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for b in range(n_boxes):
+        shape = BATCH_SHAPES[int(rng.integers(len(BATCH_SHAPES)))]
+        a = float(np.round(rng.uniform(4.0, 6.0), 3))
+        vol = float(np.prod([1 << p for p in shape]))
+        cap = max(1, int(max_fill * vol / (4.0 / 3.0 * math.pi * a ** 3)))
+        n = int(rng.integers(1, 65))
+        n = min(n, cap)
+        out.append(spm_config(shape, n, seed=1000 * seed + b, a=a, kbt=1e-3))
+    return out
