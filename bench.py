@@ -110,6 +110,23 @@ def step_bytes_model(cfg, R: int):
     return passes * N * R, passes
 
 
+def reduce_max(value: float, dist=None, device="cuda") -> float:
+    """Max over ranks of a per-rank timing (the whole-job time of replicas)."""
+    if dist is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank: int, world: int, max_seconds: float) -> float:
+    """Whole-job throughput of independent replicas: all ranks' units over the
+    slowest rank's time."""
+    return units_per_rank * world / max_seconds
+
+
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -197,11 +214,7 @@ def run_ours(args, rank, world, local_rank):
             sim._check(L.kapsel_gpu_step_graph(sim.h, 1))
             evs[k][1].record(stream)
         torch.cuda.synchronize()
-        ms = sum(a.elapsed_time(b) for a, b in evs)
-        if dist:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = reduce_max(sum(a.elapsed_time(b) for a, b in evs), dist)
         return sim, stream, ms
 
     # ---- mixed precision (headline) with clocks sampled during the timed region
@@ -243,11 +256,7 @@ def run_ours(args, rank, world, local_rank):
         sim_m._check(L.kapsel_gpu_step_graph(sim_m.h, 1))
         sim_m._check(L.kapsel_gpu_get_particles(sim_m.h, rec.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = reduce_max(time.perf_counter() - t0, dist)
     sim_m.close()
 
     # ---- the other workloads, same timing rules, fewer steps
@@ -288,10 +297,7 @@ def run_ours(args, rank, world, local_rank):
             e1.record(bstream)
             torch.cuda.synchronize()
             bms += e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([bms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            bms = float(t.item())
+        bms = reduce_max(bms, dist)
         msd = batch.msd()
         batch.close()
         for sm_ in sims:
@@ -309,8 +315,8 @@ def run_ours(args, rank, world, local_rank):
             extra["electrolyte_128cubed_64"]["cpu_baseline"] = cpu_baseline(c3, warmup=1, steps=4)
 
     steps_total = args.steps * world
-    value = steps_total / (ms_m * 1e-3)
-    fp64_value = steps_total / (ms_d * 1e-3)
+    value = replica_value(args.steps, world, ms_m * 1e-3)
+    fp64_value = replica_value(args.steps, world, ms_d * 1e-3)
     bstep, passes = step_bytes_model(cfg, 4)
     line = {
         "metric": METRIC,
