@@ -206,7 +206,9 @@ int kapsel_sekibun_cells(double a, double a_xi, double dx, int *out, int cap);
 
 /* ---- Measurement hooks. ---- */
 
-/* Number of kernel launches of one step (and its upper bound). */
+/* Number of kernel launches of one step, counted from a capture of the step
+   (nothing is executed); KAPSEL_N_STEP_KERNELS is the number of timing slots
+   of kapsel_gpu_profile_step. */
 #define KAPSEL_N_STEP_KERNELS 13
 int kapsel_gpu_launches_per_step(kapsel_ctx *ctx);
 const char *kapsel_gpu_kernel_name(int i);

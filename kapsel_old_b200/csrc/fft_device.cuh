@@ -118,6 +118,15 @@ __device__ __forceinline__ void cp_async_cx(Cx<R> *smem, const Cx<R> *gmem) {
     cp_async_8(smem, gmem);
 }
 
+// Programmatic dependent launch: let the next kernel of the stream start its
+// launch now, then wait until the previous kernel has finished and its
+// writes are visible.  Both are no-ops when the kernel was launched without
+// the programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // Cooperative copy of a twiddle table (n entries) into shared memory.
 template <typename R>
 __device__ __forceinline__ void load_twiddles(Cx<R> *dst, const Cx<R> *src, int n) {

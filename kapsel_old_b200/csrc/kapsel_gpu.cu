@@ -2,7 +2,8 @@
 // sequence, CUDA graph replay and the C ABI declared in include/kapsel_gpu.h.
 //
 // One SPM step (Time_evolution_hydro, sp_3d_ns.cxx:61-212, Navier_Stokes
-// branch) is 13 launches:
+// branch) is 12 launches (13 kernels; 8 runs in extra blocks of 7), each
+// after the first launched with programmatic stream serialization:
 //   1 k_x_zeta_to_u        truncated zeta -> u_k -> inverse x
 //   2 k_y_pass<inv>        inverse y (3 comps)
 //   3 k_z_products         inverse z, 5 products, forward z
@@ -10,7 +11,7 @@
 //   5 k_x_advect_update    forward x, Omega, slaved Euler, FIX_CELL, u*_k, inverse x
 //   6 k_y_pass<inv>        inverse y (3 comps)
 //   7 k_z_c2r              inverse z -> u* (real)
-//   8 k_particles_position AB2 / Euler positions and orientations
+//   8 (k_z_c2r blocks)     AB2 / Euler positions and orientations
 //   9 k_particles_hydro_velocity  hydro force+torque gather, LJ, gravity, velocity, thermostat
 //  10 k_particles_scatter  phi, phi*u_p
 //  11 k_z_force            clamp, f = up - phi u*, forward z, clear phi/up
@@ -126,6 +127,28 @@ __global__ void k_col_pass(Geo g, const Cx<R> *twn, int logn, int n, const Cx<R>
                            long long line_stride, long long elem_stride, int nlines);
 template <typename R>
 __global__ void k_z_c2r_full(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in, R *__restrict__ out, double scale);
+
+// Kernel launch on `st`, optionally with programmatic stream serialization
+// (the kernel may start while its predecessor drains; it waits in pdl_begin).
+template <typename... KArgs, typename... Args>
+void launch_k(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+              Args... args) {
+  if (!pdl) {
+    kern<<<grid, block, smem, st>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, args...);
+}
 
 // ---------------------------------------------------------------------------
 struct BoxBase {
@@ -268,14 +291,17 @@ struct Box : BoxBase {
   // y-pass tile width: KCY, or KCY/2 when the autotuner found it faster for
   // this box shape (kapsel_batch_create)
   int ytile_small = 0;
+  bool use_pdl = true;
   template <bool INV>
-  void launch_y(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out) {
+  void launch_y(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out, bool pdl = false) {
     constexpr int K2 = KCY / 2;
     const size_t sm = std::max(smem_y, sm_y_any);
     if (ytile_small)
-      k_y_pass<R, INV, K2><<<dim3(g.NX, nc, (gg.TZ + K2 - 1) / K2), 256, sm, stream>>>(gg, tw, in, out);
+      launch_k(pdl, k_y_pass<R, INV, K2>, dim3(g.NX, nc, (gg.TZ + K2 - 1) / K2), dim3(256), sm, stream, gg, tw, in,
+               out);
     else
-      k_y_pass<R, INV, KCY><<<dim3(g.NX, nc, (gg.TZ + KCY - 1) / KCY), 256, sm, stream>>>(gg, tw, in, out);
+      launch_k(pdl, k_y_pass<R, INV, KCY>, dim3(g.NX, nc, (gg.TZ + KCY - 1) / KCY), dim3(256), sm, stream, gg, tw,
+               in, out);
   }
   size_t sm_y_any = 0;
   float time_ypass(int small, int reps) override {
@@ -303,7 +329,7 @@ struct Box : BoxBase {
   void launch_zeta_to_real(R *out, size_t cstride, int pitch) {
     k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
     launch_y<true>(g, 3, bufA, bufB);
-    k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, out, cstride, pitch);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, out, cstride, pitch, PPar{}, nullptr, 0, nullptr);
   }
 
   // f (from phi/up and u*) -> zeta update, launches 11-13
@@ -322,34 +348,43 @@ struct Box : BoxBase {
     auto mark = [&]() {
       if (ev) cudaEventRecord(ev[e++], stream);
     };
+    const bool pdl = use_pdl && !ev;  // events between launches break the programmatic chain
+    const Cx<R> *czeta = zeta;
     mark();
-    k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
+    k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, czeta, (const double *)uk_dc, bufA);
     mark();
-    launch_y<true>(g, 3, bufA, bufB);
+    launch_y<true>(g, 3, bufA, bufB, pdl);
     mark();
-    k_z_products<R><<<gz(), 256, smem_zp, stream>>>(g, tw, bufB);
+    launch_k(pdl, k_z_products<R>, dim3(gz()), dim3(256), smem_zp, stream, g, tw, bufB);
     mark();
-    launch_y<false>(g, 5, bufB, bufA);
+    launch_y<false>(g, 5, bufB, bufA, pdl);
     mark();
-    k_x_advect_update<R, KCX><<<gx(), 256, smem_xadv, stream>>>(g, tw, bufA, zeta, uk_dc);
+    launch_k(pdl, k_x_advect_update<R, KCX, 0>, gx(), dim3(256), smem_xadv, stream, g, tw, bufA, zeta, uk_dc);
     mark();
-    launch_y<true>(g, 3, bufA, bufB);
+    launch_y<true>(g, 3, bufA, bufB, pdl);
     mark();
-    k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, npts(), g.NZ);
+    // u* and, in extra blocks, the particle positions (a launch of their own
+    // when profiling, so that each launch is timed separately)
+    const bool fuse_pos = Np > 0 && !ev;
+    const int posblk = fuse_pos ? (Np + 255) / 256 : 0;
+    launch_k(pdl, k_z_c2r<R>, dim3(gz() + posblk, 3), dim3(256), smem_zc, stream, g, tw, (const Cx<R> *)bufB, ustar,
+             npts(), g.NZ, pp, fuse_pos ? parts : (DPart *)nullptr, euler, status);
     mark();
     if (Np > 0) {
-      k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
+      if (!fuse_pos) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
       mark();
-      k_particles_hydro_velocity<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, ustar, cells, noise, euler, status,
-                                                                    partial_p, arrivals);
+      launch_k(pdl, k_particles_hydro_velocity<R>, dim3(Np * PCL), dim3(256), 0, stream, pp, parts,
+               (const R *)ustar, (const int *)cells, noise, euler, status, partial_p, arrivals);
       mark();
-      k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup);
+      launch_k(pdl, k_particles_scatter<R>, dim3(Np * PCL), dim3(256), 0, stream, pp, (const DPart *)parts,
+               (const int *)cells, phiup);
       mark();
-      k_z_force<R><<<gz(), 256, smem_zf, stream>>>(g, tw, phiup, ustar, bufB);
+      launch_k(pdl, k_z_force<R>, dim3(gz()), dim3(256), smem_zf, stream, g, tw, phiup, (const R *)ustar, bufB);
       mark();
-      launch_y<false>(g, 3, bufB, bufA);
+      launch_y<false>(g, 3, bufB, bufA, pdl);
       mark();
-      k_x_force_to_zeta<R, KCX><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc);
+      launch_k(pdl, k_x_force_to_zeta<R, KCX>, gx(), dim3(256), smem_xf, stream, g, tw, (const Cx<R> *)bufA, zeta,
+               uk_dc);
       mark();
     }
   }
@@ -447,7 +482,7 @@ struct Box : BoxBase {
     const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
     k_x_inv_op<R, KCX, XI_IDENT, 2, 2><<<gx(), 256, sm_el, stream>>>(g, tw, conc_k, nz, bufA, KOp{});
     launch_y<true>(g, 2, bufA, bufB);
-    k_z_c2r<R><<<dim3(gz(), 2), 256, sm_el, stream>>>(g, tw, bufB, creal, npts(), g.NZ);
+    k_z_c2r<R><<<dim3(gz(), 2), 256, sm_el, stream>>>(g, tw, bufB, creal, npts(), g.NZ, PPar{}, nullptr, 0, nullptr);
   }
   // surface-charge scale s0 = sum|Z_e| / (sum|surf| DX3) (operate_electrolyte.cxx:217-241)
   void el_surface_scale() {
@@ -467,7 +502,7 @@ struct Box : BoxBase {
   // inverse of three I1-layout components in bufA into real fields
   void el_inverse3(R *out) {
     launch_y<true>(g, 3, bufA, bufB);
-    k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(g, tw, bufB, out, npts(), g.NZ);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(g, tw, bufB, out, npts(), g.NZ, PPar{}, nullptr, 0, nullptr);
   }
 
   void launch_step_el(int euler) {
@@ -489,7 +524,7 @@ struct Box : BoxBase {
     // Rhs_NS_solute: u, the advection term and the explicit Euler update of zeta
     k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
     launch_y<true>(g, 3, bufA, bufB);
-    k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(g, tw, bufB, ureal, N, g.NZ);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(g, tw, bufB, ureal, N, g.NZ, PPar{}, nullptr, 0, nullptr);
     k_z_products<R><<<gz(), 256, smem_zp, stream>>>(g, tw, bufB);
     launch_y<false>(g, 5, bufB, bufA);
     k_x_advect_update<R, KCX, 1><<<gx(), 256, smem_xadv, stream>>>(g, tw, bufA, zeta, uk_dc);
@@ -521,7 +556,7 @@ struct Box : BoxBase {
     k_hermitian_planes<R><<<pb, 256, 0, stream>>>(gF, F2, 3);
     k_x_inv_op<R, KCX, XI_IDENT, 3, 3><<<gxF(), 256, sm_el, stream>>>(gF, tw, F2, nfull, F1, KOp{});
     launch_y<true>(gF, 3, F1, F2);
-    k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(gF, tw, F2, gradr, N, g.NZ);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(gF, tw, F2, gradr, N, g.NZ, PPar{}, nullptr, 0, nullptr);
     const bool ext = ext_on();
     k_el_coulomb<R><<<pb, 256, 0, stream>>>(N, charge, gradr, ext ? prm.e_ext[0] : 0.0, ext ? prm.e_ext[1] : 0.0,
                                             ext ? prm.e_ext[2] : 0.0, prm.dt / prm.rho, fluxr);
@@ -531,7 +566,7 @@ struct Box : BoxBase {
     // u (real) of the updated zeta, then the particle part of the step
     k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
     launch_y<true>(g, 3, bufA, bufB);
-    k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, N, g.NZ);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, N, g.NZ, PPar{}, nullptr, 0, nullptr);
     if (Np > 0) {
       k_particles_hydro_velocity<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, ustar, cells, nullptr, euler, status,
                                                                   partial_p, arrivals);
@@ -1524,7 +1559,25 @@ int kapsel_gpu_get_stream(kapsel_ctx *ctx, void **stream) {
 
 int kapsel_gpu_launches_per_step(kapsel_ctx *ctx) {
   if (!ctx) return KAPSEL_EINVAL;
-  return ctx->box->Np > 0 ? KAPSEL_N_STEP_KERNELS : 7;
+  // Counted, not assumed: capture one step into a throwaway graph (nothing
+  // runs) and count its kernel nodes.
+  BoxBase *b = ctx->box.get();
+  if (!b->initialised) return KAPSEL_ESTATE;
+  cudaGraph_t gr = nullptr;
+  if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return KAPSEL_ECUDA;
+  b->launch_step(b->noise_dev[0], 0);
+  if (cudaStreamEndCapture(b->stream, &gr) != cudaSuccess || !gr) return KAPSEL_ECUDA;
+  size_t nn = 0;
+  cudaGraphGetNodes(gr, nullptr, &nn);
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn) cudaGraphGetNodes(gr, nodes.data(), &nn);
+  int nk = 0;
+  for (size_t i = 0; i < nn; ++i) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nk;
+  }
+  cudaGraphDestroy(gr);
+  return nk;
 }
 
 const char *kapsel_gpu_kernel_name(int i) {

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include "fft_device.cuh"
+
 namespace kapsel {
 
 // One particle (the subset of Particle, variable.h:27-75, the step uses).
@@ -130,9 +132,8 @@ __device__ __forceinline__ void qnormalize(double *q) {
 // MD_solver_position_Euler / _AB2 (particle_solver.cxx:36-88), PBC
 // (periodic_boundary.h:9-15), MD_solver_orientation_Euler / _AB2
 // (particle_rotation_solver.h:15-39).  One thread per particle.
-__global__ void k_particles_position(PPar p, DPart *__restrict__ parts, int euler, int *__restrict__ status) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= p.Np) return;
+__device__ __forceinline__ void position_update_one(const PPar &p, DPart *__restrict__ parts, int n, int euler,
+                                                    int *__restrict__ status) {
   DPart &a = parts[n];
   const double hdt = 0.5 * p.dt;
   for (int d = 0; d < 3; ++d) {
@@ -161,6 +162,12 @@ __global__ void k_particles_position(PPar p, DPart *__restrict__ parts, int eule
     }
     qnormalize(a.q);
   }
+}
+
+
+__global__ void k_particles_position(PPar p, DPart *__restrict__ parts, int euler, int *__restrict__ status) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < p.Np) position_update_one(p, parts, n, euler, status);
 }
 
 // Block reduction of NV compensated sums; result valid in thread 0.  Warps
@@ -228,6 +235,7 @@ __global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPa
                                                                   int *__restrict__ arrivals) {
   __shared__ double sh[2 * 9 * 32];
   __shared__ int last;
+  pdl_begin();
   const int n = blockIdx.x / PCL;
   const int rank = blockIdx.x % PCL;
   const int stride = PCL * blockDim.x;
@@ -369,6 +377,7 @@ __global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPa
 template <typename R>
 __global__ void __launch_bounds__(256) k_particles_scatter(PPar p, const DPart *__restrict__ parts,
                                                            const int *__restrict__ cells, R *__restrict__ phiup) {
+  pdl_begin();
   const int n = blockIdx.x / PCL;
   const int stride = PCL * blockDim.x;
   const int first = (blockIdx.x % PCL) * blockDim.x + threadIdx.x;

@@ -15,6 +15,7 @@
 #pragma once
 
 #include "fft_device.cuh"
+#include "particle_kernels.cuh"
 #include "rfft_device.cuh"
 
 namespace kapsel {
@@ -93,6 +94,7 @@ template <typename R, int KC>
 __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ zeta,
                                                      const double *__restrict__ uk_dc, Cx<R> *__restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_begin();
   constexpr int W = 3 * KC;
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *Zt = twx + g.NX;          // [2][KXc][KC] staged zeta tile
@@ -151,6 +153,7 @@ template <typename R, bool INVERSE, int KC>
 __global__ void __launch_bounds__(256, 3) k_y_pass(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
                                                 Cx<R> *__restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_begin();
   Cx<R> *twy = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *Y = twy + g.NY;      // [NY rows][KC]
   Cx<R> *scr = Y + g.NY * KC;  // FFT scratch
@@ -227,6 +230,7 @@ constexpr int ZROWS = 8;
 template <typename R>
 __global__ void __launch_bounds__(256) k_z_products(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_begin();
   const int M = g.M;
   constexpr int NV = ZROWS * 3, NQ = ZROWS * 5;
   constexpr int EV = NV + 1, EQ = NQ + 1;  // odd element strides: conflict-free columns
@@ -286,10 +290,22 @@ __global__ void __launch_bounds__(256) k_z_products(Geo g, Twiddles<R> tw, Cx<R>
 
 // z pass, inverse to real space: in I2 [c][NX][NY][TZ], out real [c][rows][pitch]
 // scaled by 1/(NX NY NZ).  grid (NX*NY/ZROWS, ncomp).
+// Blocks past the row blocks (blockIdx.y == 0 only) run the particle position
+// update of the step (MD_solver_position_Euler / _AB2), which needs no field
+// and must finish before the hydrodynamic gather, as u* must: one launch
+// serves both.
 template <typename R>
 __global__ void __launch_bounds__(256) k_z_c2r(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
-                                               R *__restrict__ out, size_t out_cstride, int out_pitch) {
+                                               R *__restrict__ out, size_t out_cstride, int out_pitch, PPar pp,
+                                               DPart *__restrict__ parts, int euler, int *__restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_begin();
+  const int nrow_blocks = (g.NX * g.NY) / ZROWS;
+  if ((int)blockIdx.x >= nrow_blocks) {
+    const int n = ((int)blockIdx.x - nrow_blocks) * blockDim.x + threadIdx.x;
+    if (blockIdx.y == 0 && parts && n < pp.Np) position_update_one(pp, parts, n, euler, status);
+    return;
+  }
   const int M = g.M;
   constexpr int ES = ZROWS + 1;
   Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
@@ -336,6 +352,7 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_z_force(Geo g, Twiddles<R> tw, R *__restrict__ phiup,
                                                  const R *__restrict__ ustar, Cx<R> *__restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_begin();
   const int M = g.M;
   constexpr int NS = ZROWS * 3, ES = NS + 1;
   Cx<R> *twm = reinterpret_cast<Cx<R> *>(smem_raw);
@@ -441,6 +458,7 @@ template <typename R, int KC, int EULER = 0>
 __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ buf,
                                                          Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_begin();
   constexpr int W5 = 5 * KC, W3 = 3 * KC;
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *Zs = twx + g.NX;               // [2][KXc][KC] zeta tile (updated in place)
@@ -567,6 +585,7 @@ template <typename R, int KC>
 __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ buf,
                                                          Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_begin();
   constexpr int W3 = 3 * KC;
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *Zs = twx + g.NX;          // [2][KXc][KC]
