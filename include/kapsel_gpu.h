@@ -32,6 +32,7 @@ extern "C" {
 #define KAPSEL_ESTATE -4     /* call out of order (e.g. step before init) */
 #define KAPSEL_ENONFINITE -5 /* a NaN/Inf was detected in the particle state */
 #define KAPSEL_ERANGE -6     /* a particle left the box or a size limit was exceeded */
+#define KAPSEL_ETIMEOUT -7   /* a bounded device wait ran out */
 
 #define KAPSEL_FP64 0  /* all fields and FFTs in double precision */
 #define KAPSEL_MIXED 1 /* fields/FFTs/stencils in float, particles and reductions in double */
@@ -75,6 +76,11 @@ typedef struct kapsel_params {
   double dielectric, surface_charge, debye_length;
   double valency_p, valency_n, onsager_p, onsager_n;
   double e_ext[3];
+  /* Particles held at their positions and velocities while the hydrodynamic
+     force and torque are still measured each step (a resistance
+     measurement, as used to generate near-contact training pairs; no
+     counterpart in the reference).  0 for the reference dynamics. */
+  int frozen;
 } kapsel_params;
 
 typedef struct kapsel_ctx kapsel_ctx;
@@ -224,6 +230,68 @@ int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms);
 
 /* Human-readable text of a status code. */
 const char *kapsel_gpu_strerror(int status);
+
+/* ---- Learned near-contact correction (no counterpart in the reference;
+   the reference's force is the plain SPM momentum exchange of
+   Calc_f_hydro_correct_precision, md_force.cxx:263-389). ----
+
+   A 4-layer MLP, 16 -> 128 -> 128 -> 128 -> 16 with SiLU activations, BF16
+   weights and activations on the tensor cores (tcgen05, FP32 accumulation),
+   predicts the force/torque correction of a close pair of spheres:
+   inputs  log(gap/a), v2 - v1, omega1, omega2 in the pair frame (10 values,
+           shifted and scaled, zero-padded to 16);
+   outputs F1, T1, F2, T2 in the pair frame (12 values, scaled, 4 unused).
+   Parameters are one packed FP32 vector of KAPSEL_NC_NPARAM floats:
+   W1[128][16] b1[128] W2[128][128] b2[128] W3[128][128] b3[128] W4[16][128] b4[16]
+   (W[out][in]).  All buffers below are host memory. */
+#define KAPSEL_NC_IN 16
+#define KAPSEL_NC_HIDDEN 128
+#define KAPSEL_NC_OUT 16
+#define KAPSEL_NC_NPARAM 37264
+
+typedef struct kapsel_nc kapsel_nc;
+
+int kapsel_nc_create(const float *params, kapsel_nc **out);
+int kapsel_nc_destroy(kapsel_nc *nc);
+int kapsel_nc_get_params(kapsel_nc *nc, float *params);
+int kapsel_nc_set_params(kapsel_nc *nc, const float *params);
+
+/* y[n][16] = network(x[n][16]). */
+int kapsel_nc_forward(kapsel_nc *nc, const float *x, int n, float *y);
+
+/* Gradient of L = (1/n) sum_rows sum_c colw[c] (net(x)[c] - y[c])^2 with
+   respect to the packed parameters (grad: KAPSEL_NC_NPARAM floats), and L. */
+int kapsel_nc_gradient(kapsel_nc *nc, const float *x, const float *y, const float *colw, int n, float *grad,
+                       float *loss);
+
+/* Adam (0.9, 0.999, 1e-8) on minibatches of `batch` rows, `epochs` passes
+   over the n samples in MT19937(seed) shuffled order; loss_per_epoch (may be
+   NULL) receives the mean minibatch loss of each epoch. */
+int kapsel_nc_train(kapsel_nc *nc, const float *x, const float *y, const float *colw, int n, int epochs, int batch,
+                    float lr, unsigned int seed, float *loss_per_epoch);
+
+/* Input shift/scale (16 each: feature = (raw - shift) * scale), output
+   scale (16: correction = output * scale), the radius a the network was
+   trained for, and the trained gap range [gap_lo, gap_hi] in units of a.
+   Pairs outside the range keep the plain SPM force. */
+int kapsel_nc_set_scaling(kapsel_nc *nc, const float *in_shift, const float *in_scale, const float *out_scale,
+                          double a, double gap_lo, double gap_hi);
+
+/* Host evaluation of the network input of one pair of particle records
+   (KAPSEL_P_STRIDE doubles each) in a periodic box of side lengths box[3]:
+   feat[16], frame[9] (e1, e2, e3; may be NULL), and the surface gap. */
+int kapsel_nc_pair_features(const kapsel_nc *nc, const double *rec_i, const double *rec_j, const double *box,
+                            float *feat, float *frame, double *gap);
+
+/* Attach a trained, scaled network to a Navier_Stokes context (NULL
+   detaches): each step then finds the pairs in the trained gap range after
+   the position update, evaluates the network on them and adds the
+   corrections to the hydrodynamic force and torque before the velocity
+   update.  The network must outlive its use by the context. */
+int kapsel_gpu_set_nearcontact(kapsel_ctx *ctx, const kapsel_nc *nc);
+
+/* Number of pairs the last step corrected. */
+int kapsel_gpu_nearcontact_pairs(kapsel_ctx *ctx, int *n_pairs);
 
 #ifdef __cplusplus
 }

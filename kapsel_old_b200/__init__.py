@@ -63,6 +63,7 @@ class _Params(ctypes.Structure):
         ("onsager_p", ctypes.c_double),
         ("onsager_n", ctypes.c_double),
         ("e_ext", ctypes.c_double * 3),
+        ("frozen", ctypes.c_int),
     ]
 
 
@@ -156,6 +157,7 @@ def params_from_config(cfg: dict, precision: int = FP64) -> _Params:
     for d in range(3):
         p.fix_cell[d] = 1 if fc[d] else 0
     p.mt_seed = int(cfg.get("mt_seed", 0))
+    p.frozen = 1 if cfg.get("frozen", False) else 0
     el = cfg.get("electrolyte")
     if el:
         p.dielectric = float(el["dielectric"])

@@ -32,6 +32,7 @@
 
 #include "../../include/kapsel_gpu.h"
 #include "electrolyte_kernels.cuh"
+#include "nearcontact_kernels.cuh"
 #include "particle_kernels.cuh"
 #include "spectral_kernels.cuh"
 
@@ -173,6 +174,17 @@ struct BoxBase {
   bool initialised = false;
   bool particles_set = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // learned near-contact correction (off unless a network is attached)
+  const kapsel_nc *nc = nullptr;
+  float *nc_feat = nullptr, *nc_frames = nullptr;
+  int2 *nc_pairs = nullptr;
+  int *nc_count = nullptr;
+  double *nc_corr = nullptr;
+  int nc_cap = 0;
+
+  // the pair search and the network, between the position update and the
+  // hydrodynamic gather (both launched without programmatic serialization)
+  void launch_nearcontact();
 
   virtual int alloc() = 0;
   virtual float time_ypass(int small, int reps) = 0;
@@ -373,8 +385,10 @@ struct Box : BoxBase {
     if (Np > 0) {
       if (!fuse_pos) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
       mark();
+      if (nc) launch_nearcontact();  // timed with the position slot when profiling
       launch_k(pdl, k_particles_hydro_velocity<R>, dim3(Np * PCL), dim3(256), 0, stream, pp, parts,
-               (const R *)ustar, (const int *)cells, noise, euler, status, partial_p, arrivals);
+               (const R *)ustar, (const int *)cells, noise, euler, status, partial_p, arrivals,
+               nc ? nc_corr : (double *)nullptr);
       mark();
       launch_k(pdl, k_particles_scatter<R>, dim3(Np * PCL), dim3(256), 0, stream, pp, (const DPart *)parts,
                (const int *)cells, phiup);
@@ -1053,6 +1067,47 @@ __global__ void k_time_gate(unsigned long long ns) {
 }
 
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Learned near-contact correction: network parameters, Adam state and the
+// scaling of a trained network.
+struct kapsel_nc {
+  cudaStream_t stream = nullptr;
+  float *params = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr, *loss = nullptr;
+  int *status = nullptr;
+  long long adam_t = 0;
+  nc::NcScale sc{};
+  bool scaled = false;
+};
+
+static int nc_smem_setup() {
+  static std::once_flag once;
+  static int rc = 0;
+  std::call_once(once, []() {
+    if (cudaFuncSetAttribute(nc::k_mlp_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)nc::SMEM_ALLOC) != cudaSuccess ||
+        cudaFuncSetAttribute(nc::k_mlp_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)nc::SMEM_ALLOC) != cudaSuccess)
+      rc = KAPSEL_ECUDA;
+  });
+  return rc;
+}
+
+void BoxBase::launch_nearcontact() {
+  cudaMemsetAsync(nc_count, 0, sizeof(int), stream);
+  nc::k_nc_pairs<<<Np, 128, 0, stream>>>(pp, parts, nc->sc, nc_feat, nc_frames, nc_pairs, nc_count, nc_cap, status);
+  nc::TileIO io{};
+  io.x = nc_feat;
+  io.n = -1;
+  io.n_dev = nc_count;
+  io.n_cap = nc_cap;
+  io.status = status;
+  io.pairs = nc_pairs;
+  io.frames = nc_frames;
+  io.corr = nc_corr;
+  io.sc = nc->sc;
+  nc::k_mlp_tile<false><<<(nc_cap + nc::TILE - 1) / nc::TILE, 128, nc::SMEM_ALLOC, stream>>>(nc->params, io);
+}
+
 struct kapsel_ctx {
   std::unique_ptr<BoxBase> box;
 };
@@ -1091,6 +1146,7 @@ const char *kapsel_gpu_strerror(int s) {
     case KAPSEL_ESTATE: return "call out of order";
     case KAPSEL_ENONFINITE: return "non-finite particle state";
     case KAPSEL_ERANGE: return "particle out of box or size limit exceeded";
+    case KAPSEL_ETIMEOUT: return "a bounded device wait ran out";
     default: return "unknown status";
   }
 }
@@ -1190,6 +1246,8 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   const double zeta_drag_rot = 8. * M_PI * p->eta * (pp.RADIUS * pp.RADIUS * pp.RADIUS);
   pp.noise_v = 1.439 * std::sqrt(zeta_drag * p->dt * p->kbt * p->alpha_v);
   pp.noise_o = 1.22 * std::sqrt(zeta_drag_rot * p->dt * p->kbt * p->alpha_o);
+  pp.frozen = p->frozen ? 1 : 0;
+  if (pp.frozen) pp.thermostat = 0;
   b->mt.reset(new MT19937(p->mt_seed));
 
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return KAPSEL_ECUDA;
@@ -1244,6 +1302,11 @@ int kapsel_gpu_destroy(kapsel_ctx *ctx) {
     cudaFree(b->status);
     cudaFree(b->partial_p);
     cudaFree(b->arrivals);
+    cudaFree(b->nc_feat);
+    cudaFree(b->nc_frames);
+    cudaFree(b->nc_pairs);
+    cudaFree(b->nc_count);
+    cudaFree(b->nc_corr);
     cudaStreamDestroy(b->stream);
   }
   delete ctx;
@@ -1921,3 +1984,268 @@ extern "C" int kapsel_gpu_solenoidal_u_noalloc(const int *np_xyz, double dx, con
   if (cudaGetLastError() != cudaSuccess) return KAPSEL_ECUDA;
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Learned near-contact correction: C ABI (no counterpart in the reference).
+extern "C" {
+
+int kapsel_nc_create(const float *params, kapsel_nc **out) {
+  if (!params || !out) return KAPSEL_EINVAL;
+  *out = nullptr;
+  int rc = nc_smem_setup();
+  if (rc) return rc;
+  std::unique_ptr<kapsel_nc> h(new (std::nothrow) kapsel_nc());
+  if (!h) return KAPSEL_ENOMEM;
+  const size_t nb = sizeof(float) * nc::NPARAM;
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return KAPSEL_ECUDA;
+  if (cudaMalloc(&h->params, nb) != cudaSuccess || cudaMalloc(&h->grad, nb) != cudaSuccess ||
+      cudaMalloc(&h->m, nb) != cudaSuccess || cudaMalloc(&h->v, nb) != cudaSuccess ||
+      cudaMalloc(&h->loss, sizeof(float)) != cudaSuccess || cudaMalloc(&h->status, sizeof(int)) != cudaSuccess)
+    return KAPSEL_ENOMEM;
+  KCHECK(cudaMemcpyAsync(h->params, params, nb, cudaMemcpyHostToDevice, h->stream));
+  KCHECK(cudaMemsetAsync(h->grad, 0, nb, h->stream));
+  KCHECK(cudaMemsetAsync(h->m, 0, nb, h->stream));
+  KCHECK(cudaMemsetAsync(h->v, 0, nb, h->stream));
+  KCHECK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+  KCHECK(cudaStreamSynchronize(h->stream));
+  *out = h.release();
+  return 0;
+}
+
+int kapsel_nc_destroy(kapsel_nc *nc) {
+  if (!nc) return KAPSEL_EINVAL;
+  cudaStreamSynchronize(nc->stream);
+  cudaFree(nc->params);
+  cudaFree(nc->grad);
+  cudaFree(nc->m);
+  cudaFree(nc->v);
+  cudaFree(nc->loss);
+  cudaFree(nc->status);
+  cudaStreamDestroy(nc->stream);
+  delete nc;
+  return 0;
+}
+
+int kapsel_nc_get_params(kapsel_nc *nc, float *params) {
+  if (!nc || !params) return KAPSEL_EINVAL;
+  KCHECK(cudaMemcpyAsync(params, nc->params, sizeof(float) * nc::NPARAM, cudaMemcpyDeviceToHost, nc->stream));
+  KCHECK(cudaStreamSynchronize(nc->stream));
+  return 0;
+}
+
+int kapsel_nc_set_params(kapsel_nc *nc, const float *params) {
+  if (!nc || !params) return KAPSEL_EINVAL;
+  KCHECK(cudaMemcpyAsync(nc->params, params, sizeof(float) * nc::NPARAM, cudaMemcpyHostToDevice, nc->stream));
+  KCHECK(cudaStreamSynchronize(nc->stream));
+  return 0;
+}
+
+static int nc_status(kapsel_nc *nc) {
+  int st = 0;
+  KCHECK(cudaMemcpyAsync(&st, nc->status, sizeof(int), cudaMemcpyDeviceToHost, nc->stream));
+  KCHECK(cudaStreamSynchronize(nc->stream));
+  if (st) {
+    cudaMemsetAsync(nc->status, 0, sizeof(int), nc->stream);
+    cudaStreamSynchronize(nc->stream);
+  }
+  return st;
+}
+
+int kapsel_nc_forward(kapsel_nc *nc, const float *x, int n, float *y) {
+  if (!nc || !x || !y || n < 0) return KAPSEL_EINVAL;
+  if (n == 0) return 0;
+  float *dx = nullptr, *dy = nullptr;
+  if (cudaMallocAsync(&dx, sizeof(float) * nc::IN * n, nc->stream) != cudaSuccess ||
+      cudaMallocAsync(&dy, sizeof(float) * nc::OUT * n, nc->stream) != cudaSuccess)
+    return KAPSEL_ENOMEM;
+  KCHECK(cudaMemcpyAsync(dx, x, sizeof(float) * nc::IN * n, cudaMemcpyHostToDevice, nc->stream));
+  nc::TileIO io{};
+  io.x = dx;
+  io.n = n;
+  io.out = dy;
+  io.status = nc->status;
+  nc::k_mlp_tile<false><<<(n + nc::TILE - 1) / nc::TILE, 128, nc::SMEM_ALLOC, nc->stream>>>(nc->params, io);
+  KCHECK(cudaGetLastError());
+  KCHECK(cudaMemcpyAsync(y, dy, sizeof(float) * nc::OUT * n, cudaMemcpyDeviceToHost, nc->stream));
+  cudaFreeAsync(dx, nc->stream);
+  cudaFreeAsync(dy, nc->stream);
+  KCHECK(cudaStreamSynchronize(nc->stream));
+  return nc_status(nc);
+}
+
+int kapsel_nc_gradient(kapsel_nc *nc, const float *x, const float *y, const float *colw, int n, float *grad,
+                       float *loss) {
+  if (!nc || !x || !y || !colw || !grad || !loss || n <= 0) return KAPSEL_EINVAL;
+  float *dx = nullptr, *dy = nullptr, *dw = nullptr;
+  if (cudaMallocAsync(&dx, sizeof(float) * nc::IN * n, nc->stream) != cudaSuccess ||
+      cudaMallocAsync(&dy, sizeof(float) * nc::OUT * n, nc->stream) != cudaSuccess ||
+      cudaMallocAsync(&dw, sizeof(float) * nc::OUT, nc->stream) != cudaSuccess)
+    return KAPSEL_ENOMEM;
+  KCHECK(cudaMemcpyAsync(dx, x, sizeof(float) * nc::IN * n, cudaMemcpyHostToDevice, nc->stream));
+  KCHECK(cudaMemcpyAsync(dy, y, sizeof(float) * nc::OUT * n, cudaMemcpyHostToDevice, nc->stream));
+  KCHECK(cudaMemcpyAsync(dw, colw, sizeof(float) * nc::OUT, cudaMemcpyHostToDevice, nc->stream));
+  KCHECK(cudaMemsetAsync(nc->grad, 0, sizeof(float) * nc::NPARAM, nc->stream));
+  KCHECK(cudaMemsetAsync(nc->loss, 0, sizeof(float), nc->stream));
+  nc::TileIO io{};
+  io.x = dx;
+  io.y = dy;
+  io.colw = dw;
+  io.n = n;
+  io.grad = nc->grad;
+  io.loss = nc->loss;
+  io.inv_n = 1.0f / (float)n;
+  io.status = nc->status;
+  nc::k_mlp_tile<true><<<(n + nc::TILE - 1) / nc::TILE, 128, nc::SMEM_ALLOC, nc->stream>>>(nc->params, io);
+  KCHECK(cudaGetLastError());
+  KCHECK(cudaMemcpyAsync(grad, nc->grad, sizeof(float) * nc::NPARAM, cudaMemcpyDeviceToHost, nc->stream));
+  KCHECK(cudaMemcpyAsync(loss, nc->loss, sizeof(float), cudaMemcpyDeviceToHost, nc->stream));
+  KCHECK(cudaMemsetAsync(nc->grad, 0, sizeof(float) * nc::NPARAM, nc->stream));
+  cudaFreeAsync(dx, nc->stream);
+  cudaFreeAsync(dy, nc->stream);
+  cudaFreeAsync(dw, nc->stream);
+  KCHECK(cudaStreamSynchronize(nc->stream));
+  return nc_status(nc);
+}
+
+int kapsel_nc_train(kapsel_nc *nc, const float *x, const float *y, const float *colw, int n, int epochs, int batch,
+                    float lr, unsigned int seed, float *loss_per_epoch) {
+  if (!nc || !x || !y || !colw || n <= 0 || epochs <= 0 || batch <= 0 || !(lr > 0.f)) return KAPSEL_EINVAL;
+  float *dx = nullptr, *dy = nullptr, *dw = nullptr;
+  int *didx = nullptr;
+  if (cudaMallocAsync(&dx, sizeof(float) * nc::IN * n, nc->stream) != cudaSuccess ||
+      cudaMallocAsync(&dy, sizeof(float) * nc::OUT * n, nc->stream) != cudaSuccess ||
+      cudaMallocAsync(&dw, sizeof(float) * nc::OUT, nc->stream) != cudaSuccess ||
+      cudaMallocAsync(&didx, sizeof(int) * n * (size_t)epochs, nc->stream) != cudaSuccess)
+    return KAPSEL_ENOMEM;
+  KCHECK(cudaMemcpyAsync(dx, x, sizeof(float) * nc::IN * n, cudaMemcpyHostToDevice, nc->stream));
+  KCHECK(cudaMemcpyAsync(dy, y, sizeof(float) * nc::OUT * n, cudaMemcpyHostToDevice, nc->stream));
+  KCHECK(cudaMemcpyAsync(dw, colw, sizeof(float) * nc::OUT, cudaMemcpyHostToDevice, nc->stream));
+  // one permutation per epoch (MT19937 stream of `seed`, Fisher-Yates)
+  std::vector<int> perm((size_t)n * epochs);
+  MT19937 mt(seed);
+  for (int e = 0; e < epochs; ++e) {
+    int *pe = perm.data() + (size_t)e * n;
+    for (int i = 0; i < n; ++i) pe[i] = i;
+    for (int i = n - 1; i > 0; --i) {
+      const int j = (int)(mt.real3() * (i + 1));
+      std::swap(pe[i], pe[j < i ? j : i]);
+    }
+  }
+  KCHECK(cudaMemcpyAsync(didx, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice, nc->stream));
+  KCHECK(cudaMemsetAsync(nc->grad, 0, sizeof(float) * nc::NPARAM, nc->stream));
+  std::vector<float> el(epochs, 0.f);
+  const int nbatch = (n + batch - 1) / batch;
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  for (int e = 0; e < epochs; ++e) {
+    KCHECK(cudaMemsetAsync(nc->loss, 0, sizeof(float), nc->stream));
+    for (int b = 0; b < nbatch; ++b) {
+      const int r0 = b * batch, nb = std::min(batch, n - r0);
+      nc::TileIO io{};
+      io.x = dx;
+      io.y = dy;
+      io.colw = dw;
+      io.idx = didx + (size_t)e * n + r0;
+      io.n = nb;
+      io.grad = nc->grad;
+      io.loss = nc->loss;
+      io.inv_n = 1.0f / (float)nb;
+      io.status = nc->status;
+      nc::k_mlp_tile<true><<<(nb + nc::TILE - 1) / nc::TILE, 128, nc::SMEM_ALLOC, nc->stream>>>(nc->params, io);
+      nc->adam_t += 1;
+      const float c1 = 1.0f / (1.0f - powf(b1, (float)nc->adam_t)), c2 = 1.0f / (1.0f - powf(b2, (float)nc->adam_t));
+      nc::k_adam<<<(nc::NPARAM + 255) / 256, 256, 0, nc->stream>>>(nc->params, nc->grad, nc->m, nc->v, nc::NPARAM,
+                                                                   lr, b1, b2, eps, c1, c2);
+    }
+    KCHECK(cudaGetLastError());
+    KCHECK(cudaMemcpyAsync(&el[e], nc->loss, sizeof(float), cudaMemcpyDeviceToHost, nc->stream));
+  }
+  cudaFreeAsync(dx, nc->stream);
+  cudaFreeAsync(dy, nc->stream);
+  cudaFreeAsync(dw, nc->stream);
+  cudaFreeAsync(didx, nc->stream);
+  KCHECK(cudaStreamSynchronize(nc->stream));
+  if (loss_per_epoch)
+    for (int e = 0; e < epochs; ++e) loss_per_epoch[e] = el[e] / (float)nbatch;
+  return nc_status(nc);
+}
+
+int kapsel_nc_set_scaling(kapsel_nc *nc, const float *in_shift, const float *in_scale, const float *out_scale,
+                          double a, double gap_lo, double gap_hi) {
+  if (!nc || !in_shift || !in_scale || !out_scale || !(a > 0.0) || !(gap_lo > 0.0) || !(gap_hi > gap_lo))
+    return KAPSEL_EINVAL;
+  for (int i = 0; i < nc::IN; ++i) {
+    nc->sc.in_shift[i] = in_shift[i];
+    nc->sc.in_scale[i] = in_scale[i];
+  }
+  for (int i = 0; i < nc::OUT; ++i) nc->sc.out_scale[i] = out_scale[i];
+  nc->sc.a = a;
+  nc->sc.gap_lo = gap_lo;
+  nc->sc.gap_hi = gap_hi;
+  nc->scaled = true;
+  return 0;
+}
+
+int kapsel_nc_pair_features(const kapsel_nc *nc, const double *rec_i, const double *rec_j, const double *box,
+                            float *feat, float *frame, double *gap) {
+  if (!nc || !nc->scaled || !rec_i || !rec_j || !box || !feat) return KAPSEL_EINVAL;
+  double d[3];
+  for (int k = 0; k < 3; ++k) {
+    d[k] = rec_j[KAPSEL_P_X + k] - rec_i[KAPSEL_P_X + k];
+    const double q = d[k] / box[k];
+    d[k] -= (q >= 0.0 ? (double)(long long)(q + 0.5) : (double)(long long)(q - 0.5)) * box[k];
+  }
+  const double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  const double h = r - 2.0 * nc->sc.a;
+  if (gap) *gap = h;
+  if (!(h > 0.0)) return KAPSEL_ERANGE;
+  double e[9];
+  nc::nc_frame(d, e);
+  nc::nc_features(nc->sc, h, e, rec_i + KAPSEL_P_V, rec_j + KAPSEL_P_V, rec_i + KAPSEL_P_OMEGA,
+                  rec_j + KAPSEL_P_OMEGA, feat);
+  if (frame)
+    for (int k = 0; k < 9; ++k) frame[k] = (float)e[k];
+  return 0;
+}
+
+int kapsel_gpu_set_nearcontact(kapsel_ctx *ctx, const kapsel_nc *nc) {
+  if (!ctx) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (nc && (!nc->scaled || b->prm.eq != KAPSEL_EQ_NAVIER_STOKES || b->Np < 2 ||
+             std::fabs(b->pp.RADIUS - nc->sc.a) > 1e-12 * nc->sc.a))
+    return KAPSEL_EINVAL;
+  KCHECK(cudaStreamSynchronize(b->stream));
+  for (int s = 0; s < 2; ++s)
+    if (b->graph[s]) {
+      cudaGraphExecDestroy(b->graph[s]);
+      b->graph[s] = nullptr;
+    }
+  if (nc && !b->nc_feat) {
+    int rc = nc_smem_setup();
+    if (rc) return rc;
+    // at most ~25 neighbours within a surface gap of 2a per sphere
+    b->nc_cap = 32 * b->Np;
+    if (cudaMalloc(&b->nc_feat, sizeof(float) * nc::IN * b->nc_cap) != cudaSuccess ||
+        cudaMalloc(&b->nc_frames, sizeof(float) * 9 * b->nc_cap) != cudaSuccess ||
+        cudaMalloc(&b->nc_pairs, sizeof(int2) * b->nc_cap) != cudaSuccess ||
+        cudaMalloc(&b->nc_count, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->nc_corr, sizeof(double) * 6 * b->Np) != cudaSuccess)
+      return KAPSEL_ENOMEM;
+    KCHECK(cudaMemset(b->nc_count, 0, sizeof(int)));
+    KCHECK(cudaMemset(b->nc_corr, 0, sizeof(double) * 6 * b->Np));
+  }
+  b->nc = nc;
+  return 0;
+}
+
+int kapsel_gpu_nearcontact_pairs(kapsel_ctx *ctx, int *n_pairs) {
+  // pairs found by the last step's search (0 when no network is attached)
+  if (!ctx || !n_pairs) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  *n_pairs = 0;
+  if (!b->nc) return 0;
+  KCHECK(cudaStreamSynchronize(b->stream));
+  KCHECK(cudaMemcpy(n_pairs, b->nc_count, sizeof(int), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+}  // extern "C"

@@ -35,6 +35,7 @@ struct PPar {
   int gdir;
   int thermostat;
   double noise_v, noise_o;  // fluct.cxx:13-19
+  int frozen;               // positions and velocities held; forces still measured
 };
 
 __device__ __forceinline__ double nint_d(double a) {
@@ -134,6 +135,7 @@ __device__ __forceinline__ void qnormalize(double *q) {
 // (particle_rotation_solver.h:15-39).  One thread per particle.
 __device__ __forceinline__ void position_update_one(const PPar &p, DPart *__restrict__ parts, int n, int euler,
                                                     int *__restrict__ status) {
+  if (p.frozen) return;
   DPart &a = parts[n];
   const double hdt = 0.5 * p.dt;
   for (int d = 0; d < 3; ++d) {
@@ -232,7 +234,8 @@ __global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPa
                                                                   const double *__restrict__ noise, int euler,
                                                                   int *__restrict__ status,
                                                                   double *__restrict__ partial,
-                                                                  int *__restrict__ arrivals) {
+                                                                  int *__restrict__ arrivals,
+                                                                  double *__restrict__ nc_corr = nullptr) {
   __shared__ double sh[2 * 9 * 32];
   __shared__ int last;
   pdl_begin();
@@ -343,6 +346,23 @@ __global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPa
     fr[d] = tot[6 + d].s + tot[6 + d].c;
   }
   fr[p.gdir] -= p.grav;
+  if (nc_corr) {
+    // learned near-contact correction of this step's hydrodynamic force/torque
+    for (int d = 0; d < 3; ++d) {
+      fh[d] += nc_corr[6 * (size_t)n + d];
+      if (p.rotation) th[d] += nc_corr[6 * (size_t)n + 3 + d];
+      nc_corr[6 * (size_t)n + d] = 0.0;
+      nc_corr[6 * (size_t)n + 3 + d] = 0.0;
+    }
+  }
+  if (p.frozen) {
+    for (int d = 0; d < 3; ++d) {
+      a.fr_prev[d] = fr[d];
+      a.f_hydro_prev[d] = fh[d];
+      a.t_hydro_prev[d] = th[d];
+    }
+    return;
+  }
   const double hdt = 0.5 * p.dt;
   for (int d = 0; d < 3; ++d) {
     a.v_old[d] = a.v[d];

@@ -96,3 +96,11 @@ def batched(n_boxes: int = 48, seed: int = 4, max_fill: float = 0.2) -> list:
         n = min(n, cap)
         out.append(spm_config(shape, n, seed=1000 * seed + b, a=a, kbt=1e-3))
     return out
+
+
+def nearcontact_256_2048() -> dict:
+    """256^3, 2048 spheres a=5, xi=2 (solid volume fraction 0.064), minimum
+    surface gap 0.25 = 0.05a so that pairs reach into the near-contact range,
+    kBT=1e-3, dt=0.01, positions from PCG64 seed 5 (the deployment case of the
+    learned near-contact correction)."""
+    return spm_config((8, 8, 8), 2048, seed=5, kbt=1e-3, min_gap=0.25)

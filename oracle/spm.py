@@ -53,6 +53,9 @@ class Params:
         self.G_direction = {"-X": 0, "-Y": 1, "-Z": 2}[cfg.get("gravity_dir", "-Z")]
         self.EPSILON = float(cfg.get("epsilon", 1.0))
         self.ROTATION = 1 if cfg.get("rotation", "ON") == "ON" else 0
+        # particles held at their positions and velocities, forces still
+        # measured (the GPU library's resistance mode; no reference switch)
+        self.frozen = bool(cfg.get("frozen", False))
         lj = cfg.get("lj_truncate", "ON")
         self.LJ_truncate = {"ON": 1, "OFF": 0, "NONE": -1}[lj]
         self.LJ_powers = {"12:6": 0, "24:12": 1, "36:18": 2}[cfg.get("lj_powers", "12:6")]
@@ -573,11 +576,16 @@ class SpmOracle:
         zeta = np.stack([S.truncate(zeta[d]) for d in range(2)])
         u = S.zeta_k2u(zeta, self.uk_dc)
         if self.p.n > 0:
-            self.position_update()
-            self.hydro_force(u)
-            self.velocity_update()
-            if P.kBT > 0.0:
-                self.thermostat()
+            if P.frozen:
+                self.hydro_force(u)
+                self.force()
+                self.reset_forces()
+            else:
+                self.position_update()
+                self.hydro_force(u)
+                self.velocity_update()
+                if P.kBT > 0.0:
+                    self.thermostat()
             phi, up = self.phi_up(self.p.x, self.p.v, self.p.omega)
             f = S.solenoidal_u(up - phi * u)
             u = u + f

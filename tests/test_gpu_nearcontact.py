@@ -1,0 +1,212 @@
+"""Learned near-contact correction on the GPU: the tcgen05 BF16 network
+kernels against the CPU oracle (oracle/mlp.py), the frozen-particle
+resistance mode against the SPM oracle, the per-step correction hook, and
+the gain of the trained network over the plain method on the committed pair
+set (tests/golden/nearcontact_pairs.npz, generated by make_nearcontact.py).
+
+Tolerances: network output within 2e-2 of the output scale and gradients
+within 3e-2 relative L2 per tensor against the bf16-emulating oracle (the
+kernels sum in a different order and may round an activation to the other
+bf16 neighbour); frozen-mode forces <= 1e-10 relative (FP64 path).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mlp, spm, udf
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PAIRS = os.path.join(HERE, "golden", "nearcontact_pairs.npz")
+
+
+def _net(params):
+    from kapsel_old_b200 import nearcontact as nc
+
+    return nc.NearContactNet(params)
+
+
+def _random_params(seed):
+    p = mlp.init_params(seed)
+    rng = np.random.default_rng(seed + 100)
+    d = mlp.unpack(p)
+    for k in ("b1", "b2", "b3", "b4"):
+        d[k] = rng.normal(scale=0.3, size=d[k].shape).astype(np.float32)
+    d["W4"] = d["W4"] * 10.0
+    return mlp.pack(d)
+
+
+def _inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n, 16)).astype(np.float32)
+    x[:, 10:] = 0.0
+    return x
+
+
+@pytest.mark.parametrize("n", [1, 128, 300])
+def test_network_forward_matches_oracle(n):
+    p = _random_params(3)
+    x = _inputs(n, 4)
+    net = _net(p)
+    y = net.forward(x)
+    ref, _, _ = mlp.forward(p, x, "bf16")
+    scale = np.abs(ref).max()
+    assert np.abs(y - ref).max() <= 2e-2 * scale, (np.abs(y - ref).max(), scale)
+    # and the exact network within bf16 accuracy
+    ref64, _, _ = mlp.forward(p.astype(np.float64), x.astype(np.float64), "fp64")
+    assert np.abs(y - ref64).max() <= 5e-2 * np.abs(ref64).max()
+
+
+@pytest.mark.parametrize("n", [77, 256])
+def test_network_gradient_matches_oracle(n):
+    p = _random_params(5)
+    x = _inputs(n, 6)
+    rng = np.random.default_rng(7)
+    y = rng.normal(size=(n, 16)).astype(np.float32)
+    w = np.r_[np.ones(12), np.zeros(4)].astype(np.float32)
+    net = _net(p)
+    g, loss = net.gradient(x, y, w)
+    gr, lr = mlp.gradient(p, x, y, w, "bf16")
+    assert abs(loss - lr) <= 1e-3 * abs(lr)
+    G, R = mlp.unpack(g), mlp.unpack(gr)
+    for k in R:
+        e = np.linalg.norm(G[k] - R[k]) / np.linalg.norm(R[k])
+        assert e < 3e-2, (k, e)
+    # rows 12..15 carry no loss: no gradient on their weights
+    assert np.all(G["W4"][12:] == 0) and np.all(G["b4"][12:] == 0)
+
+
+def test_network_training_fits_a_smooth_map():
+    rng = np.random.default_rng(11)
+    n = 4096
+    x = np.zeros((n, 16), np.float32)
+    x[:, :10] = rng.uniform(-1.5, 1.5, size=(n, 10))
+    y = np.zeros((n, 16), np.float32)
+    y[:, :12] = np.stack([np.sin(x[:, i % 10]) * np.cos(x[:, (3 * i + 1) % 10]) + 0.3 * x[:, (i + 5) % 10]
+                          for i in range(12)], 1)
+    w = np.r_[np.ones(12), np.zeros(4)].astype(np.float32)
+    net = _net(mlp.init_params(2))
+    hist = net.train(x, y, w, epochs=40, batch=256, lr=2e-3, seed=1)
+    assert hist[-1] < 0.05 * hist[0], hist[[0, -1]]
+    yp = net.forward(x)
+    err = np.sqrt(np.mean((yp[:, :12] - y[:, :12]) ** 2)) / np.sqrt(np.mean(y[:, :12] ** 2))
+    assert err < 0.1, err
+
+
+def test_frozen_pair_forces_match_oracle():
+    import kapsel_old_b200 as kg
+
+    cfg = udf.ns_config((5, 5, 5), 2, seed=3, kbt=0.0, min_gap=1.0)
+    cfg["frozen"] = True
+    cfg["lj_truncate"] = "NONE"
+    g = kg.Simulation(cfg, precision=kg.FP64)
+    O = spm.SpmOracle(cfg)
+    st = g.particles()
+    v = np.array([[0.01, -0.02, 0.005], [-0.015, 0.0, 0.02]])
+    w = np.array([[0.001, 0.002, -0.003], [0.0, -0.002, 0.001]])
+    st["v"], st["omega"] = v, w
+    g.set_particle_state(st)
+    O.p.v[:] = v
+    O.p.omega[:] = w
+    for _ in range(4):
+        g.step(1)
+        O.step()
+    p = g.particles()
+    assert np.array_equal(p["x"], O.p.x) and np.array_equal(p["v"], v)
+    for k, ref in (("f_hydro", O.p.f_hydro_previous), ("torque_hydro", O.p.torque_hydro_previous)):
+        assert np.linalg.norm(p[k] - ref) <= 1e-10 * np.linalg.norm(ref), k
+
+
+def test_pair_features_device_equals_numpy():
+    from kapsel_old_b200 import nearcontact as nc
+
+    net = _net(mlp.init_params(1))
+    shift = np.linspace(-1, 1, 16).astype(np.float32)
+    scale = np.linspace(0.5, 2, 16).astype(np.float32)
+    net.set_scaling(shift, scale, np.ones(16), a=5.0)
+    rng = np.random.default_rng(3)
+    box = np.array([64.0, 64.0, 64.0])
+    for _ in range(20):
+        ri, rj = np.zeros(35), np.zeros(35)
+        ri[0:3] = rng.uniform(0, 64, 3)
+        d = rng.normal(size=3)
+        d *= rng.uniform(10.5, 19.0) / np.linalg.norm(d)
+        rj[0:3] = np.mod(ri[0:3] + d, 64.0)
+        ri[3:9], rj[3:9] = rng.normal(scale=0.05, size=6), rng.normal(scale=0.05, size=6)
+        f, e, gap = net.pair_features(ri, rj, box)
+        en = nc.pair_frame(d)
+        raw = nc.raw_features((np.linalg.norm(d) - 10.0) / 5.0, en, ri[3:6], rj[3:6], ri[6:9], rj[6:9])
+        assert np.allclose(e, en, atol=1e-6)
+        assert np.allclose(f, net.features(raw)[0], rtol=1e-5, atol=1e-5)
+
+
+def test_step_hook_adds_network_correction():
+    """Frozen pair at gap 0.4a: one step with the network attached changes
+    the hydrodynamic force/torque by exactly the network's correction."""
+    import kapsel_old_b200 as kg
+    from kapsel_old_b200 import nearcontact as nc
+
+    cfg = {"eq": "Navier_Stokes", "np_xyz": (6, 6, 6), "a": 5.0, "a_xi": 2.0, "kbt": 0.0, "dt": 0.05,
+           "frozen": True, "lj_truncate": "NONE",
+           "particles": [{"x": (27.3, 31.2, 30.1)}, {"x": (37.1, 33.9, 32.2)}]}
+    v = np.array([[0.02, -0.01, 0.0], [-0.03, 0.01, 0.02]])
+    w = np.array([[0.004, 0.0, -0.002], [0.001, 0.003, 0.0]])
+    runs = []
+    net = _net(_random_params(9))
+    net.set_scaling(np.zeros(16), np.ones(16) * 0.5, np.ones(16) * 0.01, a=5.0, gap_lo=0.05, gap_hi=2.0)
+    for attach in (False, True):
+        g = kg.Simulation(cfg, precision=kg.MIXED)
+        st = g.particles()
+        st["v"], st["omega"] = v, w
+        g.set_particle_state(st)
+        if attach:
+            nc.attach(g, net)
+        g.step(1, graph=attach)
+        runs.append(g.particles())
+        if attach:
+            assert nc.corrected_pairs(g) == 1
+        g.close()
+    rec = np.zeros((2, 35))
+    rec[:, 0:3] = runs[0]["x"]
+    rec[:, 3:6] = v
+    rec[:, 6:9] = w
+    f, e, gap = net.pair_features(rec[0], rec[1], np.array([64.0] * 3))
+    out = net.forward(f[None])[0, :12] * 0.01
+    corr = np.einsum("kj,vk->vj", e.astype(np.float64), out.reshape(4, 3).astype(np.float64))
+    dF = runs[1]["f_hydro"] - runs[0]["f_hydro"]
+    dT = runs[1]["torque_hydro"] - runs[0]["torque_hydro"]
+    got = np.array([dF[0], dT[0], dF[1], dT[1]])
+    assert np.abs(got - corr).max() <= 1e-6 * np.abs(corr).max() + 1e-12, (got, corr)
+
+
+@pytest.mark.skipif(not os.path.exists(PAIRS), reason="pair set not generated")
+def test_pair_set_reproduces():
+    from kapsel_old_b200 import nearcontact as nc
+
+    d = dict(np.load(PAIRS))
+    runner_c = nc.PairRunner(nc.COARSE, 1.0, int(d["steps"]))
+    runner_f = nc.PairRunner(nc.FINE, 2.0, int(d["steps"]))
+    for i in (0, len(d["gap"]) - 1):
+        args = (d["gap"][i], d["v"][i], d["w1"][i], d["w2"][i], d["offset"][i])
+        fc = runner_c.forces(*args)
+        ff = runner_f.forces(*args)
+        assert np.allclose(fc, d["f_coarse"][i], rtol=1e-9, atol=1e-14)
+        assert np.allclose(ff, d["f_fine"][i], rtol=1e-9, atol=1e-14)
+    runner_c.close()
+    runner_f.close()
+
+
+@pytest.mark.skipif(not os.path.exists(PAIRS), reason="pair set not generated")
+def test_learned_correction_cuts_force_error():
+    from kapsel_old_b200 import nearcontact as nc
+
+    d = dict(np.load(PAIRS))
+    n = len(d["gap"])
+    ntest = n // 8
+    test_idx = np.arange(n - ntest, n)
+    net, hist = nc.fit(d, np.arange(n - ntest), epochs=600)
+    e = nc.errors(net, d, test_idx)
+    assert e["force_learned"] * 3.0 <= e["force_plain"], e
+    assert e["torque_learned"] < e["torque_plain"], e

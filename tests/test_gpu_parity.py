@@ -147,6 +147,15 @@ def test_step_fp64_noncubic_gravity_fixcell():
         assert v < FP64_TOL, (k, v, w)
 
 
+@pytest.mark.parametrize("np_xyz", [(8, 5, 4), (4, 8, 5), (5, 4, 8)])
+def test_step_fp64_256_lines(np_xyz):
+    """Lines of 256 points along each axis (the longest the transforms take)."""
+    cfg = udf.ns_config(np_xyz, 2, seed=7, a=3.0, kbt=1e-3, min_gap=0.5)
+    w = _compare_run(cfg, 3, 0)
+    for k, v in w.items():
+        assert v < FP64_TOL, (k, v, w)
+
+
 def test_step_graph_equals_eager():
     cfg = _cfg((5, 5, 5), 6, seed=11, kbt=1e-3, min_gap=0.2)
     a = _sim(cfg)
