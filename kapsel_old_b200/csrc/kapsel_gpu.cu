@@ -35,6 +35,7 @@
 #include "nearcontact_kernels.cuh"
 #include "particle_kernels.cuh"
 #include "spectral_kernels.cuh"
+#include "zwarp_kernels.cuh"
 
 using namespace kapsel;
 
@@ -236,6 +237,74 @@ struct Box : BoxBase {
 
   size_t npts() const { return (size_t)g.NX * g.NY * g.NZ; }
 
+  // warp-level z kernels for NZ = 64, 128, 256 (zw = log2(NZ/2)); 0: block-level
+  static constexpr int ZNW = sizeof(R) == 4 ? 8 : 4;  // warps per block
+  int zw = 0;
+  int zw_grid_p = 0, zw_grid_c = 0, zw_grid_f = 0;
+  size_t zw_sm_p = 0, zw_sm_c = 0, zw_sm_f = 0;
+
+  template <int LM>
+  int zw_setup() {
+    using Z = ZL<LM>;
+    const size_t line = sizeof(Cx<R>) * Z::RW * Z::LS * ZNW;
+    zw_sm_p = 5 * line;
+    zw_sm_c = 2 * line;
+    zw_sm_f = 3 * line;
+    KCHECK(cudaFuncSetAttribute(k_zw_products<R, LM, ZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_p));
+    KCHECK(cudaFuncSetAttribute(k_zw_c2r<R, LM, ZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_c));
+    KCHECK(cudaFuncSetAttribute(k_zw_force<R, LM, ZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_f));
+    int dev = 0, nsm = 0, op = 0, oc = 0, of = 0;
+    KCHECK(cudaGetDevice(&dev));
+    KCHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    KCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, k_zw_products<R, LM, ZNW>, ZNW * 32, zw_sm_p));
+    KCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oc, k_zw_c2r<R, LM, ZNW>, ZNW * 32, zw_sm_c));
+    KCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&of, k_zw_force<R, LM, ZNW>, ZNW * 32, zw_sm_f));
+    const int groups = g.NX * g.NY / Z::RW;
+    zw_grid_p = std::min((groups + ZNW - 1) / ZNW, std::max(op, 1) * nsm);
+    zw_grid_c = std::min((3 * groups + ZNW - 1) / ZNW, std::max(oc, 1) * nsm);
+    zw_grid_f = std::min((groups + ZNW - 1) / ZNW, std::max(of, 1) * nsm);
+    zw = LM;
+    return 0;
+  }
+  template <int LM>
+  void zw_products(bool pdl) {
+    launch_k(pdl, k_zw_products<R, LM, ZNW>, dim3(zw_grid_p), dim3(ZNW * 32), zw_sm_p, stream, g, tw, bufB);
+  }
+  template <int LM>
+  void zw_c2r(bool pdl, DPart *pts, int euler) {
+    const int posblk = pts ? (Np + ZNW * 32 - 1) / (ZNW * 32) : 0;
+    launch_k(pdl, k_zw_c2r<R, LM, ZNW>, dim3(zw_grid_c + posblk), dim3(ZNW * 32), zw_sm_c, stream, g, tw,
+             (const Cx<R> *)bufB, ustar, npts(), g.NZ, 3, zw_grid_c, pp, pts, euler, status);
+  }
+  template <int LM>
+  void zw_force(bool pdl) {
+    launch_k(pdl, k_zw_force<R, LM, ZNW>, dim3(zw_grid_f), dim3(ZNW * 32), zw_sm_f, stream, g, tw, phiup,
+             (const R *)ustar, bufB);
+  }
+  // dispatch on the compile-time line length
+  void zdisp_products(bool pdl) {
+    if (zw == 5) zw_products<5>(pdl);
+    else if (zw == 6) zw_products<6>(pdl);
+    else if (zw == 7) zw_products<7>(pdl);
+    else launch_k(pdl, k_z_products<R>, dim3(gz()), dim3(256), smem_zp, stream, g, tw, bufB);
+  }
+  void zdisp_c2r(bool pdl, DPart *pts, int euler) {
+    if (zw == 5) zw_c2r<5>(pdl, pts, euler);
+    else if (zw == 6) zw_c2r<6>(pdl, pts, euler);
+    else if (zw == 7) zw_c2r<7>(pdl, pts, euler);
+    else {
+      const int posblk = pts ? (Np + 255) / 256 : 0;
+      launch_k(pdl, k_z_c2r<R>, dim3(gz() + posblk, 3), dim3(256), smem_zc, stream, g, tw, (const Cx<R> *)bufB,
+               ustar, npts(), g.NZ, pp, pts, euler, status);
+    }
+  }
+  void zdisp_force(bool pdl) {
+    if (zw == 5) zw_force<5>(pdl);
+    else if (zw == 6) zw_force<6>(pdl);
+    else if (zw == 7) zw_force<7>(pdl);
+    else launch_k(pdl, k_z_force<R>, dim3(gz()), dim3(256), smem_zf, stream, g, tw, phiup, (const R *)ustar, bufB);
+  }
+
   int alloc() override {
     const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
     const size_t nA = (size_t)g.NX * g.KYc * g.TZ;
@@ -279,6 +348,13 @@ struct Box : BoxBase {
     smem_zr = C * (g.M + g.NZ + (size_t)g.M * (2 * ZROWS + 1) + (size_t)ZROWS * P);
     const size_t mx = 227 * 1024;
     if (smem_xadv > mx || smem_xu > mx || smem_y > mx || smem_zp > mx) return KAPSEL_ERANGE;
+    {
+      int rc = 0;
+      if (g.NZ == 64) rc = zw_setup<5>();
+      else if (g.NZ == 128) rc = zw_setup<6>();
+      else if (g.NZ == 256) rc = zw_setup<7>();
+      if (rc) return rc;
+    }
     KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
     KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xadv));
     KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xf));
@@ -304,8 +380,25 @@ struct Box : BoxBase {
   // this box shape (kapsel_batch_create)
   int ytile_small = 0;
   bool use_pdl = true;
+  template <bool INV, int LY>
+  void yw(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out, bool pdl) {
+    using Y = ZL<LY>;
+    const int items = nc * gg.NX * ((gg.TZ + Y::RW - 1) / Y::RW);
+    const size_t sm = sizeof(Cx<R>) * Y::RW * Y::LS;
+    if (gg.KYc == gg.NY)
+      launch_k(pdl, k_yw_pass<R, INV, LY, true>, dim3(items), dim3(32), sm, stream, gg, tw, in, out, nc);
+    else
+      launch_k(pdl, k_yw_pass<R, INV, LY, false>, dim3(items), dim3(32), sm, stream, gg, tw, in, out, nc);
+  }
   template <bool INV>
   void launch_y(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out, bool pdl = false) {
+    switch (gg.NY) {
+      case 32: yw<INV, 5>(gg, nc, in, out, pdl); return;
+      case 64: yw<INV, 6>(gg, nc, in, out, pdl); return;
+      case 128: yw<INV, 7>(gg, nc, in, out, pdl); return;
+      case 256: yw<INV, 8>(gg, nc, in, out, pdl); return;
+      default: break;
+    }
     constexpr int K2 = KCY / 2;
     const size_t sm = std::max(smem_y, sm_y_any);
     if (ytile_small)
@@ -346,7 +439,7 @@ struct Box : BoxBase {
 
   // f (from phi/up and u*) -> zeta update, launches 11-13
   void launch_force_to_zeta() {
-    k_z_force<R><<<gz(), 256, smem_zf, stream>>>(g, tw, phiup, ustar, bufB);
+    zdisp_force(false);
     launch_y<false>(g, 3, bufB, bufA);
     k_x_force_to_zeta<R, KCX><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc);
   }
@@ -367,7 +460,7 @@ struct Box : BoxBase {
     mark();
     launch_y<true>(g, 3, bufA, bufB, pdl);
     mark();
-    launch_k(pdl, k_z_products<R>, dim3(gz()), dim3(256), smem_zp, stream, g, tw, bufB);
+    zdisp_products(pdl);
     mark();
     launch_y<false>(g, 5, bufB, bufA, pdl);
     mark();
@@ -378,9 +471,7 @@ struct Box : BoxBase {
     // u* and, in extra blocks, the particle positions (a launch of their own
     // when profiling, so that each launch is timed separately)
     const bool fuse_pos = Np > 0 && !ev;
-    const int posblk = fuse_pos ? (Np + 255) / 256 : 0;
-    launch_k(pdl, k_z_c2r<R>, dim3(gz() + posblk, 3), dim3(256), smem_zc, stream, g, tw, (const Cx<R> *)bufB, ustar,
-             npts(), g.NZ, pp, fuse_pos ? parts : (DPart *)nullptr, euler, status);
+    zdisp_c2r(pdl, fuse_pos ? parts : (DPart *)nullptr, euler);
     mark();
     if (Np > 0) {
       if (!fuse_pos) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
@@ -393,7 +484,7 @@ struct Box : BoxBase {
       launch_k(pdl, k_particles_scatter<R>, dim3(Np * PCL), dim3(256), 0, stream, pp, (const DPart *)parts,
                (const int *)cells, phiup);
       mark();
-      launch_k(pdl, k_z_force<R>, dim3(gz()), dim3(256), smem_zf, stream, g, tw, phiup, (const R *)ustar, bufB);
+      zdisp_force(pdl);
       mark();
       launch_y<false>(g, 3, bufB, bufA, pdl);
       mark();
