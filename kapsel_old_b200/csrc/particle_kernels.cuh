@@ -61,6 +61,13 @@ __device__ __forceinline__ R prof_phi(double x, const PPar &p) {
   return sizeof(R) == 8 ? h / (h + h2) : R(__fdividef((float)h, (float)(h + h2)));
 }
 
+// Phi of the mixed path with every argument in float: rp = RADIUS + HXI,
+// rm = RADIUS - HXI (profile.h:29-49).
+__device__ __forceinline__ float prof_phi_f(float x, float rp, float rm, float dx) {
+  const float h = prof_H<float>(rp - x, dx), h2 = prof_H<float>(x - rm, dx);
+  return __fdividef(h, h + h2);
+}
+
 // Stencil geometry shared by the gather and the scatter: Particle_cell
 // (make_phi.h:102-130), Relative_coord (:143-160), Distance (interaction.h:110-133).
 struct StencilBase {
@@ -254,6 +261,46 @@ __global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPa
   double a9[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) a9[i] = 0.0;
+  float f6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if constexpr (sizeof(R) == 4) {
+    // mixed path: the point's offset from the sphere centre, its distance,
+    // phi and the momentum-exchange terms in float (the offset is an integer
+    // cell shift minus the centre's sub-cell residue, so it is exact to one
+    // float ulp); the per-thread and per-warp sums in float, every wider sum
+    // in double (compensated)
+    const float dxf = (float)p.DX, rpf = (float)(p.RADIUS + p.HXI), rmf = (float)(p.RADIUS - p.HXI);
+    const float resf[3] = {(float)b.res[0], (float)b.res[1], (float)b.res[2]};
+    const float vpf[3] = {(float)vp[0], (float)vp[1], (float)vp[2]};
+    const float wpf[3] = {(float)wp[0], (float)wp[1], (float)wp[2]};
+    for (int m = first; m < p.S; m += stride) {
+      const int *cell = cells + 3 * m;
+      int rm[3];
+      float r[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);
+        r[d] = (float)cell[d] * dxf - resf[d];
+      }
+      const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
+      const float ug[3] = {(float)__ldg(u + im), (float)__ldg(u + npts + im), (float)__ldg(u + 2 * npts + im)};
+      const float ph = prof_phi_f(sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]), rpf, rmf, dxf);
+      float vr[3] = {0.f, 0.f, 0.f};
+      if (p.rotation) {
+        vr[0] = wpf[1] * r[2] - wpf[2] * r[1];
+        vr[1] = wpf[2] * r[0] - wpf[0] * r[2];
+        vr[2] = wpf[0] * r[1] - wpf[1] * r[0];
+      }
+      float fp[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        fp[d] = ((vpf[d] + vr[d]) - ug[d]) * ph;
+        f6[d] += fp[d];
+      }
+      f6[3] += r[1] * fp[2] - r[2] * fp[1];
+      f6[4] += r[2] * fp[0] - r[0] * fp[2];
+      f6[5] += r[0] * fp[1] - r[1] * fp[0];
+    }
+  } else
   for (int m = first; m < p.S; m += stride) {
     int rm[3];
     double r[3], dist;
@@ -314,9 +361,38 @@ __global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPa
     }
   }
   KSum acc[9];
+  if constexpr (sizeof(R) == 4) {
+    // warp sums (float hydro terms, plain double LJ terms), then a
+    // compensated double sum over the warps
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-  for (int i = 0; i < 9; ++i) acc[i] = {a9[i], 0.0};
-  block_reduce<9>(acc, sh);
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) f6[i] += __shfl_xor_sync(0xffffffffu, f6[i], o);
+#pragma unroll
+    for (int i = 6; i < 9; ++i)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a9[i] += __shfl_xor_sync(0xffffffffu, a9[i], o);
+    if (lane == 0)
+#pragma unroll
+      for (int i = 0; i < 9; ++i) sh[(2 * i) * 32 + wid] = i < 6 ? (double)f6[i] : a9[i];
+    __syncthreads();
+    if (threadIdx.x < 9) {
+      const int i = threadIdx.x;
+      KSum k{0.0, 0.0};
+      for (int w = 0; w < nw; ++w) k.add(sh[(2 * i) * 32 + w]);
+      sh[(2 * i) * 32] = k.s;
+      sh[(2 * i + 1) * 32] = k.c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int i = 0; i < 9; ++i) acc[i] = {sh[(2 * i) * 32], sh[(2 * i + 1) * 32]};
+  } else {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) acc[i] = {a9[i], 0.0};
+    block_reduce<9>(acc, sh);
+  }
   if (threadIdx.x == 0) {
     double *pp = partial + ((size_t)n * PCL + rank) * 18;
     for (int i = 0; i < 9; ++i) {
@@ -407,6 +483,37 @@ __global__ void __launch_bounds__(256) k_particles_scatter(PPar p, const DPart *
   const double wp[3] = {a.omega[0], a.omega[1], a.omega[2]};
   const StencilBase b = stencil_base(xp, p);
   const size_t npts = (size_t)p.N[0] * p.N[1] * p.N[2];
+  if constexpr (sizeof(R) == 4) {
+    // mixed path: offset, distance, phi and phi*(v + omega x r) in float
+    const float dxf = (float)p.DX, rpf = (float)(p.RADIUS + p.HXI), rmf = (float)(p.RADIUS - p.HXI);
+    const float resf[3] = {(float)b.res[0], (float)b.res[1], (float)b.res[2]};
+    const float vpf[3] = {(float)vp[0], (float)vp[1], (float)vp[2]};
+    const float wpf[3] = {(float)wp[0], (float)wp[1], (float)wp[2]};
+#pragma unroll 2
+    for (int m = first; m < p.S; m += stride) {
+      const int *cell = cells + 3 * m;
+      int rm[3];
+      float r[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);
+        r[d] = (float)cell[d] * dxf - resf[d];
+      }
+      const float ph = prof_phi_f(sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]), rpf, rmf, dxf);
+      float vr[3] = {0.f, 0.f, 0.f};
+      if (p.rotation) {
+        vr[0] = wpf[1] * r[2] - wpf[2] * r[1];
+        vr[1] = wpf[2] * r[0] - wpf[0] * r[2];
+        vr[2] = wpf[0] * r[1] - wpf[1] * r[0];
+      }
+      const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
+      atomicAdd(reinterpret_cast<float *>(phiup) + im, ph);
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        atomicAdd(reinterpret_cast<float *>(phiup) + (1 + d) * npts + im, (vpf[d] + vr[d]) * ph);
+    }
+    return;
+  }
 #pragma unroll 2
   for (int m = first; m < p.S; m += stride) {
     int rm[3];
