@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(256) k_x_inv_op(Geo g, Twiddles<R> tw, const C
   const int ncol = min(KC, g.TZ - kz0);
   for (int it = threadIdx.x; it < NIN * g.KXc * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
-    if (col < ncol) cp_async_cx(Zt + it, in + c * in_cstride + ((size_t)ix * g.KYc + iy) * g.TZ + kz0 + col);
+    if (col < ncol) cp_async_cx(Zt + it, in + c * in_cstride + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
   }
   load_twiddles(twx, tw.x, g.NX);
   cp_async_wait_all();
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(256) k_x_inv_op(Geo g, Twiddles<R> tw, const C
   fft2_smem<R, -1, W>(U, scr, g.lx, 1, W, twx);
   for (int it = threadIdx.x; it < NOUT * g.NX * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
-    if (col < ncol) out[(((size_t)c * g.NX + x) * g.KYc + iy) * g.TZ + kz0 + col] = U[x * W + c * KC + col];
+    if (col < ncol) out[(((size_t)c * g.NX + x) * g.KYc + iy) * g.TS + kz0 + col] = U[x * W + c * KC + col];
   }
 }
 
@@ -110,12 +110,12 @@ __global__ void __launch_bounds__(256) k_x_fwd_op(Geo g, Twiddles<R> tw, const C
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
-  const size_t cstr = (size_t)g.NX * g.KYc * g.TZ;
+  const size_t cstr = (size_t)g.NX * g.KYc * g.TS;
   for (int it = threadIdx.x; it < NIN * g.NX * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
     Cx<R> *d = Pb + x * W + c * KC + col;
     if (col < ncol)
-      cp_async_cx(d, in + c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col);
+      cp_async_cx(d, in + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col);
     else
       *d = {R(0), R(0)};
   }
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(256) k_x_fwd_op(Geo g, Twiddles<R> tw, const C
     const int KXi = ix < g.TX ? ix : ix - g.KXc;
     const int i = KXi >= 0 ? KXi : KXi + g.NX;
     const int kz = kz0 + col;
-    const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
+    const size_t o = ((size_t)ix * g.KYc + iy) * g.TS + kz;
     const Cx<R> *p = Pb + i * W + col;
     const R kx = R(g.wave[0] * KXi), kzr = R(g.wave[2] * kz);
     if (OP == XF_STORE) {
@@ -153,10 +153,10 @@ __global__ void __launch_bounds__(256) k_x_fwd_op(Geo g, Twiddles<R> tw, const C
 }
 
 // Forward z transform of real fields, kz < nkeep kept:
-// in [c][rows][pitch] (planes in_cstride apart) -> out [c][rows][nkeep].
+// in [c][rows][pitch] (planes in_cstride apart) -> out [c][rows][ostride], k < nkeep.
 template <typename R>
 __global__ void __launch_bounds__(256) k_z_r2c(Geo g, Twiddles<R> tw, const R *__restrict__ in, int in_pitch,
-                                               size_t in_cstride, Cx<R> *__restrict__ out, int nkeep) {
+                                               size_t in_cstride, Cx<R> *__restrict__ out, int nkeep, int ostride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int M = g.M;
   constexpr int ES = ZROWS + 1;
@@ -183,10 +183,10 @@ __global__ void __launch_bounds__(256) k_z_r2c(Geo g, Twiddles<R> tw, const R *_
     scr[rr * TA + k] = r2c_post(S + rr, ES, k, M, twz);
   }
   __syncthreads();
-  Cx<R> *dst = out + c * rows * nkeep + row0 * nkeep;
+  Cx<R> *dst = out + c * rows * ostride + row0 * ostride;
   for (int it = threadIdx.x; it < ZROWS * nkeep; it += blockDim.x) {
     const int k = it % nkeep, rr = it / nkeep;
-    dst[it] = scr[rr * TA + k];
+    dst[rr * ostride + k] = scr[rr * TA + k];
   }
 }
 
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(256) k_z_r2c(Geo g, Twiddles<R> tw, const R *_
 // (c, plane, i, j).
 template <typename R>
 __global__ void k_hermitian_planes(Geo g, Cx<R> *__restrict__ spec, int ncomp) {
-  const int M1 = g.M + 1;
+  const int M1 = g.TS;  // row stride of the [c][NX][NY][M+1] spectra
   const int n1 = g.NX, n2 = g.NY, n1h = n1 / 2, n2h = n2 / 2;
   const size_t cstr = (size_t)n1 * n2 * M1;
   const int total = ncomp * 2 * n1 * n2;

@@ -224,9 +224,9 @@ struct BoxBase {
 
 template <typename R>
 struct Box : BoxBase {
-  Cx<R> *zeta = nullptr;  // [2][KXc][KYc][TZ]
-  Cx<R> *bufA = nullptr;  // I1-shaped, 5 comps [c][NX][KYc][TZ]
-  Cx<R> *bufB = nullptr;  // I2-shaped, 5 comps [c][NX][NY][TZ]
+  Cx<R> *zeta = nullptr;  // [2][KXc][KYc][TS]
+  Cx<R> *bufA = nullptr;  // I1-shaped, 5 comps [c][NX][KYc][TS]
+  Cx<R> *bufB = nullptr;  // I2-shaped, 5 comps [c][NX][NY][TS]
   R *ustar = nullptr;     // [3][NX][NY][NZ]
   R *phiup = nullptr;     // [4][NX][NY][NZ]
   Cx<R> *twbuf = nullptr;
@@ -306,9 +306,9 @@ struct Box : BoxBase {
   }
 
   int alloc() override {
-    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
-    const size_t nA = (size_t)g.NX * g.KYc * g.TZ;
-    const size_t nB = (size_t)g.NX * g.NY * g.TZ;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TS;
+    const size_t nA = (size_t)g.NX * g.KYc * g.TS;
+    const size_t nB = (size_t)g.NX * g.NY * g.TS;
     KCHECK(cudaMalloc(&zeta, sizeof(Cx<R>) * 2 * nz));
     KCHECK(cudaMalloc(&bufA, sizeof(Cx<R>) * 5 * nA));
     KCHECK(cudaMalloc(&bufB, sizeof(Cx<R>) * 5 * nB));
@@ -380,15 +380,34 @@ struct Box : BoxBase {
   // this box shape (kapsel_batch_create)
   int ytile_small = 0;
   bool use_pdl = true;
+  // warp-level y pass: persistent grid of YNW-warp blocks, two slots per warp
+  static constexpr int YNW = 4;
+  int yw_occ[2][2] = {{0, 0}, {0, 0}};  // blocks per SM, [inverse][full spectrum]
+  int nsm = 0;
+  template <bool INV, int LY, bool FULL>
+  void yw_launch(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out, bool pdl) {
+    using Y = ZL<LY>;
+    auto kern = k_yw_pass<R, INV, LY, FULL, YNW>;
+    const size_t sm = sizeof(Cx<R>) * 2 * Y::RW * Y::LS * YNW;
+    int &occ = yw_occ[INV ? 1 : 0][FULL ? 1 : 0];
+    if (!occ) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, YNW * 32, sm);
+      occ = std::max(occ, 1);
+    }
+    const int items = nc * gg.NX * ((gg.TZ + Y::RW - 1) / Y::RW);
+    const int grid = std::min((items + YNW - 1) / YNW, occ * nsm);
+    launch_k(pdl, kern, dim3(grid), dim3(YNW * 32), sm, stream, gg, tw, in, out, nc);
+  }
   template <bool INV, int LY>
   void yw(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out, bool pdl) {
-    using Y = ZL<LY>;
-    const int items = nc * gg.NX * ((gg.TZ + Y::RW - 1) / Y::RW);
-    const size_t sm = sizeof(Cx<R>) * Y::RW * Y::LS;
     if (gg.KYc == gg.NY)
-      launch_k(pdl, k_yw_pass<R, INV, LY, true>, dim3(items), dim3(32), sm, stream, gg, tw, in, out, nc);
+      yw_launch<INV, LY, true>(gg, nc, in, out, pdl);
     else
-      launch_k(pdl, k_yw_pass<R, INV, LY, false>, dim3(items), dim3(32), sm, stream, gg, tw, in, out, nc);
+      yw_launch<INV, LY, false>(gg, nc, in, out, pdl);
   }
   template <bool INV>
   void launch_y(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out, bool pdl = false) {
@@ -498,7 +517,7 @@ struct Box : BoxBase {
     // Init_zeta_k gives zeta = 0 and u = 0 (init_fluid.cxx:10-26); the
     // initial rigidity projection (sp_3d_ns.cxx:510-524) is then
     // zeta = U2zeta_k(Solenoidal_u(up - phi*0)), followed by uk_dc = 0.
-    cudaMemsetAsync(zeta, 0, sizeof(Cx<R>) * 2 * (size_t)g.KXc * g.KYc * g.TZ, stream);
+    cudaMemsetAsync(zeta, 0, sizeof(Cx<R>) * 2 * (size_t)g.KXc * g.KYc * g.TS, stream);
     cudaMemsetAsync(ustar, 0, sizeof(R) * 3 * npts(), stream);
     cudaMemsetAsync(uk_dc, 0, sizeof(double) * 3, stream);
     if (Np > 0) {
@@ -509,15 +528,15 @@ struct Box : BoxBase {
   }
 
   // ---- Electrolyte branch (two ion species) --------------------------------
-  Cx<R> *conc_k = nullptr;  // [2][KXc][KYc][TZ]
-  Cx<R> *rho_k = nullptr;   // [KXc][KYc][TZ]
+  Cx<R> *conc_k = nullptr;  // [2][KXc][KYc][TS]
+  Cx<R> *rho_k = nullptr;   // [KXc][KYc][TS]
   R *phiq = nullptr;        // [5][N]: phi, surface charge, normal x/y/z
   R *creal = nullptr;       // [2][N]
   R *gradr = nullptr;       // [3][N]
   R *ureal = nullptr;       // [3][N]
   R *fluxr = nullptr;       // [3][N]
   R *charge = nullptr;      // [N]
-  Cx<R> *F1 = nullptr, *F2 = nullptr;  // full spectra [3][NX][NY][M+1]
+  Cx<R> *F1 = nullptr, *F2 = nullptr;  // full spectra [3][NX][NY][TS of M+1]
   double *scal = nullptr;   // [0] surface-charge scale, [1..2] rescale factors, [3] free volume
   double *partial = nullptr;
   double *total_solute = nullptr;  // [2]
@@ -531,8 +550,9 @@ struct Box : BoxBase {
     gF.TY = g.NY / 2 + 1;
     gF.KYc = g.NY;
     gF.TZ = g.M + 1;
-    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ, N = npts();
-    const size_t nfull = (size_t)g.NX * g.NY * (g.M + 1);
+    gF.TS = (gF.TZ + 3) & ~3;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TS, N = npts();
+    const size_t nfull = (size_t)g.NX * g.NY * gF.TS;
     KCHECK(cudaMalloc(&conc_k, sizeof(Cx<R>) * 2 * nz));
     KCHECK(cudaMalloc(&rho_k, sizeof(Cx<R>) * nz));
     KCHECK(cudaMalloc(&phiq, sizeof(R) * 5 * N));
@@ -584,7 +604,7 @@ struct Box : BoxBase {
 
   // real c_n = A_k2a_out(conc_k[n]) for both species
   void el_conc_real() {
-    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TS;
     k_x_inv_op<R, KCX, XI_IDENT, 2, 2><<<gx(), 256, sm_el, stream>>>(g, tw, conc_k, nz, bufA, KOp{});
     launch_y<true>(g, 2, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 2), 256, sm_el, stream>>>(g, tw, bufB, creal, npts(), g.NZ, PPar{}, nullptr, 0, nullptr);
@@ -601,7 +621,7 @@ struct Box : BoxBase {
   }
   // forward transform of ncomp real fields, 2/3 modes kept, into bufA (I1 layout)
   void el_forward_trunc(const R *real, int ncomp) {
-    k_z_r2c<R><<<dim3(gz(), ncomp), 256, sm_el, stream>>>(g, tw, real, g.NZ, npts(), bufB, g.TZ);
+    k_z_r2c<R><<<dim3(gz(), ncomp), 256, sm_el, stream>>>(g, tw, real, g.NZ, npts(), bufB, g.TZ, g.TS);
     launch_y<false>(g, ncomp, bufB, bufA);
   }
   // inverse of three I1-layout components in bufA into real fields
@@ -611,7 +631,7 @@ struct Box : BoxBase {
   }
 
   void launch_step_el(int euler) {
-    const size_t N = npts(), nz = (size_t)g.KXc * g.KYc * g.TZ;
+    const size_t N = npts(), nz = (size_t)g.KXc * g.KYc * g.TS;
     const double dx3 = prm.dx * prm.dx * prm.dx;
     const double ve[2] = {prm.valency_p, prm.valency_n}, L[2] = {prm.onsager_p, prm.onsager_n};
     const double ieps = 1.0 / prm.dielectric;
@@ -653,8 +673,8 @@ struct Box : BoxBase {
     k_scale_conc<R><<<pb, 256, 0, stream>>>(nz, conc_k, scal);
     k_el_charge<R><<<pb, 256, 0, stream>>>(N, phiq, creal, scal, 1, ve[0], ve[1], charge);
     // full (untruncated) potential gradient with the Ooura inverse semantics
-    const size_t nfull = (size_t)g.NX * g.NY * (g.M + 1);
-    k_z_r2c<R><<<dim3(gz(), 1), 256, sm_el, stream>>>(gF, tw, charge, g.NZ, N, F2, g.M + 1);
+    const size_t nfull = (size_t)g.NX * g.NY * gF.TS;
+    k_z_r2c<R><<<dim3(gz(), 1), 256, sm_el, stream>>>(gF, tw, charge, g.NZ, N, F2, gF.TZ, gF.TS);
     launch_y<false>(gF, 1, F2, F1);
     k_x_fwd_op<R, KCX, XF_GRADPSI_FULL, 1><<<gxF(), 256, sm_el, stream>>>(gF, tw, F1, F2, nfull,
                                                                              KOp{ieps, {0, 0, 0}});
@@ -698,7 +718,7 @@ struct Box : BoxBase {
     const double c1 = neg / (vol * dx3) + -rho_inf / (v1 * (v0 - v1));
     const double tot[2] = {c0 * vol * dx3, c1 * vol * dx3};
     const double Nn = (double)npts();
-    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TS;
     KCHECK(cudaMemsetAsync(conc_k, 0, sizeof(Cx<R>) * 2 * nz, stream));
     const Cx<R> k0[2] = {{(R)(c0 * Nn), (R)0}, {(R)(c1 * Nn), (R)0}};
     KCHECK(cudaMemcpyAsync(conc_k, &k0[0], sizeof(Cx<R>), cudaMemcpyHostToDevice, stream));
@@ -710,7 +730,7 @@ struct Box : BoxBase {
 
   int conc_to_host(double *c) override {
     if (!conc_k) return KAPSEL_ESTATE;
-    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TS;
     std::vector<Cx<R>> h(2 * nz);
     KCHECK(cudaMemcpyAsync(h.data(), conc_k, sizeof(Cx<R>) * h.size(), cudaMemcpyDeviceToHost, stream));
     KCHECK(cudaStreamSynchronize(stream));
@@ -723,7 +743,7 @@ struct Box : BoxBase {
         for (int iy = 0; iy < g.KYc; ++iy) {
           const int j = iy < g.TY ? iy : g.NY + iy - g.KYc;
           for (int k = 0; k < g.TZ; ++k) {
-            const Cx<R> v = h[q * nz + ((size_t)ix * g.KYc + iy) * g.TZ + k];
+            const Cx<R> v = h[q * nz + ((size_t)ix * g.KYc + iy) * g.TS + k];
             double *o = c + q * plane + ((size_t)i * g.NY + j) * NZ_ + 2 * k;
             o[0] = (double)v.x;
             o[1] = (double)v.y;
@@ -751,7 +771,7 @@ struct Box : BoxBase {
   }
 
   int zeta_to_host(double *z) override {
-    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TS;
     std::vector<Cx<R>> h(2 * nz);
     KCHECK(cudaMemcpyAsync(h.data(), zeta, sizeof(Cx<R>) * h.size(), cudaMemcpyDeviceToHost, stream));
     KCHECK(cudaStreamSynchronize(stream));
@@ -764,7 +784,7 @@ struct Box : BoxBase {
         for (int iy = 0; iy < g.KYc; ++iy) {
           const int j = iy < g.TY ? iy : g.NY + iy - g.KYc;
           for (int k = 0; k < g.TZ; ++k) {
-            const Cx<R> v = h[c * nz + ((size_t)ix * g.KYc + iy) * g.TZ + k];
+            const Cx<R> v = h[c * nz + ((size_t)ix * g.KYc + iy) * g.TS + k];
             double *o = z + c * plane + ((size_t)i * g.NY + j) * NZ_ + 2 * k;
             o[0] = (double)v.x;
             o[1] = (double)v.y;
@@ -775,7 +795,7 @@ struct Box : BoxBase {
   }
 
   int zeta_from_host(const double *z) override {
-    const size_t nz = (size_t)g.KXc * g.KYc * g.TZ;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TS;
     std::vector<Cx<R>> h(2 * nz);
     const int NZ_ = g.NZ + 2;
     const size_t plane = (size_t)g.NX * g.NY * NZ_;
@@ -786,7 +806,7 @@ struct Box : BoxBase {
           const int j = iy < g.TY ? iy : g.NY + iy - g.KYc;
           for (int k = 0; k < g.TZ; ++k) {
             const double *o = z + c * plane + ((size_t)i * g.NY + j) * NZ_ + 2 * k;
-            h[c * nz + ((size_t)ix * g.KYc + iy) * g.TZ + k] = {(R)o[0], (R)o[1]};
+            h[c * nz + ((size_t)ix * g.KYc + iy) * g.TS + k] = {(R)o[0], (R)o[1]};
           }
         }
       }
@@ -1273,6 +1293,7 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   g.TX = (g.NX + 2) / 3;
   g.TY = (g.NY + 2) / 3;
   g.TZ = (g.NZ + 2) / 3;
+  g.TS = (g.TZ + 3) & ~3;
   g.KXc = 2 * g.TX - 1;
   g.KYc = 2 * g.TY - 1;
   const double L[3] = {g.NX * p->dx, g.NY * p->dx, g.NZ * p->dx};
@@ -2010,6 +2031,7 @@ extern "C" int kapsel_gpu_solenoidal_u_noalloc(const int *np_xyz, double dx, con
   g.TX = (g.NX + 2) / 3;
   g.TY = (g.NY + 2) / 3;
   g.TZ = (g.NZ + 2) / 3;
+  g.TS = (g.TZ + 3) & ~3;
   g.KXc = 2 * g.TX - 1;
   g.KYc = 2 * g.TY - 1;
   g.wave[0] = 2.0 * M_PI / (g.NX * dx);

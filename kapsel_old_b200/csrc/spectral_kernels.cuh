@@ -2,9 +2,10 @@
 // fused into them.
 //
 // Storage (per field component, complex values in the reference's Ooura sign):
-//   zeta   [2][KXc][KYc][TZ]   reduced vorticity, 2/3-rule modes only
-//   I1     [c][NX][KYc][TZ]    after the x transform (x in real space)
-//   I2     [c][NX][NY][TZ]     after the y transform (x, y in real space)
+//   zeta   [2][KXc][KYc][TS]   reduced vorticity, 2/3-rule modes only
+//   I1     [c][NX][KYc][TS]    after the x transform (x in real space)
+//   I2     [c][NX][NY][TS]     after the y transform (x, y in real space)
+// (kz < TZ is used; rows are padded to TS so that every row starts on 32 bytes)
 //   real   [c][NX][NY][NZ]     real-space fields
 // KXc = 2*TX-1 holds kx = 0..TX-1, -(TX-1)..-1 (compact index ix, kx = ix
 // for ix < TX, else ix - KXc); likewise KYc.  Only kz < TZ is stored.  The
@@ -24,6 +25,7 @@ struct Geo {
   int NX, NY, NZ, M;      // M = NZ/2
   int lx, ly, lm;         // log2 of NX, NY, M
   int TX, TY, TZ;         // TRN = (N+2)/3 (input.cxx:297)
+  int TS;                 // storage stride of the kz dimension: TZ rounded up to 4 (32-byte rows in FP32)
   int KXc, KYc;           // 2*TRN-1
   double wave[3];         // 2 pi / L
   double nu, dt;
@@ -103,11 +105,11 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
-  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
+  const size_t zplane = (size_t)g.KXc * g.KYc * g.TS;
   for (int it = threadIdx.x; it < 2 * g.KXc * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
     if (col < ncol)
-      cp_async_cx(Zt + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TZ + kz0 + col);
+      cp_async_cx(Zt + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
   }
   load_twiddles(twx, tw.x, g.NX);
   cp_async_wait_all();
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
   for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
     if (col < ncol)
-      out[(((size_t)c * g.NX + x) * g.KYc + iy) * g.TZ + kz0 + col] = U[x * W + c * KC + col];
+      out[(((size_t)c * g.NX + x) * g.KYc + iy) * g.TS + kz0 + col] = U[x * W + c * KC + col];
   }
 }
 
@@ -162,8 +164,8 @@ __global__ void __launch_bounds__(256, 3) k_y_pass(Geo g, Twiddles<R> tw, const 
   const int ncol = min(KC, g.TZ - kz0);
   const int rows_in = INVERSE ? g.KYc : g.NY;
   const int rows_out = INVERSE ? g.NY : g.KYc;
-  const Cx<R> *src = in + ((size_t)c * g.NX + x) * rows_in * g.TZ + kz0;
-  Cx<R> *dst = out + ((size_t)c * g.NX + x) * rows_out * g.TZ + kz0;
+  const Cx<R> *src = in + ((size_t)c * g.NX + x) * rows_in * g.TS + kz0;
+  Cx<R> *dst = out + ((size_t)c * g.NX + x) * rows_out * g.TS + kz0;
   // each thread keeps one column and walks rows (256/KC rows apart)
   constexpr int RSTEP = 256 / KC;
   const int col = threadIdx.x % KC, j0 = threadIdx.x / KC;
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(256, 3) k_y_pass(Geo g, Twiddles<R> tw, const 
       srow = abs(KYi) < g.TY ? (KYi >= 0 ? KYi : KYi + g.KYc) : -1;
     }
     if (colok && srow >= 0)
-      cp_async_cx(d, src + (size_t)srow * g.TZ + col);
+      cp_async_cx(d, src + (size_t)srow * g.TS + col);
     else
       *d = {R(0), R(0)};
   }
@@ -187,7 +189,7 @@ __global__ void __launch_bounds__(256, 3) k_y_pass(Geo g, Twiddles<R> tw, const 
   if (colok)
     for (int r = j0; r < rows_out; r += RSTEP) {
       const int j = INVERSE ? r : full_from_compact(r, g.TY, g.KYc, g.NY);
-      dst[(size_t)r * g.TZ + col] = Y[j * KC + col];
+      dst[(size_t)r * g.TS + col] = Y[j * KC + col];
     }
 }
 
@@ -243,10 +245,10 @@ __global__ void __launch_bounds__(256) k_z_products(Geo g, Twiddles<R> tw, Cx<R>
   const int TA = g.TZ + 1;
   const size_t rows = (size_t)g.NX * g.NY;
   const size_t row0 = (size_t)blockIdx.x * ZROWS;
-  const size_t cstr = rows * g.TZ;
+  const size_t cstr = rows * g.TS;
   for (int it = threadIdx.x; it < NV * g.TZ; it += blockDim.x) {
     const int k = it % g.TZ, q = it / g.TZ, c = q % 3, rr = q / 3;
-    cp_async_cx(A + q * TA + k, io + c * cstr + (row0 + rr) * g.TZ + k);
+    cp_async_cx(A + q * TA + k, io + c * cstr + (row0 + rr) * g.TS + k);
   }
   load_twiddles(twm, tw.m, M);
   load_twiddles(twz, tw.z, g.NZ);
@@ -284,7 +286,7 @@ __global__ void __launch_bounds__(256) k_z_products(Geo g, Twiddles<R> tw, Cx<R>
   __syncthreads();
   for (int it = threadIdx.x; it < NQ * g.TZ; it += blockDim.x) {
     const int k = it % g.TZ, q = it / g.TZ, rr = q / 5, c = q % 5;
-    io[c * cstr + (row0 + rr) * g.TZ + k] = O[q * TA + k];
+    io[c * cstr + (row0 + rr) * g.TS + k] = O[q * TA + k];
   }
 }
 
@@ -317,10 +319,10 @@ __global__ void __launch_bounds__(256) k_z_c2r(Geo g, Twiddles<R> tw, const Cx<R
   const int c = blockIdx.y;
   const size_t rows = (size_t)g.NX * g.NY;
   const size_t row0 = (size_t)blockIdx.x * ZROWS;
-  const Cx<R> *src = in + c * rows * g.TZ + row0 * g.TZ;
+  const Cx<R> *src = in + c * rows * g.TS + row0 * g.TS;
   for (int it = threadIdx.x; it < ZROWS * g.TZ; it += blockDim.x) {
     const int k = it % g.TZ, rr = it / g.TZ;
-    cp_async_cx(A + rr * TA + k, src + it);
+    cp_async_cx(A + rr * TA + k, src + rr * g.TS + k);
   }
   load_twiddles(twm, tw.m, M);
   load_twiddles(twz, tw.z, g.NZ);
@@ -409,7 +411,7 @@ __global__ void __launch_bounds__(256) k_z_force(Geo g, Twiddles<R> tw, R *__res
   __syncthreads();
   for (int it = threadIdx.x; it < NS * g.TZ; it += blockDim.x) {
     const int k = it % g.TZ, q = it / g.TZ, d = q % 3, rr = q / 3;
-    out[d * rows * g.TZ + (row0 + rr) * g.TZ + k] = O[q * TA + k];
+    out[d * rows * g.TS + (row0 + rr) * g.TS + k] = O[q * TA + k];
   }
 }
 
@@ -468,20 +470,20 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
-  const size_t cstr = (size_t)g.NX * g.KYc * g.TZ;
-  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
+  const size_t cstr = (size_t)g.NX * g.KYc * g.TS;
+  const size_t zplane = (size_t)g.KXc * g.KYc * g.TS;
   // stage the five product spectra (bit-reversed rows) and the zeta tile
   for (int it = threadIdx.x; it < 5 * g.NX * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
     Cx<R> *d = Pb + x * W5 + c * KC + col;
     if (col < ncol)
-      cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col);
+      cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col);
     else
       *d = {R(0), R(0)};
   }
   for (int it = threadIdx.x; it < 2 * g.KXc * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
-    if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TZ + kz0 + col);
+    if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
   }
   load_twiddles(twx, tw.x, g.NX);
   const bool has_k0 = (iy == 0 && blockIdx.y == 0);
@@ -535,7 +537,7 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
       z0 = {z0.x + dmy * (z0.x - c1 * f0.x), z0.y + dmy * (z0.y - c1 * f0.y)};
       z1 = {z1.x + dmy * (z1.x - c1 * f1.x), z1.y + dmy * (z1.y - c1 * f1.y)};
     }
-    const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
+    const size_t o = ((size_t)ix * g.KYc + iy) * g.TS + kz;
     zeta[o] = z0;
     zeta[zplane + o] = z1;
     Zs[ix * KC + col] = z0;
@@ -569,7 +571,7 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
   fft2_smem<R, -1, W3>(Pb, scr, g.lx, 1, W3, twx);
   for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
-    if (col < ncol) buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col] = Pb[x * W3 + c * KC + col];
+    if (col < ncol) buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col] = Pb[x * W3 + c * KC + col];
   }
 }
 
@@ -594,19 +596,19 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
-  const size_t cstr = (size_t)g.NX * g.KYc * g.TZ;
-  const size_t zplane = (size_t)g.KXc * g.KYc * g.TZ;
+  const size_t cstr = (size_t)g.NX * g.KYc * g.TS;
+  const size_t zplane = (size_t)g.KXc * g.KYc * g.TS;
   for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
     Cx<R> *d = Pb + x * W3 + c * KC + col;
     if (col < ncol)
-      cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TZ + kz0 + col);
+      cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col);
     else
       *d = {R(0), R(0)};
   }
   for (int it = threadIdx.x; it < 2 * g.KXc * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
-    if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TZ + kz0 + col);
+    if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
   }
   load_twiddles(twx, tw.x, g.NX);
   cp_async_wait_all();
@@ -642,7 +644,7 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
     w[2] = cmul_mi(Cx<R>{kx * f1.x - ky * f0.x, kx * f1.y - ky * f0.y});
     Cx<R> z0, z1;
     select_zeta(KXi, KYi, w, z0, z1);
-    const size_t o = ((size_t)ix * g.KYc + iy) * g.TZ + kz;
+    const size_t o = ((size_t)ix * g.KYc + iy) * g.TS + kz;
     zeta[o] = cadd(Zs[ix * KC + col], z0);
     zeta[zplane + o] = cadd(Zs[(g.KXc + ix) * KC + col], z1);
   }

@@ -24,7 +24,7 @@ namespace kapsel {
 
 template <int LM>
 struct ZL {
-  static constexpr int M = 1 << LM, NZ = 2 * M, TZ = (NZ + 2) / 3;
+  static constexpr int M = 1 << LM, NZ = 2 * M, TZ = (NZ + 2) / 3, TS = (TZ + 3) & ~3;
   static constexpr int L1 = ((LM + 1) >> 1) > 4 ? 4 : ((LM + 1) >> 1);
   static constexpr int N1 = 1 << L1, L2 = LM - L1, N2 = 1 << L2;
   static constexpr int RW = 32 / N2;                         // lines per warp batch
@@ -34,7 +34,7 @@ struct ZL {
   static constexpr int KW = M / 32;                          // k values per lane in pre/post
   static constexpr int LR = L2 > 5 ? 0 : 5 - L2;             // log2(RW)
   static_assert(LM >= 5 && LM <= 8, "line length");
-  static_assert(LM == 8 || 2 * LS >= 3 * TZ, "staging fits in two line groups");
+  static_assert(LM == 8 || 2 * LS >= 3 * TS, "staging fits in two line groups");
 };
 
 template <int LM>
@@ -146,27 +146,27 @@ __global__ void __launch_bounds__(NW * 32) k_zw_products(Geo g, Twiddles<R> tw, 
   pdl_begin();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   Cx<R> *buf = reinterpret_cast<Cx<R> *>(smem_raw) + (size_t)warp * 5 * Z::RW * Z::LS;
-  Cx<R> *stage = buf + 3 * Z::RW * Z::LS;  // staged input rows [3][RW][TZ]; later product lines 3, 4
+  Cx<R> *stage = buf + 3 * Z::RW * Z::LS;  // staged input rows [3][RW][TS]; later product lines 3, 4
   Cx<R> wi[Z::N1], wf[Z::N1], wk[Z::KW];
   wfft_twiddles<R, LM, -1>(tw.m, wi);
   wfft_twiddles<R, LM, 1>(tw.m, wf);
   wpre_twiddles<R, LM>(tw.z, wk);
   const size_t rows = (size_t)g.NX * g.NY;
-  const size_t cstr = rows * Z::TZ;
+  const size_t cstr = rows * Z::TS;
   const int ngroups = (int)(rows / Z::RW);
   const R sc = R(g.inv_n);
   for (int grp = blockIdx.x * NW + warp; grp < ngroups; grp += gridDim.x * NW) {
     const size_t row0 = (size_t)grp * Z::RW;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const Cx<R> *src = io + c * cstr + row0 * Z::TZ;
-      for (int i = lane; i < Z::RW * Z::TZ; i += 32) stage[c * Z::RW * Z::TZ + i] = src[i];
+      const Cx<R> *src = io + c * cstr + row0 * Z::TS;
+      for (int i = lane; i < Z::RW * Z::TS; i += 32) stage[c * Z::RW * Z::TS + i] = src[i];
     }
     __syncwarp();
 #pragma unroll
     for (int c = 0; c < 3; ++c)
       for (int rr = 0; rr < Z::RW; ++rr)
-        wpack_c2r<R, LM>(stage + (c * Z::RW + rr) * Z::TZ, buf + (c * Z::RW + rr) * Z::LS, wk);
+        wpack_c2r<R, LM>(stage + (c * Z::RW + rr) * Z::TS, buf + (c * Z::RW + rr) * Z::LS, wk);
     __syncwarp();
 #pragma unroll
     for (int c = 0; c < 3; ++c) wfft<R, LM, -1>(buf + c * Z::RW * Z::LS, wi);
@@ -186,10 +186,10 @@ __global__ void __launch_bounds__(NW * 32) k_zw_products(Geo g, Twiddles<R> tw, 
     for (int q = 0; q < 5; ++q) wfft<R, LM, 1>(buf + q * Z::RW * Z::LS, wf);
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-      Cx<R> *dst = io + q * cstr + row0 * Z::TZ;
+      Cx<R> *dst = io + q * cstr + row0 * Z::TS;
       for (int i = lane; i < Z::RW * Z::TZ; i += 32) {
         const int rr = i / Z::TZ, k = i - rr * Z::TZ;
-        dst[i] = wunpack_r2c<R, LM>(buf + (q * Z::RW + rr) * Z::LS, k, tw.z);
+        dst[rr * Z::TS + k] = wunpack_r2c<R, LM>(buf + (q * Z::RW + rr) * Z::LS, k, tw.z);
       }
     }
     __syncwarp();
@@ -226,10 +226,10 @@ __global__ void __launch_bounds__(NW * 32) k_zw_c2r(Geo g, Twiddles<R> tw, const
   for (int task = blockIdx.x * NW + warp; task < ncomp * ngroups; task += nblk * NW) {
     const int c = task / ngroups;
     const size_t row0 = (size_t)(task - c * ngroups) * Z::RW;
-    const Cx<R> *src = in + c * rows * Z::TZ + row0 * Z::TZ;
-    for (int i = lane; i < Z::RW * Z::TZ; i += 32) stage[i] = src[i];
+    const Cx<R> *src = in + c * rows * Z::TS + row0 * Z::TS;
+    for (int i = lane; i < Z::RW * Z::TS; i += 32) stage[i] = src[i];
     __syncwarp();
-    for (int rr = 0; rr < Z::RW; ++rr) wpack_c2r<R, LM>(stage + rr * Z::TZ, buf + rr * Z::LS, wk);
+    for (int rr = 0; rr < Z::RW; ++rr) wpack_c2r<R, LM>(stage + rr * Z::TS, buf + rr * Z::LS, wk);
     __syncwarp();
     wfft<R, LM, -1>(buf, wi);
     R *dst = out + c * out_cstride + row0 * (size_t)out_pitch;
@@ -318,10 +318,10 @@ __global__ void __launch_bounds__(NW * 32) k_zw_force(Geo g, Twiddles<R> tw, R *
     for (int d = 0; d < 3; ++d) wfft<R, LM, 1>(buf + d * Z::RW * Z::LS, wf);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      Cx<R> *dst = out + d * rows * Z::TZ + row0 * Z::TZ;
+      Cx<R> *dst = out + d * rows * Z::TS + row0 * Z::TS;
       for (int i = lane; i < Z::RW * Z::TZ; i += 32) {
         const int rr = i / Z::TZ, k = i - rr * Z::TZ;
-        dst[i] = wunpack_r2c<R, LM>(buf + (d * Z::RW + rr) * Z::LS, k, tw.z);
+        dst[rr * Z::TS + k] = wunpack_r2c<R, LM>(buf + (d * Z::RW + rr) * Z::LS, k, tw.z);
       }
     }
     __syncwarp();
@@ -329,61 +329,79 @@ __global__ void __launch_bounds__(NW * 32) k_zw_force(Geo g, Twiddles<R> tw, R *
 }
 
 // ---------------------------------------------------------------------------
-// y pass with compile-time NY = 2^LY, one warp per work item (as k_y_pass).
-// An item is RW consecutive kz columns of one (component, x) plane: the warp
-// gathers their rows, transforms them as RW lines in its own shared-memory
-// slot and writes the rows back; no block barrier.  Blocks are one warp, so
-// the hardware refills SMs item by item.  FULLY: the retained box spans
-// every ky (the untruncated half spectrum).
-//   inverse: in [c][NX][KYc][TZ] -> out [c][NX][NY][TZ]
-//   forward: in [c][NX][NY][TZ] -> out [c][NX][KYc][TZ] (|ky| < TY kept)
+// y pass with compile-time NY = 2^LY (as k_y_pass).  A work item is RW
+// consecutive kz columns of one (component, x) plane; each warp of a
+// persistent grid walks its items with two shared-memory slots: while it
+// transforms item k from one slot, cp.async brings item k+1 into the other,
+// so the global-memory latency of the gather overlaps the transform.  The
+// gather lands each element straight at its padded-line position.  FULLY:
+// the retained box spans every ky (the untruncated half spectrum).
+//   inverse: in [c][NX][KYc][TS] -> out [c][NX][NY][TS]
+//   forward: in [c][NX][NY][TS] -> out [c][NX][KYc][TS] (|ky| < TY kept)
 template <typename R, bool INVERSE, int LY, bool FULLY>
-__global__ void __launch_bounds__(32, 16) k_yw_pass(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
-                                                    Cx<R> *__restrict__ out, int ncomp) {
+__device__ __forceinline__ void yw_issue(const Geo &g, const Cx<R> *__restrict__ in, Cx<R> *slot, int item,
+                                         int nbatch) {
   using Y = ZL<LY>;
   constexpr int RW = Y::RW, NY = Y::M;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  pdl_begin();
-  const int lane = threadIdx.x;
-  Cx<R> *buf = reinterpret_cast<Cx<R> *>(smem_raw);
-  const int nbatch = (g.TZ + RW - 1) / RW;
-  const int item = blockIdx.x;
-  const int batch = item % nbatch, plane = item / nbatch;  // plane = c*NX + x
-  const int col0 = batch * RW, ncols = min(RW, g.TZ - col0);
-  const int rows_in = INVERSE ? g.KYc : NY;
-  const int rows_out = INVERSE ? NY : g.KYc;
-  const Cx<R> *src = in + (size_t)plane * rows_in * g.TZ + col0;
-  Cx<R> *dst = out + (size_t)plane * rows_out * g.TZ + col0;
-  Cx<R> w[Y::N1];
-  wfft_twiddles<R, LY, INVERSE ? -1 : 1>(tw.y, w);
-  const Cx<R> zero = {R(0), R(0)};
-  // all loads of the item in flight before the first shared store
   constexpr int TYc = FULLY ? NY / 2 + 1 : (NY + 2) / 3, KYc = FULLY ? NY : 2 * TYc - 1;
-  constexpr int RIN = INVERSE ? KYc : NY, NIT = (RIN * RW + 31) / 32;
-  Cx<R> v[NIT];
-#pragma unroll
-  for (int q = 0; q < NIT; ++q) {
-    const int i = lane + 32 * q, r = i >> Y::LR, col = i & (RW - 1);
-    v[q] = (i < RIN * RW && col < ncols) ? src[(size_t)r * g.TZ + col] : zero;
-  }
-#pragma unroll
-  for (int q = 0; q < NIT; ++q) {
-    const int i = lane + 32 * q, r = i >> Y::LR, col = i & (RW - 1);
+  constexpr int RIN = INVERSE ? KYc : NY;
+  const int lane = threadIdx.x & 31;
+  const int batch = item % nbatch, plane = item / nbatch;
+  const int col0 = batch * RW, ncols = min(RW, g.TZ - col0);
+  const Cx<R> *src = in + (size_t)plane * RIN * g.TS + col0;
+  const Cx<R> zero = {R(0), R(0)};
+  for (int i = lane; i < RIN * RW; i += 32) {
+    const int r = i >> Y::LR, col = i & (RW - 1);
     const int j = INVERSE ? (r < TYc ? r : NY + r - KYc) : r;
-    if (i < RIN * RW) buf[col * Y::LS + zpos<LY>(j)] = v[q];
+    Cx<R> *d = slot + col * Y::LS + zpos<LY>(j);
+    if (col < ncols)
+      cp_async_cx(d, src + (size_t)r * g.TS + col);
+    else
+      *d = zero;
   }
   if (INVERSE)
     for (int i = lane; i < (NY - KYc) * RW; i += 32) {
       const int j = TYc + (i >> Y::LR), col = i & (RW - 1);
-      buf[col * Y::LS + zpos<LY>(j)] = zero;
+      slot[col * Y::LS + zpos<LY>(j)] = zero;
     }
-  __syncwarp();
-  wfft<R, LY, INVERSE ? -1 : 1>(buf, w);
-  for (int i = lane; i < rows_out * RW; i += 32) {
-    const int r = i >> Y::LR, col = i & (RW - 1);
-    const int j = INVERSE ? r : full_from_compact(r, g.TY, g.KYc, NY);
-    if (col < ncols) dst[(size_t)r * g.TZ + col] = buf[col * Y::LS + zpos<LY>(j)];
+}
+
+template <typename R, bool INVERSE, int LY, bool FULLY, int NW>
+__global__ void __launch_bounds__(NW * 32) k_yw_pass(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
+                                                     Cx<R> *__restrict__ out, int ncomp) {
+  using Y = ZL<LY>;
+  constexpr int RW = Y::RW, NY = Y::M, SLOT = RW * Y::LS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_begin();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  Cx<R> *slots = reinterpret_cast<Cx<R> *>(smem_raw) + (size_t)warp * 2 * SLOT;
+  const int nbatch = (g.TZ + RW - 1) / RW;
+  const int nitems = ncomp * g.NX * nbatch;
+  const int rows_out = INVERSE ? NY : g.KYc;
+  Cx<R> w[Y::N1];
+  wfft_twiddles<R, LY, INVERSE ? -1 : 1>(tw.y, w);
+  const int stride = gridDim.x * NW;
+  int item = blockIdx.x * NW + warp;
+  if (item < nitems) yw_issue<R, INVERSE, LY, FULLY>(g, in, slots, item, nbatch);
+  cp_async_commit();
+  for (int k = 0; item < nitems; ++k, item += stride) {
+    Cx<R> *cur = slots + (k & 1) * SLOT;
+    if (item + stride < nitems) yw_issue<R, INVERSE, LY, FULLY>(g, in, slots + ((k + 1) & 1) * SLOT, item + stride, nbatch);
+    cp_async_commit();
+    cp_async_wait_group<1>();
+    __syncwarp();
+    wfft<R, LY, INVERSE ? -1 : 1>(cur, w);
+    const int batch = item % nbatch, plane = item / nbatch;
+    const int col0 = batch * RW, ncols = min(RW, g.TZ - col0);
+    Cx<R> *dst = out + (size_t)plane * rows_out * g.TS + col0;
+    for (int i = lane; i < rows_out * RW; i += 32) {
+      const int r = i >> Y::LR, col = i & (RW - 1);
+      const int j = INVERSE ? r : full_from_compact(r, g.TY, g.KYc, NY);
+      if (col < ncols) dst[(size_t)r * g.TS + col] = cur[col * Y::LS + zpos<LY>(j)];
+    }
+    __syncwarp();
   }
+  cp_async_wait_all();
 }
 
 }  // namespace kapsel
