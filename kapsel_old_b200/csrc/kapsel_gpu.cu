@@ -237,6 +237,58 @@ struct Box : BoxBase {
 
   size_t npts() const { return (size_t)g.NX * g.NY * g.NZ; }
 
+  // x passes with compile-time NX for NX = 32..256 (the runtime-NX kernels otherwise)
+  template <int LX>
+  int x_setup() {
+    KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R, KCX, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
+    KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX, 0, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_xadv));
+    KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX, 1, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_xadv));
+    KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xf));
+    return 0;
+  }
+  template <int LX>
+  void xz_l(bool pdl, const Cx<R> *z, const double *u, Cx<R> *out) {
+    launch_k(pdl, k_x_zeta_to_u<R, KCX, LX>, gx(), dim3(256), smem_xu, stream, g, tw, z, u, out);
+  }
+  template <int EU, int LX>
+  void xa_l(bool pdl) {
+    launch_k(pdl, k_x_advect_update<R, KCX, EU, LX>, gx(), dim3(256), smem_xadv, stream, g, tw, bufA, zeta, uk_dc);
+  }
+  template <int LX>
+  void xf_l(bool pdl, const Cx<R> *in) {
+    launch_k(pdl, k_x_force_to_zeta<R, KCX, LX>, gx(), dim3(256), smem_xf, stream, g, tw, in, zeta, uk_dc);
+  }
+  void x_zeta(bool pdl, const Cx<R> *z, const double *u, Cx<R> *out) {
+    switch (g.NX) {
+      case 32: xz_l<5>(pdl, z, u, out); return;
+      case 64: xz_l<6>(pdl, z, u, out); return;
+      case 128: xz_l<7>(pdl, z, u, out); return;
+      case 256: xz_l<8>(pdl, z, u, out); return;
+      default: xz_l<0>(pdl, z, u, out);
+    }
+  }
+  template <int EU>
+  void x_advect(bool pdl) {
+    switch (g.NX) {
+      case 32: xa_l<EU, 5>(pdl); return;
+      case 64: xa_l<EU, 6>(pdl); return;
+      case 128: xa_l<EU, 7>(pdl); return;
+      case 256: xa_l<EU, 8>(pdl); return;
+      default: xa_l<EU, 0>(pdl);
+    }
+  }
+  void x_force(bool pdl, const Cx<R> *in) {
+    switch (g.NX) {
+      case 32: xf_l<5>(pdl, in); return;
+      case 64: xf_l<6>(pdl, in); return;
+      case 128: xf_l<7>(pdl, in); return;
+      case 256: xf_l<8>(pdl, in); return;
+      default: xf_l<0>(pdl, in);
+    }
+  }
+
   // warp-level z kernels for NZ = 64, 128, 256 (zw = log2(NZ/2)); 0: block-level
   static constexpr int ZNW = sizeof(R) == 4 ? 8 : 4;  // warps per block
   int zw = 0;
@@ -350,6 +402,11 @@ struct Box : BoxBase {
     if (smem_xadv > mx || smem_xu > mx || smem_y > mx || smem_zp > mx) return KAPSEL_ERANGE;
     {
       int rc = 0;
+      if (g.NX == 32) rc = x_setup<5>();
+      else if (g.NX == 64) rc = x_setup<6>();
+      else if (g.NX == 128) rc = x_setup<7>();
+      else if (g.NX == 256) rc = x_setup<8>();
+      if (rc) return rc;
       if (g.NZ == 64) rc = zw_setup<5>();
       else if (g.NZ == 128) rc = zw_setup<6>();
       else if (g.NZ == 256) rc = zw_setup<7>();
@@ -451,7 +508,7 @@ struct Box : BoxBase {
 
   // zeta -> u* (real) through launches 1,2,(7); used by the velocity readout
   void launch_zeta_to_real(R *out, size_t cstride, int pitch) {
-    k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
+    x_zeta(false, zeta, uk_dc, bufA);
     launch_y<true>(g, 3, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, out, cstride, pitch, PPar{}, nullptr, 0, nullptr);
   }
@@ -460,7 +517,7 @@ struct Box : BoxBase {
   void launch_force_to_zeta() {
     zdisp_force(false);
     launch_y<false>(g, 3, bufB, bufA);
-    k_x_force_to_zeta<R, KCX><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc);
+    x_force(false, bufA);
   }
 
   void launch_step(const double *noise, int euler, cudaEvent_t *ev = nullptr) override {
@@ -475,7 +532,7 @@ struct Box : BoxBase {
     const bool pdl = use_pdl && !ev;  // events between launches break the programmatic chain
     const Cx<R> *czeta = zeta;
     mark();
-    k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, czeta, (const double *)uk_dc, bufA);
+    x_zeta(false, czeta, (const double *)uk_dc, bufA);
     mark();
     launch_y<true>(g, 3, bufA, bufB, pdl);
     mark();
@@ -483,7 +540,7 @@ struct Box : BoxBase {
     mark();
     launch_y<false>(g, 5, bufB, bufA, pdl);
     mark();
-    launch_k(pdl, k_x_advect_update<R, KCX, 0>, gx(), dim3(256), smem_xadv, stream, g, tw, bufA, zeta, uk_dc);
+    x_advect<0>(pdl);
     mark();
     launch_y<true>(g, 3, bufA, bufB, pdl);
     mark();
@@ -507,8 +564,7 @@ struct Box : BoxBase {
       mark();
       launch_y<false>(g, 3, bufB, bufA, pdl);
       mark();
-      launch_k(pdl, k_x_force_to_zeta<R, KCX>, gx(), dim3(256), smem_xf, stream, g, tw, (const Cx<R> *)bufA, zeta,
-               uk_dc);
+      x_force(pdl, (const Cx<R> *)bufA);
       mark();
     }
   }
@@ -647,12 +703,12 @@ struct Box : BoxBase {
     k_x_inv_op<R, KCX, XI_GRADPSI, 1, 3><<<gx(), 256, sm_el, stream>>>(g, tw, rho_k, nz, bufA, gp);
     el_inverse3(gradr);
     // Rhs_NS_solute: u, the advection term and the explicit Euler update of zeta
-    k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
+    x_zeta(false, zeta, uk_dc, bufA);
     launch_y<true>(g, 3, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(g, tw, bufB, ureal, N, g.NZ, PPar{}, nullptr, 0, nullptr);
     k_z_products<R><<<gz(), 256, smem_zp, stream>>>(g, tw, bufB);
     launch_y<false>(g, 5, bufB, bufA);
-    k_x_advect_update<R, KCX, 1><<<gx(), 256, smem_xadv, stream>>>(g, tw, bufA, zeta, uk_dc);
+    x_advect<1>(false);
     // ion fluxes and the Euler update of each concentration
     for (int n = 0; n < 2; ++n) {
       KOp dk{prm.kbt * L[n], {0, 0, 0}};
@@ -687,9 +743,9 @@ struct Box : BoxBase {
                                             ext ? prm.e_ext[2] : 0.0, prm.dt / prm.rho, fluxr);
     // u += f dt/rho; Solenoidal_u: in k-space zeta += zeta(sol f), uk_dc += f(0)
     el_forward_trunc(fluxr, 3);
-    k_x_force_to_zeta<R, KCX><<<gx(), 256, smem_xf, stream>>>(g, tw, bufA, zeta, uk_dc);
+    x_force(false, bufA);
     // u (real) of the updated zeta, then the particle part of the step
-    k_x_zeta_to_u<R, KCX><<<gx(), 256, smem_xu, stream>>>(g, tw, zeta, uk_dc, bufA);
+    x_zeta(false, zeta, uk_dc, bufA);
     launch_y<true>(g, 3, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, N, g.NZ, PPar{}, nullptr, 0, nullptr);
     if (Np > 0) {

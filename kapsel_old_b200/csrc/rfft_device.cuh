@@ -124,8 +124,11 @@ __device__ __forceinline__ void phase2_item(Cx<R> *data, const Cx<R> *scr, int s
 // Transforms NSEQ lines of length 2^logn in place; element e of line s is at
 // data[s*ss + e*es]; scr holds at least NSEQ*N values; tw[j] = exp(+2 pi i j/N).
 // All threads of the block call it; it ends with a barrier.
-template <typename R, int SIGN, int NSEQ>
-__device__ void fft2_smem(Cx<R> *data, Cx<R> *scr, int logn, int ss, int es, const Cx<R> *tw) {
+// LOGN > 0 fixes the length at compile time (constant indexing and loop
+// bounds); LOGN = 0 takes it from logn_rt.
+template <typename R, int SIGN, int NSEQ, int LOGN = 0>
+__device__ __forceinline__ void fft2_smem(Cx<R> *data, Cx<R> *scr, int logn_rt, int ss, int es, const Cx<R> *tw) {
+  const int logn = LOGN > 0 ? LOGN : logn_rt;
   const int N = 1 << logn;
   const int N1 = fft2_n1(logn), N2 = N / N1;
   for (int it = threadIdx.x; it < NSEQ * N2; it += blockDim.x) {

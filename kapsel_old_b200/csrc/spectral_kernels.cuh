@@ -92,16 +92,17 @@ __device__ __forceinline__ void select_zeta(int KXi, int KYi, const Cx<R> w[3], 
 // ---------------------------------------------------------------------------
 // x pass, inverse: zeta -> u_k (Zeta_k2u_k) -> inverse x transform.
 // grid (KYc, ceil(TZ/KC)), out I1[3][NX][KYc][TZ].
-template <typename R, int KC>
+template <typename R, int KC, int LX = 0>
 __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ zeta,
                                                      const double *__restrict__ uk_dc, Cx<R> *__restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_begin();
+  const int NXv = LX > 0 ? (1 << LX) : g.NX, LXv = LX > 0 ? LX : g.lx;
   constexpr int W = 3 * KC;
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
-  Cx<R> *Zt = twx + g.NX;          // [2][KXc][KC] staged zeta tile
+  Cx<R> *Zt = twx + NXv;          // [2][KXc][KC] staged zeta tile
   Cx<R> *U = Zt + 2 * g.KXc * KC;  // [NX rows][3*KC]
-  Cx<R> *scr = U + g.NX * W;       // FFT scratch, NX*3*KC
+  Cx<R> *scr = U + NXv * W;       // FFT scratch, NX*3*KC
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
@@ -111,15 +112,15 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
     if (col < ncol)
       cp_async_cx(Zt + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
   }
-  load_twiddles(twx, tw.x, g.NX);
+  load_twiddles(twx, tw.x, NXv);
   cp_async_wait_all();
   __syncthreads();
   const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
   const R ky = R(g.wave[1] * KYi);
-  for (int it = threadIdx.x; it < g.NX * KC; it += blockDim.x) {
+  for (int it = threadIdx.x; it < NXv * KC; it += blockDim.x) {
     const int col = it % KC, i = it / KC;
     Cx<R> u[3] = {{R(0), R(0)}, {R(0), R(0)}, {R(0), R(0)}};
-    const int KXi = signed_k(i, g.NX);
+    const int KXi = signed_k(i, NXv);
     if (col < ncol && abs(KXi) < g.TX) {
       const int ix = KXi >= 0 ? KXi : KXi + g.KXc;
       const int kz = kz0 + col;
@@ -139,11 +140,11 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
     U[i * W + 2 * KC + col] = u[2];
   }
   __syncthreads();
-  fft2_smem<R, -1, W>(U, scr, g.lx, 1, W, twx);
-  for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
+  fft2_smem<R, -1, W, LX>(U, scr, LXv, 1, W, twx);
+  for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
     if (col < ncol)
-      out[(((size_t)c * g.NX + x) * g.KYc + iy) * g.TS + kz0 + col] = U[x * W + c * KC + col];
+      out[(((size_t)c * NXv + x) * g.KYc + iy) * g.TS + kz0 + col] = U[x * W + c * KC + col];
   }
 }
 
@@ -456,25 +457,26 @@ __global__ void __launch_bounds__(256) k_z_r2c_full(Geo g, Twiddles<R> tw, const
 // NSsolute_solver_Euler (Add_zeta_viscous_term then Field_solver_Euler,
 // fluid_solver.cxx:122-135, operate_omega.cxx:172-184) instead of the slaved
 // step, and no u* output (the electrolyte rebuilds u after the Coulomb force).
-template <typename R, int KC, int EULER = 0>
+template <typename R, int KC, int EULER = 0, int LX = 0>
 __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ buf,
                                                          Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_begin();
+  const int NXv = LX > 0 ? (1 << LX) : g.NX, LXv = LX > 0 ? LX : g.lx;
   constexpr int W5 = 5 * KC, W3 = 3 * KC;
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
-  Cx<R> *Zs = twx + g.NX;               // [2][KXc][KC] zeta tile (updated in place)
+  Cx<R> *Zs = twx + NXv;               // [2][KXc][KC] zeta tile (updated in place)
   Cx<R> *Pb = Zs + 2 * g.KXc * KC;       // [NX][5*KC], later [NX][3*KC]
-  Cx<R> *scr = Pb + g.NX * W5;            // FFT scratch
+  Cx<R> *scr = Pb + NXv * W5;            // FFT scratch
   __shared__ double ukd[3];
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
-  const size_t cstr = (size_t)g.NX * g.KYc * g.TS;
+  const size_t cstr = (size_t)NXv * g.KYc * g.TS;
   const size_t zplane = (size_t)g.KXc * g.KYc * g.TS;
   // stage the five product spectra (bit-reversed rows) and the zeta tile
-  for (int it = threadIdx.x; it < 5 * g.NX * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
+  for (int it = threadIdx.x; it < 5 * NXv * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
     Cx<R> *d = Pb + x * W5 + c * KC + col;
     if (col < ncol)
       cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col);
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
     const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
     if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
   }
-  load_twiddles(twx, tw.x, g.NX);
+  load_twiddles(twx, tw.x, NXv);
   const bool has_k0 = (iy == 0 && blockIdx.y == 0);
   if (threadIdx.x < 3) {
     double v = 0.0;
@@ -497,14 +499,14 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
   }
   cp_async_wait_all();
   __syncthreads();
-  fft2_smem<R, 1, W5>(Pb, scr, g.lx, 1, W5, twx);
+  fft2_smem<R, 1, W5, LX>(Pb, scr, LXv, 1, W5, twx);
   const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
   const R ky = R(g.wave[1] * KYi);
   for (int it = threadIdx.x; it < g.KXc * KC; it += blockDim.x) {
     const int col = it % KC, ix = it / KC;
     if (col >= ncol) continue;
     const int KXi = ix < g.TX ? ix : ix - g.KXc;
-    const int i = KXi >= 0 ? KXi : KXi + g.NX;
+    const int i = KXi >= 0 ? KXi : KXi + NXv;
     const int kz = kz0 + col;
     const R k1 = R(g.wave[0] * KXi), k2 = ky, k3 = R(g.wave[2] * kz);
     const Cx<R> *p = Pb + i * W5 + col;
@@ -546,10 +548,10 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
   if (EULER) return;
   __syncthreads();
   // u*_k = Zeta_k2u_k(zeta', uk_dc) on all NX rows (zero outside |kx| < TX)
-  for (int it = threadIdx.x; it < g.NX * KC; it += blockDim.x) {
+  for (int it = threadIdx.x; it < NXv * KC; it += blockDim.x) {
     const int col = it % KC, i = it / KC;
     Cx<R> u[3] = {{R(0), R(0)}, {R(0), R(0)}, {R(0), R(0)}};
-    const int KXi = signed_k(i, g.NX);
+    const int KXi = signed_k(i, NXv);
     if (col < ncol && abs(KXi) < g.TX) {
       const int ix = KXi >= 0 ? KXi : KXi + g.KXc;
       const int kz = kz0 + col;
@@ -568,9 +570,9 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
     Pb[i * W3 + 2 * KC + col] = u[2];
   }
   __syncthreads();
-  fft2_smem<R, -1, W3>(Pb, scr, g.lx, 1, W3, twx);
-  for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
+  fft2_smem<R, -1, W3, LX>(Pb, scr, LXv, 1, W3, twx);
+  for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
     if (col < ncol) buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col] = Pb[x * W3 + c * KC + col];
   }
 }
@@ -583,23 +585,24 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
 // The velocity before the force is Zeta_k2u of the truncated zeta, so its
 // own U2zeta_k is that zeta again (linearity; parity up to roundoff).
 // in buf [3][NX][KYc][TZ].  grid (KYc, ceil(TZ/KC)).
-template <typename R, int KC>
+template <typename R, int KC, int LX = 0>
 __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ buf,
                                                          Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_begin();
+  const int NXv = LX > 0 ? (1 << LX) : g.NX, LXv = LX > 0 ? LX : g.lx;
   constexpr int W3 = 3 * KC;
   Cx<R> *twx = reinterpret_cast<Cx<R> *>(smem_raw);
-  Cx<R> *Zs = twx + g.NX;          // [2][KXc][KC]
+  Cx<R> *Zs = twx + NXv;          // [2][KXc][KC]
   Cx<R> *Pb = Zs + 2 * g.KXc * KC;  // [NX][3*KC]
-  Cx<R> *scr = Pb + g.NX * W3;       // FFT scratch
+  Cx<R> *scr = Pb + NXv * W3;       // FFT scratch
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
-  const size_t cstr = (size_t)g.NX * g.KYc * g.TS;
+  const size_t cstr = (size_t)NXv * g.KYc * g.TS;
   const size_t zplane = (size_t)g.KXc * g.KYc * g.TS;
-  for (int it = threadIdx.x; it < 3 * g.NX * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest & (g.NX - 1), c = rest >> g.lx;
+  for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
     Cx<R> *d = Pb + x * W3 + c * KC + col;
     if (col < ncol)
       cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col);
@@ -610,17 +613,17 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
     const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
     if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
   }
-  load_twiddles(twx, tw.x, g.NX);
+  load_twiddles(twx, tw.x, NXv);
   cp_async_wait_all();
   __syncthreads();
-  fft2_smem<R, 1, W3>(Pb, scr, g.lx, 1, W3, twx);
+  fft2_smem<R, 1, W3, LX>(Pb, scr, LXv, 1, W3, twx);
   const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
   const R ky = R(g.wave[1] * KYi);
   for (int it = threadIdx.x; it < g.KXc * KC; it += blockDim.x) {
     const int col = it % KC, ix = it / KC;
     if (col >= ncol) continue;
     const int KXi = ix < g.TX ? ix : ix - g.KXc;
-    const int i = KXi >= 0 ? KXi : KXi + g.NX;
+    const int i = KXi >= 0 ? KXi : KXi + NXv;
     const int kz = kz0 + col;
     const R kx = R(g.wave[0] * KXi), kzr = R(g.wave[2] * kz);
     const Cx<R> *p = Pb + i * W3 + col;
