@@ -124,6 +124,20 @@ int kapsel_gpu_get_velocity(kapsel_ctx *ctx, double *u);
 int kapsel_gpu_get_particles(kapsel_ctx *ctx, double *out);
 int kapsel_gpu_set_particle_state(kapsel_ctx *ctx, const double *in);
 
+/* Restart records.  save writes the state that Save_Restart_udf
+   (resume.cxx:10-78, 166-272) records -- zeta over all NX*NY*NZ_ Ooura
+   entries, uk_dc, the particles, jikan, and the concentrations in the
+   Electrolyte branch -- as `<path> = <value>` text lines with the
+   reference's record paths (resume.CONTINUE.Saved_Data.Zeta[i][j][k].zeta0,
+   ...Particles[n].R.x, ...jikan.ts, ...).  load reads such a file (lines may
+   carry a leading `record <n> `) into an initialised context as
+   Force_restore_parameters does (resume.cxx:274-365, 366-512): quaternions
+   normalised, x_nopbc reset to x, the step counter continuing after the
+   saved jikan.ts, and the thermostat stream seeded afresh and advanced by
+   the one step the reference's resumed run takes before it restores. */
+int kapsel_gpu_save_restart(kapsel_ctx *ctx, const char *path);
+int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path);
+
 /* Time step counter jikan.ts and time jikan.time. */
 int kapsel_gpu_get_time(kapsel_ctx *ctx, int *ts, double *time);
 

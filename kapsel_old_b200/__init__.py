@@ -107,6 +107,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_calc_f_hydro": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP, _DP]),
         "kapsel_gpu_calc_fr": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+        "kapsel_gpu_save_restart": (ctypes.c_int, [_VP, ctypes.c_char_p]),
+        "kapsel_gpu_load_restart": (ctypes.c_int, [_VP, ctypes.c_char_p]),
         "kapsel_batch_create": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.c_int, ctypes.c_int,
                                                ctypes.POINTER(_VP)]),
         "kapsel_batch_step": (ctypes.c_int, [_VP, ctypes.c_int]),
@@ -266,6 +268,14 @@ class Simulation:
         a[: self.Np, 27:31] = st["q"]
         a[: self.Np, 31:35] = st["q_old"]
         self._check(self.L.kapsel_gpu_set_particle_state(self.h, _ptr(a)))
+
+    def save_restart(self, path: str):
+        """Write the restart records (Save_Restart_udf paths, text)."""
+        self._check(self.L.kapsel_gpu_save_restart(self.h, str(path).encode()))
+
+    def load_restart(self, path: str):
+        """Restore from restart records as Force_restore_parameters does."""
+        self._check(self.L.kapsel_gpu_load_restart(self.h, str(path).encode()))
 
     def concentration(self) -> np.ndarray:
         """Ion concentrations (2, NX, NY, NZ_) in the Ooura layout (Electrolyte)."""

@@ -28,6 +28,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "../../include/kapsel_gpu.h"
@@ -193,6 +194,7 @@ struct BoxBase {
   virtual int alloc_el() = 0;
   virtual int init_el() = 0;
   virtual int conc_to_host(double *c) = 0;
+  virtual int conc_from_host(const double *c) = 0;
   virtual void launch_step(const double *noise, int euler, cudaEvent_t *ev = nullptr) = 0;
   virtual void launch_init() = 0;
   virtual int velocity_to_host(double *u) = 0;
@@ -780,6 +782,30 @@ struct Box : BoxBase {
     KCHECK(cudaMemcpyAsync(conc_k, &k0[0], sizeof(Cx<R>), cudaMemcpyHostToDevice, stream));
     KCHECK(cudaMemcpyAsync(conc_k + nz, &k0[1], sizeof(Cx<R>), cudaMemcpyHostToDevice, stream));
     KCHECK(cudaMemcpyAsync(total_solute, tot, sizeof(tot), cudaMemcpyHostToDevice, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    return 0;
+  }
+
+  // Concentration fields (2, NX, NY, NZ_) in the Ooura layout -> compact
+  // retained modes (the others are truncated before any use).
+  int conc_from_host(const double *c) override {
+    if (!conc_k) return KAPSEL_ESTATE;
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TS;
+    std::vector<Cx<R>> h(2 * nz, Cx<R>{R(0), R(0)});
+    const int NZ_ = g.NZ + 2;
+    const size_t plane = (size_t)g.NX * g.NY * NZ_;
+    for (int q = 0; q < 2; ++q)
+      for (int ix = 0; ix < g.KXc; ++ix) {
+        const int i = ix < g.TX ? ix : g.NX + ix - g.KXc;
+        for (int iy = 0; iy < g.KYc; ++iy) {
+          const int j = iy < g.TY ? iy : g.NY + iy - g.KYc;
+          for (int k = 0; k < g.TZ; ++k) {
+            const double *o = c + q * plane + ((size_t)i * g.NY + j) * NZ_ + 2 * k;
+            h[q * nz + ((size_t)ix * g.KYc + iy) * g.TS + k] = {(R)o[0], (R)o[1]};
+          }
+        }
+      }
+    KCHECK(cudaMemcpyAsync(conc_k, h.data(), sizeof(Cx<R>) * h.size(), cudaMemcpyHostToDevice, stream));
     KCHECK(cudaStreamSynchronize(stream));
     return 0;
   }
@@ -2414,6 +2440,216 @@ int kapsel_gpu_nearcontact_pairs(kapsel_ctx *ctx, int *n_pairs) {
   if (!b->nc) return 0;
   KCHECK(cudaStreamSynchronize(b->stream));
   KCHECK(cudaMemcpy(n_pairs, b->nc_count, sizeof(int), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Restart records: Save_Restart_udf / Force_restore_parameters
+// (resume.cxx:10-78, 166-272, 274-365, 366-512) as `path = value` text lines
+// with the reference's record paths (resume.CONTINUE.Saved_Data...).
+namespace {
+
+const char *const kRes = "resume.CONTINUE.Saved_Data.";
+
+// per-particle vectors of Save_Particle_udf, in its order; n = 3 or 4
+struct PField {
+  const char *name;
+  int n;
+};
+const PField kPFields[] = {{"R", 3},           {"v", 3},
+                           {"v_old", 3},       {"q", 4},
+                           {"q_old", 4},       {"f_hydro", 3},
+                           {"f_hydro_previous", 3}, {"f_hydro1", 3},
+                           {"f_slip", 3},      {"f_slip_previous", 3},
+                           {"fr", 3},          {"fr_previous", 3},
+                           {"omega", 3},       {"omega_old", 3},
+                           {"torque_hydro", 3}, {"torque_hydro_previous", 3},
+                           {"torque_hydro1", 3}, {"torque_slip", 3},
+                           {"torque_slip_previous", 3}};
+constexpr int kNPF = sizeof(kPFields) / sizeof(kPFields[0]);
+const char *const kXYZ[3] = {"x", "y", "z"};
+const char *const kQ[4] = {"q0", "q1", "q2", "q3"};
+
+// record values of particle n for field f (from a KAPSEL_P_* record)
+void pfield_values(const double *rec, int f, double *v) {
+  const std::string nm = kPFields[f].name;
+  for (int i = 0; i < 4; ++i) v[i] = 0.0;
+  if (nm == "R") memcpy(v, rec + KAPSEL_P_X, 3 * sizeof(double));
+  else if (nm == "v") memcpy(v, rec + KAPSEL_P_V, 3 * sizeof(double));
+  else if (nm == "v_old") memcpy(v, rec + KAPSEL_P_VOLD, 3 * sizeof(double));
+  else if (nm == "q") memcpy(v, rec + KAPSEL_P_Q, 4 * sizeof(double));
+  else if (nm == "q_old") memcpy(v, rec + KAPSEL_P_QOLD, 4 * sizeof(double));
+  else if (nm == "f_hydro_previous") memcpy(v, rec + KAPSEL_P_FHYDRO, 3 * sizeof(double));
+  else if (nm == "fr_previous") memcpy(v, rec + KAPSEL_P_FR, 3 * sizeof(double));
+  else if (nm == "omega") memcpy(v, rec + KAPSEL_P_OMEGA, 3 * sizeof(double));
+  else if (nm == "omega_old") memcpy(v, rec + KAPSEL_P_OMEGAOLD, 3 * sizeof(double));
+  else if (nm == "torque_hydro_previous") memcpy(v, rec + KAPSEL_P_THYDRO, 3 * sizeof(double));
+  // f_hydro, fr and torque_hydro are zero after reset_Forces; the slip and
+  // electrolyte-diagnostic terms are zero for the spherical particles here
+}
+
+}  // namespace
+
+extern "C" {
+
+int kapsel_gpu_save_restart(kapsel_ctx *ctx, const char *path) {
+  if (!ctx || !path) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (!b->initialised) return KAPSEL_ESTATE;
+  const int NX = b->g.NX, NY = b->g.NY, NZ_ = b->g.NZ + 2;
+  const size_t plane = (size_t)NX * NY * NZ_;
+  std::vector<double> z(2 * plane), uk(3), rec((size_t)KAPSEL_P_STRIDE * std::max(b->Np, 1));
+  int rc = kapsel_gpu_get_zeta(ctx, z.data(), uk.data());
+  if (rc) return rc;
+  rc = kapsel_gpu_get_particles(ctx, rec.data());
+  if (rc) return rc;
+  const bool el = b->prm.eq == KAPSEL_EQ_ELECTROLYTE;
+  std::vector<double> conc(el ? 2 * plane : 0);
+  if (el && (rc = b->conc_to_host(conc.data()))) return rc;
+  FILE *f = fopen(path, "w");
+  if (!f) return KAPSEL_EINVAL;
+  fprintf(f, "resume.Calculation = CONTINUE\n");
+  for (int i = 0; i < NX; ++i)
+    for (int j = 0; j < NY; ++j)
+      for (int k = 0; k < NZ_; ++k) {
+        const size_t im = ((size_t)i * NY + j) * NZ_ + k;
+        fprintf(f, "%sZeta[%d][%d][%d].zeta0 = %.17g\n", kRes, i, j, k, z[im]);
+        fprintf(f, "%sZeta[%d][%d][%d].zeta1 = %.17g\n", kRes, i, j, k, z[plane + im]);
+        if (el)
+          for (int n = 0; n < 2; ++n)
+            fprintf(f, "%sConcentration[%d][%d][%d][%d].ck = %.17g\n", kRes, n, i, j, k, conc[n * plane + im]);
+      }
+  for (int d = 0; d < 3; ++d) fprintf(f, "%suk_dc.%s = %.17g\n", kRes, kXYZ[d], uk[d]);
+  for (int n = 0; n < b->Np; ++n)
+    for (int fi = 0; fi < kNPF; ++fi) {
+      double v[4];
+      pfield_values(rec.data() + (size_t)KAPSEL_P_STRIDE * n, fi, v);
+      for (int c = 0; c < kPFields[fi].n; ++c)
+        fprintf(f, "%sParticles[%d].%s.%s = %.17g\n", kRes, n, kPFields[fi].name,
+                kPFields[fi].n == 4 ? kQ[c] : kXYZ[c], v[c]);
+    }
+  // jikan.ts is the index of the step just completed (the reference saves
+  // inside its step loop, sp_3d_ns.cxx:606-616)
+  fprintf(f, "%sjikan.ts = %d\n", kRes, b->ts - 1);
+  fprintf(f, "%sjikan.time = %.17g\n", kRes, b->time);
+  fprintf(f, "%soblique.degree_oblique = %.17g\n", kRes, 0.0);
+  const bool ok = !ferror(f);
+  fclose(f);
+  return ok ? 0 : KAPSEL_EINVAL;
+}
+
+int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path) {
+  if (!ctx || !path) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (!b->initialised) return KAPSEL_ESTATE;
+  const int NX = b->g.NX, NY = b->g.NY, NZ_ = b->g.NZ + 2, Np = b->Np;
+  const size_t plane = (size_t)NX * NY * NZ_;
+  const bool el = b->prm.eq == KAPSEL_EQ_ELECTROLYTE;
+  std::vector<double> z(2 * plane, 0.0), conc(el ? 2 * plane : 0, 0.0), uk(3, 0.0);
+  std::vector<double> pv((size_t)std::max(Np, 1) * kNPF * 4, 0.0);
+  std::vector<unsigned char> seen((size_t)std::max(Np, 1) * kNPF, 0);
+  size_t nz_seen = 0;
+  int ts = -1, have_time = 0, nuk = 0;
+  double time = 0.0;
+  FILE *f = fopen(path, "r");
+  if (!f) return KAPSEL_EINVAL;
+  std::vector<char> line(1 << 12);
+  const size_t lr = strlen(kRes);
+  int bad = 0;
+  while (fgets(line.data(), (int)line.size(), f)) {
+    char *s = line.data();
+    // the reference's record writer prefixes "record <n> "
+    if (!strncmp(s, "record ", 7)) {
+      s += 7;
+      while (*s && *s != ' ') ++s;
+      while (*s == ' ') ++s;
+    }
+    if (strncmp(s, kRes, lr)) continue;
+    s += lr;
+    char *eq = strchr(s, '=');
+    if (!eq) continue;
+    const double val = strtod(eq + 1, nullptr);
+    int i, j, k, n, c;
+    char name[128], comp[16];
+    if (sscanf(s, "Zeta[%d][%d][%d].zeta%d", &i, &j, &k, &c) == 4) {
+      if (i < 0 || i >= NX || j < 0 || j >= NY || k < 0 || k >= NZ_ || c < 0 || c > 1) { bad = 1; continue; }
+      z[c * plane + ((size_t)i * NY + j) * NZ_ + k] = val;
+      ++nz_seen;
+    } else if (sscanf(s, "Concentration[%d][%d][%d][%d].ck", &n, &i, &j, &k) == 4) {
+      if (!el) continue;
+      if (n < 0 || n > 1 || i < 0 || i >= NX || j < 0 || j >= NY || k < 0 || k >= NZ_) { bad = 1; continue; }
+      conc[n * plane + ((size_t)i * NY + j) * NZ_ + k] = val;
+    } else if (sscanf(s, "uk_dc.%15[a-z]", comp) == 1) {
+      for (int d = 0; d < 3; ++d)
+        if (!strcmp(comp, kXYZ[d])) { uk[d] = val; ++nuk; }
+    } else if (sscanf(s, "Particles[%d].%127[A-Za-z0-9_].%15[a-z0-9]", &n, name, comp) == 3) {
+      if (n < 0 || n >= Np) continue;
+      for (int fi = 0; fi < kNPF; ++fi)
+        if (!strcmp(name, kPFields[fi].name))
+          for (int cc = 0; cc < kPFields[fi].n; ++cc)
+            if (!strcmp(comp, kPFields[fi].n == 4 ? kQ[cc] : kXYZ[cc])) {
+              pv[((size_t)n * kNPF + fi) * 4 + cc] = val;
+              seen[(size_t)n * kNPF + fi] |= (unsigned char)(1u << cc);
+            }
+    } else if (!strncmp(s, "jikan.ts", 8) && (s[8] == ' ' || s[8] == '=')) {
+      ts = (int)strtol(eq + 1, nullptr, 10);
+    } else if (!strncmp(s, "jikan.time", 10)) {
+      time = val;
+      have_time = 1;
+    }
+  }
+  fclose(f);
+  if (bad || nz_seen != 2 * plane || nuk != 3 || ts < 0 || !have_time) return KAPSEL_EINVAL;
+  for (int n = 0; n < Np; ++n)
+    for (int fi = 0; fi < kNPF; ++fi) {
+      const std::string nm = kPFields[fi].name;
+      const bool needed = nm == "R" || nm == "v" || nm == "v_old" || nm == "q" || nm == "q_old" ||
+                          nm == "omega" || nm == "omega_old" || nm == "fr_previous";
+      if (needed && seen[(size_t)n * kNPF + fi] != (1u << kPFields[fi].n) - 1) return KAPSEL_EINVAL;
+    }
+  // Read_Particle_udf (resume.cxx:366-512): quaternions normalised, the
+  // unwrapped position restarts at the position
+  std::vector<double> rec((size_t)KAPSEL_P_STRIDE * std::max(Np, 1), 0.0);
+  auto fld = [&](int n, const char *nm) -> const double * {
+    for (int fi = 0; fi < kNPF; ++fi)
+      if (!strcmp(kPFields[fi].name, nm)) return &pv[((size_t)n * kNPF + fi) * 4];
+    return nullptr;
+  };
+  for (int n = 0; n < Np; ++n) {
+    double *o = rec.data() + (size_t)KAPSEL_P_STRIDE * n;
+    memcpy(o + KAPSEL_P_X, fld(n, "R"), 3 * sizeof(double));
+    memcpy(o + KAPSEL_P_XNOPBC, fld(n, "R"), 3 * sizeof(double));
+    memcpy(o + KAPSEL_P_V, fld(n, "v"), 3 * sizeof(double));
+    memcpy(o + KAPSEL_P_VOLD, fld(n, "v_old"), 3 * sizeof(double));
+    memcpy(o + KAPSEL_P_OMEGA, fld(n, "omega"), 3 * sizeof(double));
+    memcpy(o + KAPSEL_P_OMEGAOLD, fld(n, "omega_old"), 3 * sizeof(double));
+    memcpy(o + KAPSEL_P_FHYDRO, fld(n, "f_hydro_previous"), 3 * sizeof(double));
+    memcpy(o + KAPSEL_P_THYDRO, fld(n, "torque_hydro_previous"), 3 * sizeof(double));
+    memcpy(o + KAPSEL_P_FR, fld(n, "fr_previous"), 3 * sizeof(double));
+    for (int which = 0; which < 2; ++which) {
+      const double *q = fld(n, which ? "q_old" : "q");
+      const double nq = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+      if (!(nq > 0.0)) return KAPSEL_EINVAL;
+      for (int i = 0; i < 4; ++i) o[(which ? KAPSEL_P_QOLD : KAPSEL_P_Q) + i] = q[i] * (1.0 / nq);
+    }
+  }
+  int rc = kapsel_gpu_set_zeta(ctx, z.data(), uk.data());
+  if (rc) return rc;
+  if (el && (rc = b->conc_from_host(conc.data()))) return rc;
+  if (Np > 0 && (rc = kapsel_gpu_set_particle_state(ctx, rec.data()))) return rc;
+  b->ts = ts + 1;
+  b->time = time;
+  // The reference's resumed run seeds the thermostat stream afresh
+  // (MT_seed(GIVEN_SEED, 0), sp_3d_ns.cxx:477) and takes one step before the
+  // restore overwrites the state (sp_3d_ns.cxx:547-627), which draws one
+  // step of normals: the stream continues after those.
+  b->mt.reset(new MT19937(b->prm.mt_seed));
+  if (b->pp.thermostat) {
+    double pair[2];
+    for (int n = 0; n < 3 * Np; ++n) b->mt->gauss2(pair);
+  }
   return 0;
 }
 

@@ -54,6 +54,8 @@ class RefSim:
         L.kref_A2a_k.argtypes = [dp]
         L.kref_A_k2a.argtypes = [dp]
         L.kref_solenoidal_u.argtypes = [dp, dp, dp]
+        L.kref_save_restart.argtypes = [ctypes.c_char_p]
+        L.kref_resume.argtypes = [ctypes.c_char_p]
         L.kref_time_steps.argtypes = [ctypes.c_int]
         L.kref_time_steps.restype = ctypes.c_double
         self.cfg = cfg
@@ -71,6 +73,17 @@ class RefSim:
 
     def step(self, n: int = 1):
         self.lib.kref_step(n)
+
+    def save_restart(self, path: str):
+        """Save_Restart_udf through the stand-in record writer."""
+        assert self.lib.kref_save_restart(str(path).encode()) == 0
+
+    def resume(self, path: str):
+        """The first pass of a resumed run: one step, then Force_restore_parameters."""
+        assert self.lib.kref_resume(str(path).encode()) == 0
+
+    def ts(self) -> int:
+        return int(self.lib.kref_ts())
 
     def time_steps(self, n: int) -> float:
         return self.lib.kref_time_steps(n)

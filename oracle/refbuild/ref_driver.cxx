@@ -11,7 +11,8 @@
  * MT_seed(GIVEN_SEED,0), Init_fft, Mem_alloc_var, Init_Particle, Init_zeta_k,
  * the initial rigidity projection and (electrolyte) Init_rho_ion.  Each step
  * is Time_evolution(...) followed by jikan.time += dt (sp_3d_ns.cxx:593-594).
- * UDF/AVS snapshot output and restart writing are not called.
+ * UDF/AVS snapshot output is not called; restart records are written and
+ * read back on request (kref_save_restart, kref_resume).
  */
 #include "sp_3d_ns.h"
 
@@ -160,6 +161,41 @@ void kref_A_k2a(double *a) { A_k2a(a); }
 void kref_solenoidal_u(double *f0, double *f1, double *f2) {
   double *f[3] = {f0, f1, f2};
   Solenoidal_u(f);
+}
+
+/* Save_Restart_udf as the step loop calls it after its last step
+   (sp_3d_ns.cxx:606-616: jikan.ts is the index of the step just done),
+   written through the stand-in record writer. */
+int kref_save_restart(const char *path) {
+  if (!g_ready) return -1;
+  UDFManager res(path, "", 0);
+  UDFManager *old = ufres;
+  ufres = &res;
+  CTime j = g_jikan;
+  j.ts -= 1;
+  Save_Restart_udf(g_zeta, g_uk_dc, g_particles, j, Concentration);
+  res.write();
+  ufres = old;
+  return 0;
+}
+
+/* The first pass of a resumed run's step loop (sp_3d_ns.cxx:545-627): one
+   Time_evolution at ts = last_ts, then Force_restore_parameters from the
+   restart file, then ts++. */
+int kref_resume(const char *path) {
+  if (!g_ready) return -1;
+  UDFManager in(path);
+  int last_ts = 0;
+  if (!in.get("resume.CONTINUE.Saved_Data.jikan.ts", last_ts)) return -2;
+  g_jikan.ts = last_ts;
+  Time_evolution(g_zeta, g_uk_dc, f_particle, g_particles, g_jikan);
+  g_jikan.time += g_jikan.dt_fluid;
+  UDFManager *old = ufin;
+  ufin = &in;
+  Force_restore_parameters(g_zeta, g_uk_dc, g_particles, g_jikan, Concentration);
+  ufin = old;
+  g_jikan.ts += 1;
+  return 0;
 }
 
 /* Wall-clock seconds of n steps (excludes initialisation). */

@@ -182,6 +182,11 @@ class UDFManager {
     char line[4096];
     while (fgets(line, sizeof line, f)) {
       std::string s(line);
+      /* lines written by write() carry a "record <n> " prefix */
+      if (s.compare(0, 7, "record ") == 0) {
+        size_t sp = s.find(' ', 7);
+        s = sp == std::string::npos ? std::string() : s.substr(sp + 1);
+      }
       size_t hash = s.find('#');
       if (hash != std::string::npos) s.resize(hash);
       size_t eq = s.find('=');
