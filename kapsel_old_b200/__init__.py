@@ -370,3 +370,11 @@ class Batch:
 
 
 __all__ = ["Batch", "Simulation", "KapselError", "load_library", "params_from_config", "FP64", "MIXED", "LIB_PATH"]
+
+
+def simulation_from_udf(path: str, precision: int = FP64, seed: int = 0) -> "Simulation":
+    """A Simulation configured from a KAPSEL input UDF (its define.udf
+    resolved through \\include); see udf_io.to_config for what is supported."""
+    from . import udf_io
+
+    return Simulation(udf_io.to_config(udf_io.read(path), seed=seed), precision=precision)

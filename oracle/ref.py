@@ -30,7 +30,7 @@ class RefSim:
     """One reference simulation.  The reference keeps global state, so each
     instance loads its own private copy of the library (copied to a temp file)."""
 
-    def __init__(self, cfg: dict, omp: bool = False, workdir: str | None = None):
+    def __init__(self, cfg: dict | None, omp: bool = False, workdir: str | None = None, kv_path: str | None = None):
         self._tmp = tempfile.mkdtemp(prefix="kref_", dir=workdir)
         src = lib_path(omp)
         dst = os.path.join(self._tmp, "lib.so")
@@ -59,7 +59,7 @@ class RefSim:
         L.kref_time_steps.argtypes = [ctypes.c_int]
         L.kref_time_steps.restype = ctypes.c_double
         self.cfg = cfg
-        self.kv = udf.write_udf(os.path.join(self._tmp, "input.kv"), cfg)
+        self.kv = kv_path or udf.write_udf(os.path.join(self._tmp, "input.kv"), cfg)
         rc = L.kref_init(self.kv.encode())
         if rc != 0:
             raise RuntimeError(f"kref_init failed: {rc}")
