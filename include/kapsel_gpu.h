@@ -138,6 +138,18 @@ int kapsel_gpu_set_particle_state(kapsel_ctx *ctx, const double *in);
 int kapsel_gpu_save_restart(kapsel_ctx *ctx, const char *path);
 int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path);
 
+/* AVS/Express field snapshot of a Navier_Stokes context, as Output_avs
+   writes it in its BINARY mode on a uniform field (avs_output.cxx:20-342):
+   with init != 0 the header <out_dir>/<out_name>.fld (nstep snapshots) and
+   the coordinate file <out_name>.cod are (re)written and <out_dir>/avs is
+   created; every call appends the snapshot's description to the .fld file
+   and writes <out_dir>/avs/<out_name>_<ts>.dat: float32 columns ux uy uz phi
+   pressure tau_xy tau_yz tau_zx tau_xx tau_yy, x fastest.  phi is the
+   unclamped profile sum of Make_phi_particle; tau is ETA times the
+   symmetric strain rate of the velocity by the spectral formula of
+   Zeta_k2Strain_k; the pressure column is zero (the step computes none). */
+int kapsel_gpu_write_avs(kapsel_ctx *ctx, const char *out_dir, const char *out_name, int nstep, int init);
+
 /* Time step counter jikan.ts and time jikan.time. */
 int kapsel_gpu_get_time(kapsel_ctx *ctx, int *ts, double *time);
 

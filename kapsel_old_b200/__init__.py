@@ -108,6 +108,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_calc_fr": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_strerror": (ctypes.c_char_p, [ctypes.c_int]),
         "kapsel_gpu_save_restart": (ctypes.c_int, [_VP, ctypes.c_char_p]),
+        "kapsel_gpu_write_avs": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
         "kapsel_gpu_load_restart": (ctypes.c_int, [_VP, ctypes.c_char_p]),
         "kapsel_batch_create": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.c_int, ctypes.c_int,
                                                ctypes.POINTER(_VP)]),
@@ -276,6 +277,11 @@ class Simulation:
     def load_restart(self, path: str):
         """Restore from restart records as Force_restore_parameters does."""
         self._check(self.L.kapsel_gpu_load_restart(self.h, str(path).encode()))
+
+    def write_avs(self, out_dir: str, out_name: str, nstep: int, init: bool = False):
+        """Append an AVS field snapshot (Output_avs, binary, uniform field)."""
+        self._check(self.L.kapsel_gpu_write_avs(self.h, str(out_dir).encode(), str(out_name).encode(), int(nstep),
+                                                1 if init else 0))
 
     def concentration(self) -> np.ndarray:
         """Ion concentrations (2, NX, NY, NZ_) in the Ooura layout (Electrolyte)."""

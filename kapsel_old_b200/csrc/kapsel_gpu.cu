@@ -25,6 +25,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <sys/stat.h>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -204,6 +205,7 @@ struct BoxBase {
   virtual int fft_inv_host(double *a) = 0;
   virtual int solenoidal_host(double *u0, double *u1, double *u2) = 0;
   virtual int phi_up_host(double *phi, double *up0, double *up1, double *up2) = 0;
+  virtual int phi_only_host(double *phi) = 0;  // Make_phi_particle: no clamp
   virtual int fhydro_host(const double *u0, const double *u1, const double *u2, double *f, double *t) = 0;
   virtual void free_all() = 0;
 
@@ -901,6 +903,7 @@ struct Box : BoxBase {
   int fft_inv_host(double *a) override;
   int solenoidal_host(double *u0, double *u1, double *u2) override;
   int phi_up_host(double *phi, double *up0, double *up1, double *up2) override;
+  int phi_only_host(double *phi) override;
   int fhydro_host(const double *u0, const double *u1, const double *u2, double *f, double *t) override;
 
   void free_all() override {
@@ -1174,6 +1177,22 @@ int Box<R>::phi_up_host(double *phi, double *up0, double *up1, double *up2) {
   cudaFree(d);
   double *outs[4] = {phi, up0, up1, up2};
   for (int c = 0; c < 4; ++c) unpack_real<R>(outs[c], h.data() + c * npt, g);
+  return 0;
+}
+
+template <typename R>
+int Box<R>::phi_only_host(double *phi) {
+  const size_t npt = npts();
+  R *d = nullptr;
+  KCHECK(cudaMalloc(&d, sizeof(R) * 4 * npt));
+  KCHECK(cudaMemsetAsync(d, 0, sizeof(R) * 4 * npt, stream));
+  if (Np > 0) k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, d);
+  KCHECK(cudaGetLastError());
+  std::vector<R> h(npt);
+  KCHECK(cudaMemcpyAsync(h.data(), d, sizeof(R) * npt, cudaMemcpyDeviceToHost, stream));
+  KCHECK(cudaStreamSynchronize(stream));
+  cudaFree(d);
+  unpack_real<R>(phi, h.data(), g);
   return 0;
 }
 
@@ -2651,6 +2670,119 @@ int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path) {
     for (int n = 0; n < 3 * Np; ++n) b->mt->gauss2(pair);
   }
   return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// AVS/Express field snapshots: Init_avs, Add_field_description and the
+// binary branch of Output_avs (avs_output.cxx:20-109, 162-342), Navier_Stokes
+// columns "ux uy uz phi pressure tau_xy tau_yz tau_zx tau_xx tau_yy".
+namespace {
+
+void avs_binary_write(FILE *f, const double *a, int NX, int NY, int NZ) {
+  // Binary_write (avs_output.cxx:162-175): i fastest, then j, then k
+  const int NZ_ = NZ + 2;
+  std::vector<float> row((size_t)NX);
+  for (int k = 0; k < NZ; ++k)
+    for (int j = 0; j < NY; ++j) {
+      for (int i = 0; i < NX; ++i) row[i] = (float)a[((size_t)i * NY + j) * NZ_ + k];
+      fwrite(row.data(), sizeof(float), row.size(), f);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int kapsel_gpu_write_avs(kapsel_ctx *ctx, const char *out_dir, const char *out_name, int nstep, int init) {
+  if (!ctx || !out_dir || !out_name || nstep < 1) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (!b->initialised) return KAPSEL_ESTATE;
+  if (b->prm.eq != KAPSEL_EQ_NAVIER_STOKES) return KAPSEL_EINVAL;
+  const int NX = b->g.NX, NY = b->g.NY, NZ = b->g.NZ, NZ_ = NZ + 2;
+  const double DX = b->prm.dx, ETA = b->prm.eta;
+  const size_t plane = (size_t)NX * NY * NZ_;
+  const std::string dir(out_dir), name(out_name);
+  const std::string fld = dir + "/" + name + ".fld", cod = name + ".cod";
+  const int veclen = 10;
+  if (init) {
+    mkdir((dir + "/avs").c_str(), 0755);
+    FILE *f = fopen(fld.c_str(), "w");
+    if (!f) return KAPSEL_EINVAL;
+    fprintf(f, "# AVS field file\nndim=%d\ndim1=%d\ndim2=%d\ndim3=%d\nnspace=%d\nveclen=%d\n", 3, NX, NY, NZ, 3,
+            veclen);
+    fprintf(f, "data=float\nfield=uniform\nnstep=%d\n", nstep);
+    fprintf(f, "label = %s\n", "ux uy uz phi pressure tau_xy tau_yz tau_zx tau_xx tau_yy");
+    fclose(f);
+    f = fopen((dir + "/" + cod).c_str(), "wb");
+    if (!f) return KAPSEL_EINVAL;
+    fprintf(f, "%g\n%g\n%g\n%g\n%g\n%g\n", 0.0, (double)(NX - 1) * DX, 0.0, (double)(NY - 1) * DX, 0.0,
+            (double)(NZ - 1) * DX);
+    fclose(f);
+  }
+  // fields in the Ooura real layout [NX][NY][NZ_]
+  std::vector<double> u(3 * plane), phi(plane), strain(5 * plane, 0.0);
+  int rc = b->velocity_to_host(u.data());
+  if (rc) return rc;
+  if ((rc = b->phi_only_host(phi.data()))) return rc;
+  // viscous strain tensor eta*(d_i u_j + d_j u_i)/2 of the velocity, by the
+  // spectral formula of Zeta_k2Strain_k (fft_wrapper.cxx:201-257)
+  std::vector<double> uk(u);
+  for (int c = 0; c < 3; ++c)
+    if ((rc = b->fft_fwd_host(uk.data() + c * plane))) return rc;
+  const double wx = 2.0 * M_PI / (NX * DX), wy = 2.0 * M_PI / (NY * DX), wz = 2.0 * M_PI / (NZ * DX);
+  for (int i = 0; i < NX; ++i)
+    for (int j = 0; j < NY; ++j)
+      for (int k = 0; k < NZ_ / 2; ++k) {
+        const size_t im0 = ((size_t)i * NY + j) * NZ_ + 2 * k, im1 = im0 + 1;
+        const double ks[3] = {(i > NX / 2 ? i - NX : i) * wx * .5, (j > NY / 2 ? j - NY : j) * wy * .5, k * wz * .5};
+        double ud[3][2];
+        for (int d = 0; d < 3; ++d) {
+          ud[d][0] = ETA * uk[d * plane + im0];
+          ud[d][1] = ETA * uk[d * plane + im1];
+        }
+        double *s0 = strain.data();
+        s0[0 * plane + im0] = ks[0] * ud[0][1] * 2.;
+        s0[0 * plane + im1] = -ks[0] * ud[0][0] * 2.;
+        s0[1 * plane + im0] = ks[0] * ud[1][1] + ks[1] * ud[0][1];
+        s0[1 * plane + im1] = -ks[0] * ud[1][0] - ks[1] * ud[0][0];
+        s0[2 * plane + im0] = ks[0] * ud[2][1] + ks[2] * ud[0][1];
+        s0[2 * plane + im1] = -ks[0] * ud[2][0] - ks[2] * ud[0][0];
+        s0[3 * plane + im0] = ks[1] * ud[1][1] * 2.;
+        s0[3 * plane + im1] = -ks[1] * ud[1][0] * 2.;
+        s0[4 * plane + im0] = ks[1] * ud[2][1] + ks[2] * ud[1][1];
+        s0[4 * plane + im1] = -ks[1] * ud[2][0] - ks[2] * ud[1][0];
+      }
+  for (int c = 0; c < 5; ++c)
+    if ((rc = b->fft_inv_host(strain.data() + c * plane))) return rc;
+  // Add_field_description (BINARY, uniform field)
+  const size_t data_size = sizeof(float) * (size_t)NX * NY * NZ;
+  const std::string pfx = "avs/" + name + "_";
+  FILE *f = fopen(fld.c_str(), "a");
+  if (!f) return KAPSEL_EINVAL;
+  fprintf(f, "time value = \"step%dtime%g\"\n", b->ts, b->time);
+  for (int n = 0; n < 3; ++n) fprintf(f, "coord %d file = %s filetype = ascii skip = %d\n", n + 1, cod.c_str(), n * 2);
+  for (int n = 0; n < veclen; ++n)
+    fprintf(f, "variable %d file = %s%d.dat filetype = binary skip = %d\n", n + 1, pfx.c_str(), b->ts,
+            (int)(n * data_size));
+  fprintf(f, "EOT\n");
+  fclose(f);
+  const std::string dat = dir + "/" + pfx + std::to_string(b->ts) + ".dat";
+  f = fopen(dat.c_str(), "wb");
+  if (!f) return KAPSEL_EINVAL;
+  for (int c = 0; c < 3; ++c) avs_binary_write(f, u.data() + c * plane, NX, NY, NZ);
+  avs_binary_write(f, phi.data(), NX, NY, NZ);
+  {
+    // the Navier_Stokes step computes no pressure field
+    std::vector<double> zero(plane, 0.0);
+    avs_binary_write(f, zero.data(), NX, NY, NZ);
+  }
+  const int order[5] = {1, 4, 2, 0, 3};  // xy, yz, zx, xx, yy
+  for (int c = 0; c < 5; ++c) avs_binary_write(f, strain.data() + order[c] * plane, NX, NY, NZ);
+  const bool ok = !ferror(f);
+  fclose(f);
+  return ok ? 0 : KAPSEL_EINVAL;
 }
 
 }  // extern "C"

@@ -55,6 +55,7 @@ class RefSim:
         L.kref_A_k2a.argtypes = [dp]
         L.kref_solenoidal_u.argtypes = [dp, dp, dp]
         L.kref_save_restart.argtypes = [ctypes.c_char_p]
+        L.kref_output_avs.argtypes = [ctypes.c_int]
         L.kref_resume.argtypes = [ctypes.c_char_p]
         L.kref_time_steps.argtypes = [ctypes.c_int]
         L.kref_time_steps.restype = ctypes.c_double
@@ -81,6 +82,10 @@ class RefSim:
     def resume(self, path: str):
         """The first pass of a resumed run: one step, then Force_restore_parameters."""
         assert self.lib.kref_resume(str(path).encode()) == 0
+
+    def output_avs(self, init: bool = False):
+        """Output_avs of the current state (needs cfg["avs"])."""
+        assert self.lib.kref_output_avs(1 if init else 0) == 0
 
     def ts(self) -> int:
         return int(self.lib.kref_ts())

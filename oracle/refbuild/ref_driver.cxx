@@ -198,6 +198,17 @@ int kref_resume(const char *path) {
   return 0;
 }
 
+/* Output_avs of the current state as the step loop calls it
+   (sp_3d_ns.cxx:553-566, BINARY); init writes the .fld header and .cod file
+   first (Init_avs).  Needs output.AVS = ON in the input. */
+int kref_output_avs(int init) {
+  if (!g_ready || !SW_AVS || SW_EQ != Navier_Stokes) return -1;
+  Set_avs_parameters(Avs_parameters);
+  if (init) Init_avs(Avs_parameters);
+  Output_avs(Avs_parameters, g_zeta, g_uk_dc, g_particles, g_jikan);
+  return 0;
+}
+
 /* Wall-clock seconds of n steps (excludes initialisation). */
 double kref_time_steps(int n) {
   struct timeval a, b;

@@ -110,7 +110,14 @@ def spm_udf_lines(cfg: dict) -> list[str]:
             put(f"{t}.q.{n}", float(val))
     put("output.GTS", int(cfg.get("gts", 1000)))
     put("output.Num_snap", int(cfg.get("num_snap", 1)))
-    put("output.AVS", "OFF")
+    avs = cfg.get("avs")  # {"dir": ..., "name": ...}: Output_avs files, BINARY
+    if avs:
+        put("output.AVS", "ON")
+        put("output.ON.Out_dir", avs["dir"])
+        put("output.ON.Out_name", avs["name"])
+        put("output.ON.FileType", "BINARY")
+    else:
+        put("output.AVS", "OFF")
     put("output.UDF", "OFF")
     return L
 
