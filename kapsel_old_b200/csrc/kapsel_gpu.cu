@@ -557,7 +557,7 @@ struct Box : BoxBase {
       if (!fuse_pos) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
       mark();
       if (nc) launch_nearcontact();  // timed with the position slot when profiling
-      launch_k(pdl, k_particles_hydro_velocity<R>, dim3(Np * PCL), dim3(256), 0, stream, pp, parts,
+      launch_k(pdl, k_particles_hydro_velocity<R>, dim3(Np * PCLH), dim3(HYD_THREADS), 0, stream, pp, parts,
                (const R *)ustar, (const int *)cells, noise, euler, status, partial_p, arrivals,
                nc ? nc_corr : (double *)nullptr);
       mark();
@@ -753,7 +753,7 @@ struct Box : BoxBase {
     launch_y<true>(g, 3, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, N, g.NZ, PPar{}, nullptr, 0, nullptr);
     if (Np > 0) {
-      k_particles_hydro_velocity<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, ustar, cells, nullptr, euler, status,
+      k_particles_hydro_velocity<R><<<Np * PCLH, HYD_THREADS, 0, stream>>>(pp, parts, ustar, cells, nullptr, euler, status,
                                                                   partial_p, arrivals);
       k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup);
       launch_force_to_zeta();
@@ -1785,10 +1785,10 @@ int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr) {
   p.thermostat = 0;  // no kick
   // u is never read with S == 0
   if (b->prm.precision == KAPSEL_FP64)
-    k_particles_hydro_velocity<double><<<b->Np * PCL, 256, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
+    k_particles_hydro_velocity<double><<<b->Np * PCLH, HYD_THREADS, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
                                                                            b->status, b->partial_p, b->arrivals);
   else
-    k_particles_hydro_velocity<float><<<b->Np * PCL, 256, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
+    k_particles_hydro_velocity<float><<<b->Np * PCLH, HYD_THREADS, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
                                                                           b->status, b->partial_p, b->arrivals);
   std::vector<DPart> h(b->Np);
   cudaMemcpyAsync(h.data(), scratch, sizeof(DPart) * b->Np, cudaMemcpyDeviceToHost, b->stream);

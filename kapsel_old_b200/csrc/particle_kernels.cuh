@@ -228,15 +228,18 @@ __device__ void block_reduce(KSum (&v)[NV], double *sh /* [2*NV][32] */) {
 // (particle_solver.cxx:106-147, 247-289, 11-34) and, when kBT > 0, the
 // thermostat kick of Add_random_force_thermostat (fluct.cxx:10-36) from a
 // precomputed table of its normals.
-// PCL blocks per particle: each block sums a quarter of the Sekibun points
-// and of the LJ partners and stores its partial sums; the block that
-// finishes last (a per-particle arrival counter) adds the PCL partials in a
-// fixed order -- the result does not depend on block scheduling -- and
-// updates the particle.
+// The scatters run PCL blocks per particle.  The gather runs PCLH blocks of
+// HYD_THREADS threads per particle (about 7.5 Sekibun points per thread at
+// a = 5, every block resident in one wave): each block sums its share of
+// the Sekibun points and of the LJ partners and stores its partial sums;
+// the block that finishes last (a per-particle arrival counter) adds the
+// PCLH partials in a fixed order -- the result does not depend on block
+// scheduling -- and updates the particle.
 constexpr int PCL = 4;
+constexpr int PCLH = 2, HYD_THREADS = 128;
 
 template <typename R>
-__global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPart *__restrict__ parts,
+__global__ void __launch_bounds__(HYD_THREADS, 8) k_particles_hydro_velocity(PPar p, DPart *__restrict__ parts,
                                                                   const R *__restrict__ u, const int *__restrict__ cells,
                                                                   const double *__restrict__ noise, int euler,
                                                                   int *__restrict__ status,
@@ -246,9 +249,9 @@ __global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPa
   __shared__ double sh[2 * 9 * 32];
   __shared__ int last;
   pdl_begin();
-  const int n = blockIdx.x / PCL;
-  const int rank = blockIdx.x % PCL;
-  const int stride = PCL * blockDim.x;
+  const int n = blockIdx.x / PCLH;
+  const int rank = blockIdx.x % PCLH;
+  const int stride = PCLH * blockDim.x;
   const int first = rank * blockDim.x + threadIdx.x;
   DPart &a = parts[n];
   const double xp[3] = {a.x[0], a.x[1], a.x[2]};
@@ -272,6 +275,7 @@ __global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPa
     const float resf[3] = {(float)b.res[0], (float)b.res[1], (float)b.res[2]};
     const float vpf[3] = {(float)vp[0], (float)vp[1], (float)vp[2]};
     const float wpf[3] = {(float)wp[0], (float)wp[1], (float)wp[2]};
+#pragma unroll 2
     for (int m = first; m < p.S; m += stride) {
       const int *cell = cells + 3 * m;
       int rm[3];
@@ -394,13 +398,13 @@ __global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPa
     block_reduce<9>(acc, sh);
   }
   if (threadIdx.x == 0) {
-    double *pp = partial + ((size_t)n * PCL + rank) * 18;
+    double *pp = partial + ((size_t)n * PCLH + rank) * 18;
     for (int i = 0; i < 9; ++i) {
       pp[2 * i] = acc[i].s;
       pp[2 * i + 1] = acc[i].c;
     }
     __threadfence();
-    last = (atomicAdd(arrivals + n, 1) == PCL - 1);
+    last = (atomicAdd(arrivals + n, 1) == PCLH - 1);
   }
   __syncthreads();
   if (!last || threadIdx.x != 0) return;
@@ -408,8 +412,8 @@ __global__ void __launch_bounds__(256, 4) k_particles_hydro_velocity(PPar p, DPa
   arrivals[n] = 0;
   KSum tot[9];
   for (int i = 0; i < 9; ++i) tot[i] = {0.0, 0.0};
-  for (int q = 0; q < PCL; ++q) {
-    const volatile double *pq = partial + ((size_t)n * PCL + q) * 18;
+  for (int q = 0; q < PCLH; ++q) {
+    const volatile double *pq = partial + ((size_t)n * PCLH + q) * 18;
     for (int i = 0; i < 9; ++i) {
       tot[i].add(pq[2 * i]);
       tot[i].c += pq[2 * i + 1];
