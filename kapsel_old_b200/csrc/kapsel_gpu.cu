@@ -406,12 +406,17 @@ struct Box : BoxBase {
     if (smem_xadv > mx || smem_xu > mx || smem_y > mx || smem_zp > mx) return KAPSEL_ERANGE;
     {
       int rc = 0;
+      // the warp-level z kernels give one row group to a warp: below about
+      // 16 groups per SM (64^3 and smaller) the block-level kernels, which
+      // spread a row group over a whole block, keep more of the GPU busy
+      const bool zw_ok = (size_t)g.NX * g.NY >= 16384;
       if (g.NX == 32) rc = x_setup<5>();
       else if (g.NX == 64) rc = x_setup<6>();
       else if (g.NX == 128) rc = x_setup<7>();
       else if (g.NX == 256) rc = x_setup<8>();
       if (rc) return rc;
-      if (g.NZ == 64) rc = zw_setup<5>();
+      if (!zw_ok) rc = 0;
+      else if (g.NZ == 64) rc = zw_setup<5>();
       else if (g.NZ == 128) rc = zw_setup<6>();
       else if (g.NZ == 256) rc = zw_setup<7>();
       if (rc) return rc;
@@ -557,7 +562,7 @@ struct Box : BoxBase {
       if (!fuse_pos) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
       mark();
       if (nc) launch_nearcontact();  // timed with the position slot when profiling
-      launch_k(pdl, k_particles_hydro_velocity<R>, dim3(Np * PCLH), dim3(HYD_THREADS), 0, stream, pp, parts,
+      launch_k(pdl, k_particles_hydro_velocity<R>, dim3(Np * pp.hyd_pcl), dim3(pp.hyd_threads), 0, stream, pp, parts,
                (const R *)ustar, (const int *)cells, noise, euler, status, partial_p, arrivals,
                nc ? nc_corr : (double *)nullptr);
       mark();
@@ -753,7 +758,7 @@ struct Box : BoxBase {
     launch_y<true>(g, 3, bufA, bufB);
     k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ustar, N, g.NZ, PPar{}, nullptr, 0, nullptr);
     if (Np > 0) {
-      k_particles_hydro_velocity<R><<<Np * PCLH, HYD_THREADS, 0, stream>>>(pp, parts, ustar, cells, nullptr, euler, status,
+      k_particles_hydro_velocity<R><<<Np * pp.hyd_pcl, pp.hyd_threads, 0, stream>>>(pp, parts, ustar, cells, nullptr, euler, status,
                                                                   partial_p, arrivals);
       k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup);
       launch_force_to_zeta();
@@ -1460,6 +1465,10 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   pp.noise_v = 1.439 * std::sqrt(zeta_drag * p->dt * p->kbt * p->alpha_v);
   pp.noise_o = 1.22 * std::sqrt(zeta_drag_rot * p->dt * p->kbt * p->alpha_o);
   pp.frozen = p->frozen ? 1 : 0;
+  // one gather block per particle: 512 threads when there are enough
+  // particles to fill the GPU, 1024 (two Sekibun points a thread) otherwise
+  pp.hyd_pcl = 1;
+  pp.hyd_threads = b->Np >= 128 ? 512 : 1024;
   if (pp.frozen) pp.thermostat = 0;
   b->mt.reset(new MT19937(p->mt_seed));
 
@@ -1480,7 +1489,7 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   cudaMemset(b->uk_dc, 0, sizeof(double) * 3);
   if (cudaMalloc(&b->status, sizeof(int)) != cudaSuccess) return KAPSEL_ENOMEM;
   cudaMemset(b->status, 0, sizeof(int));
-  if (cudaMalloc(&b->partial_p, sizeof(double) * 18 * PCL * np1) != cudaSuccess) return KAPSEL_ENOMEM;
+  if (cudaMalloc(&b->partial_p, sizeof(double) * 18 * HYD_PCL_MAX * np1) != cudaSuccess) return KAPSEL_ENOMEM;
   if (cudaMalloc(&b->arrivals, sizeof(int) * np1) != cudaSuccess) return KAPSEL_ENOMEM;
   cudaMemset(b->arrivals, 0, sizeof(int) * np1);
   for (int s = 0; s < 2; ++s) {
@@ -1785,10 +1794,10 @@ int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr) {
   p.thermostat = 0;  // no kick
   // u is never read with S == 0
   if (b->prm.precision == KAPSEL_FP64)
-    k_particles_hydro_velocity<double><<<b->Np * PCLH, HYD_THREADS, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
+    k_particles_hydro_velocity<double><<<b->Np * p.hyd_pcl, p.hyd_threads, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
                                                                            b->status, b->partial_p, b->arrivals);
   else
-    k_particles_hydro_velocity<float><<<b->Np * PCLH, HYD_THREADS, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
+    k_particles_hydro_velocity<float><<<b->Np * p.hyd_pcl, p.hyd_threads, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
                                                                           b->status, b->partial_p, b->arrivals);
   std::vector<DPart> h(b->Np);
   cudaMemcpyAsync(h.data(), scratch, sizeof(DPart) * b->Np, cudaMemcpyDeviceToHost, b->stream);

@@ -36,6 +36,8 @@ struct PPar {
   int thermostat;
   double noise_v, noise_o;  // fluct.cxx:13-19
   int frozen;               // positions and velocities held; forces still measured
+  int hyd_pcl;              // gather blocks per particle (at most HYD_PCL_MAX)
+  int hyd_threads;          // threads per gather block (at most 1024)
 };
 
 __device__ __forceinline__ double nint_d(double a) {
@@ -228,18 +230,17 @@ __device__ void block_reduce(KSum (&v)[NV], double *sh /* [2*NV][32] */) {
 // (particle_solver.cxx:106-147, 247-289, 11-34) and, when kBT > 0, the
 // thermostat kick of Add_random_force_thermostat (fluct.cxx:10-36) from a
 // precomputed table of its normals.
-// The scatters run PCL blocks per particle.  The gather runs PCLH blocks of
-// HYD_THREADS threads per particle (about 7.5 Sekibun points per thread at
-// a = 5, every block resident in one wave): each block sums its share of
-// the Sekibun points and of the LJ partners and stores its partial sums;
-// the block that finishes last (a per-particle arrival counter) adds the
-// PCLH partials in a fixed order -- the result does not depend on block
-// scheduling -- and updates the particle.
+// The scatters run PCL blocks per particle.  The gather runs p.hyd_pcl
+// blocks of p.hyd_threads threads per particle.  With one block per particle
+// the block's sums are the particle's and thread 0 updates it; with several,
+// each block stores its partial sums and the block that finishes last (a
+// per-particle arrival counter) adds the partials in a fixed order -- the
+// result does not depend on block scheduling -- and updates the particle.
 constexpr int PCL = 4;
-constexpr int PCLH = 2, HYD_THREADS = 128;
+constexpr int HYD_PCL_MAX = 8;
 
 template <typename R>
-__global__ void __launch_bounds__(HYD_THREADS, 8) k_particles_hydro_velocity(PPar p, DPart *__restrict__ parts,
+__global__ void __launch_bounds__(1024) k_particles_hydro_velocity(PPar p, DPart *__restrict__ parts,
                                                                   const R *__restrict__ u, const int *__restrict__ cells,
                                                                   const double *__restrict__ noise, int euler,
                                                                   int *__restrict__ status,
@@ -249,9 +250,9 @@ __global__ void __launch_bounds__(HYD_THREADS, 8) k_particles_hydro_velocity(PPa
   __shared__ double sh[2 * 9 * 32];
   __shared__ int last;
   pdl_begin();
-  const int n = blockIdx.x / PCLH;
-  const int rank = blockIdx.x % PCLH;
-  const int stride = PCLH * blockDim.x;
+  const int n = blockIdx.x / p.hyd_pcl;
+  const int rank = blockIdx.x % p.hyd_pcl;
+  const int stride = p.hyd_pcl * blockDim.x;
   const int first = rank * blockDim.x + threadIdx.x;
   DPart &a = parts[n];
   const double xp[3] = {a.x[0], a.x[1], a.x[2]};
@@ -397,26 +398,32 @@ __global__ void __launch_bounds__(HYD_THREADS, 8) k_particles_hydro_velocity(PPa
     for (int i = 0; i < 9; ++i) acc[i] = {a9[i], 0.0};
     block_reduce<9>(acc, sh);
   }
-  if (threadIdx.x == 0) {
-    double *pp = partial + ((size_t)n * PCLH + rank) * 18;
-    for (int i = 0; i < 9; ++i) {
-      pp[2 * i] = acc[i].s;
-      pp[2 * i + 1] = acc[i].c;
-    }
-    __threadfence();
-    last = (atomicAdd(arrivals + n, 1) == PCLH - 1);
-  }
-  __syncthreads();
-  if (!last || threadIdx.x != 0) return;
-  __threadfence();
-  arrivals[n] = 0;
   KSum tot[9];
-  for (int i = 0; i < 9; ++i) tot[i] = {0.0, 0.0};
-  for (int q = 0; q < PCLH; ++q) {
-    const volatile double *pq = partial + ((size_t)n * PCLH + q) * 18;
-    for (int i = 0; i < 9; ++i) {
-      tot[i].add(pq[2 * i]);
-      tot[i].c += pq[2 * i + 1];
+  if (p.hyd_pcl == 1) {
+    // one block per particle: its sums are the particle's
+    if (threadIdx.x != 0) return;
+    for (int i = 0; i < 9; ++i) tot[i] = acc[i];
+  } else {
+    if (threadIdx.x == 0) {
+      double *pp = partial + ((size_t)n * p.hyd_pcl + rank) * 18;
+      for (int i = 0; i < 9; ++i) {
+        pp[2 * i] = acc[i].s;
+        pp[2 * i + 1] = acc[i].c;
+      }
+      __threadfence();
+      last = (atomicAdd(arrivals + n, 1) == p.hyd_pcl - 1);
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    arrivals[n] = 0;
+    for (int i = 0; i < 9; ++i) tot[i] = {0.0, 0.0};
+    for (int q = 0; q < p.hyd_pcl; ++q) {
+      const volatile double *pq = partial + ((size_t)n * p.hyd_pcl + q) * 18;
+      for (int i = 0; i < 9; ++i) {
+        tot[i].add(pq[2 * i]);
+        tot[i].c += pq[2 * i + 1];
+      }
     }
   }
   double fh[3], th[3], fr[3];
