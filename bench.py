@@ -384,7 +384,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "algorithmic_bytes_per_launch": kb[top_name], "avg_launch_ms": round(float(acc[top]), 5),
-                     "traffic": None},
+                     "traffic": ncu_traffic(top_name)},
         "step_roofline": {"bytes_per_step_model": int(bstep), "field_passes": round(passes, 2),
                           "achieved_gbs": round(bstep / (ms_m / args.steps * 1e-3) / 1e9, 1),
                           "frac": round(bstep / (ms_m / args.steps * 1e-3) / 1e9 / hbm, 4)},
@@ -401,6 +401,21 @@ def run_ours(args, rank, world, local_rank):
 
 
 # ---------------------------------------------------------------------------
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/<kernel without the leading k_>_*.md, line `traffic_bytes_per_launch`), or None."""
+    import glob
+    import re
+
+    stem = kernel[2:] if kernel.startswith("k_") else kernel
+    here = os.path.dirname(os.path.abspath(__file__))
+    for f in sorted(glob.glob(os.path.join(here, "profiles", f"k_*{stem.replace('z_', 'z*_')}*.md"))):
+        m = re.search(r"\|\s*traffic_bytes_per_launch\s*\|\s*([0-9]+)\s*\|", open(f).read())
+        if m:
+            return int(m.group(1))
+    return None
+
+
 def cpu_baseline(cfg, warmup: int, steps: int, threads: int | None = None):
     """Reference CPU timing on the host cores (oracle/_ref; else the numpy port)."""
     from oracle import ref, udf

@@ -444,6 +444,44 @@ __global__ void __launch_bounds__(256) k_z_r2c_full(Geo g, Twiddles<R> tw, const
   }
 }
 
+// One retained mode of the nonlinear term and the fluid update
+// (operate_omega.cxx:60-97, Omega_k2zeta_k, NS_solver_slavedEuler
+// fluid_solver.cxx:328-354; EULER: Add_zeta_viscous_term + Field_solver_Euler,
+// fluid_solver.cxx:122-135): from the five forward-transformed product
+// spectra at wavevector (k1, k2, k3), update the reduced vorticity (z0, z1).
+template <typename R, int EULER>
+__device__ __forceinline__ void advect_mode_update(const Geo &g, int KXi, int KYi, R k1, R k2, R k3, Cx<R> a23,
+                                                   Cx<R> a31, Cx<R> a12, Cx<R> b2233, Cx<R> b3311, Cx<R> &z0,
+                                                   Cx<R> &z1) {
+  const Cx<R> b1122 = {-b3311.x - b2233.x, -b3311.y - b2233.y};
+  const R k1k2 = k1 * k2, k2k3 = k2 * k3, k3k1 = k3 * k1;
+  const R d32 = (k3 - k2) * (k3 + k2), d13 = (k1 - k3) * (k1 + k3), d21 = (k2 - k1) * (k2 + k1);
+  Cx<R> w[3];
+  w[0] = {-(k2k3 * b2233.x + d32 * a23.x + k3k1 * a12.x - k1k2 * a31.x),
+          -(k2k3 * b2233.y + d32 * a23.y + k3k1 * a12.y - k1k2 * a31.y)};
+  w[1] = {-(k3k1 * b3311.x + d13 * a31.x + k1k2 * a23.x - k2k3 * a12.x),
+          -(k3k1 * b3311.y + d13 * a31.y + k1k2 * a23.y - k2k3 * a12.y)};
+  w[2] = {-(k1k2 * b1122.x + d21 * a12.x + k2k3 * a31.x - k3k1 * a23.x),
+          -(k1k2 * b1122.y + d21 * a12.y + k2k3 * a31.y - k3k1 * a23.y)};
+  Cx<R> f0, f1;
+  select_zeta(KXi, KYi, w, f0, f1);
+  const R K2 = k1 * k1 + k2 * k2 + k3 * k3;
+  const R IK2 = K2 > R(0) ? R(1) / K2 : R(0);
+  if (EULER) {
+    const R nk2 = R(g.nu) * K2, dt = R(g.dt);
+    const Cx<R> r0 = {f0.x + -(nk2 * z0.x), f0.y + -(nk2 * z0.y)};
+    const Cx<R> r1 = {f1.x + -(nk2 * z1.x), f1.y + -(nk2 * z1.y)};
+    z0 = {z0.x + dt * r0.x, z0.y + dt * r0.y};
+    z1 = {z1.x + dt * r1.x, z1.y + dt * r1.y};
+  } else {
+    const double arg = -g.nu * g.dt * (double)K2;
+    const R dmy = R(g.fp64_exp ? exp(arg) - 1.0 : expm1(arg));
+    const R c1 = R(1.0 / g.nu) * IK2;
+    z0 = {z0.x + dmy * (z0.x - c1 * f0.x), z0.y + dmy * (z0.y - c1 * f0.y)};
+    z1 = {z1.x + dmy * (z1.x - c1 * f1.x), z1.y + dmy * (z1.y - c1 * f1.y)};
+  }
+}
+
 // ---------------------------------------------------------------------------
 // x pass, forward, of the five product spectra fused with the rest of
 // NS_solver_slavedEuler (fluid_solver.cxx:328-354) and the next inverse:
@@ -510,35 +548,8 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
     const int kz = kz0 + col;
     const R k1 = R(g.wave[0] * KXi), k2 = ky, k3 = R(g.wave[2] * kz);
     const Cx<R> *p = Pb + i * W5 + col;
-    const Cx<R> a23 = p[0], a31 = p[KC], a12 = p[2 * KC], b2233 = p[3 * KC], b3311 = p[4 * KC];
-    const Cx<R> b1122 = {-b3311.x - b2233.x, -b3311.y - b2233.y};
-    const R k1k2 = k1 * k2, k2k3 = k2 * k3, k3k1 = k3 * k1;
-    const R d32 = (k3 - k2) * (k3 + k2), d13 = (k1 - k3) * (k1 + k3), d21 = (k2 - k1) * (k2 + k1);
-    Cx<R> w[3];
-    w[0] = {-(k2k3 * b2233.x + d32 * a23.x + k3k1 * a12.x - k1k2 * a31.x),
-            -(k2k3 * b2233.y + d32 * a23.y + k3k1 * a12.y - k1k2 * a31.y)};
-    w[1] = {-(k3k1 * b3311.x + d13 * a31.x + k1k2 * a23.x - k2k3 * a12.x),
-            -(k3k1 * b3311.y + d13 * a31.y + k1k2 * a23.y - k2k3 * a12.y)};
-    w[2] = {-(k1k2 * b1122.x + d21 * a12.x + k2k3 * a31.x - k3k1 * a23.x),
-            -(k1k2 * b1122.y + d21 * a12.y + k2k3 * a31.y - k3k1 * a23.y)};
-    Cx<R> f0, f1;
-    select_zeta(KXi, KYi, w, f0, f1);
-    const R K2 = k1 * k1 + k2 * k2 + k3 * k3;
-    const R IK2 = K2 > R(0) ? R(1) / K2 : R(0);
     Cx<R> z0 = Zs[ix * KC + col], z1 = Zs[(g.KXc + ix) * KC + col];
-    if (EULER) {
-      const R nk2 = R(g.nu) * K2, dt = R(g.dt);
-      const Cx<R> r0 = {f0.x + -(nk2 * z0.x), f0.y + -(nk2 * z0.y)};
-      const Cx<R> r1 = {f1.x + -(nk2 * z1.x), f1.y + -(nk2 * z1.y)};
-      z0 = {z0.x + dt * r0.x, z0.y + dt * r0.y};
-      z1 = {z1.x + dt * r1.x, z1.y + dt * r1.y};
-    } else {
-      const double arg = -g.nu * g.dt * (double)K2;
-      const R dmy = R(g.fp64_exp ? exp(arg) - 1.0 : expm1(arg));
-      const R c1 = R(1.0 / g.nu) * IK2;
-      z0 = {z0.x + dmy * (z0.x - c1 * f0.x), z0.y + dmy * (z0.y - c1 * f0.y)};
-      z1 = {z1.x + dmy * (z1.x - c1 * f1.x), z1.y + dmy * (z1.y - c1 * f1.y)};
-    }
+    advect_mode_update<R, EULER>(g, KXi, KYi, k1, k2, k3, p[0], p[KC], p[2 * KC], p[3 * KC], p[4 * KC], z0, z1);
     const size_t o = ((size_t)ix * g.KYc + iy) * g.TS + kz;
     zeta[o] = z0;
     zeta[zplane + o] = z1;
