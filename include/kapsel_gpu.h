@@ -37,8 +37,9 @@ extern "C" {
 #define KAPSEL_FP64 0  /* all fields and FFTs in double precision */
 #define KAPSEL_MIXED 1 /* fields/FFTs/stencils in float, particles and reductions in double */
 
-#define KAPSEL_EQ_NAVIER_STOKES 0 /* EQ::Navier_Stokes (input.h:49) */
-#define KAPSEL_EQ_ELECTROLYTE 3   /* EQ::Electrolyte (input.h:52) */
+#define KAPSEL_EQ_NAVIER_STOKES 0 /* EQ::Navier_Stokes (input.h:46) */
+#define KAPSEL_EQ_SHEAR_LE 2      /* EQ::Shear_Navier_Stokes_Lees_Edwards (input.h:48) */
+#define KAPSEL_EQ_ELECTROLYTE 3   /* EQ::Electrolyte (input.h:49) */
 
 /* Per-particle record layout used by kapsel_gpu_get_particles (doubles). */
 #define KAPSEL_P_X 0         /* x[3]                      */
@@ -81,6 +82,10 @@ typedef struct kapsel_params {
      measurement, as used to generate near-contact training pairs; no
      counterpart in the reference).  0 for the reference dynamics. */
   int frozen;
+  /* Shear_Navier_Stokes_Lees_Edwards: Shear_rate of the DC external field
+     (constitutive_eq.Shear_Navier_Stokes_Lees_Edwards.External_field.DC,
+     input.cxx:634-645); ignored by the other branches. */
+  double shear_rate;
 } kapsel_params;
 
 typedef struct kapsel_ctx kapsel_ctx;
@@ -160,6 +165,14 @@ int kapsel_gpu_get_dims(kapsel_ctx *ctx, int *dims);
    only: the reference reads it from the UDF (input.cxx:743-790); switching it
    mid-run replaces a restart with a new Electric_field. */
 int kapsel_gpu_set_efield(kapsel_ctx *ctx, const double *e);
+
+/* Lees-Edwards branch: out[0] = degree_oblique (the strain of the oblique
+   grid, input.cxx:271), out[1] = Shear_rate_eff (Calc_shear_rate_eff,
+   sp_3d_ns.h:174-196), out[2] = Shear_strain_realized (sp_3d_ns.cxx:600). */
+int kapsel_gpu_get_oblique(kapsel_ctx *ctx, double *out);
+/* Sets degree_oblique and Shear_rate_eff, as a resumed run restores
+   degree_oblique (resume.cxx:333-360).  KAPSEL_EINVAL outside the branch. */
+int kapsel_gpu_set_oblique(kapsel_ctx *ctx, double degree_oblique, double shear_rate_eff);
 
 /* Ion concentrations conc_k[2] in the Ooura layout (2*NX*NY*NZ_ doubles;
    the Concentration array of solute_rhs.cxx:16), Electrolyte only. */

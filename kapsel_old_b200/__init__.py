@@ -23,7 +23,10 @@ LIB_PATH = os.path.join(_HERE, "libkapsel_gpu.so")
 FP64 = 0
 MIXED = 1
 EQ_NAVIER_STOKES = 0
+EQ_SHEAR_LE = 2
 EQ_ELECTROLYTE = 3
+_EQ = {"Navier_Stokes": EQ_NAVIER_STOKES, "Shear_Navier_Stokes_Lees_Edwards": EQ_SHEAR_LE,
+       "Electrolyte": EQ_ELECTROLYTE}
 P_STRIDE = 35
 
 
@@ -64,6 +67,7 @@ class _Params(ctypes.Structure):
         ("onsager_n", ctypes.c_double),
         ("e_ext", ctypes.c_double * 3),
         ("frozen", ctypes.c_int),
+        ("shear_rate", ctypes.c_double),
     ]
 
 
@@ -99,6 +103,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_get_time": (ctypes.c_int, [_VP, _IP, _DP]),
         "kapsel_gpu_get_dims": (ctypes.c_int, [_VP, _IP]),
         "kapsel_gpu_set_efield": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_get_oblique": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_set_oblique": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double]),
         "kapsel_gpu_get_concentration": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_A2a_k": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_A_k2a": (ctypes.c_int, [_VP, _DP]),
@@ -137,7 +143,11 @@ def params_from_config(cfg: dict, precision: int = FP64) -> _Params:
     L.kapsel_params_default(ctypes.byref(p))
     for d in range(3):
         p.np_xyz[d] = int(cfg["np_xyz"][d])
-    p.eq = EQ_ELECTROLYTE if cfg.get("eq", "Navier_Stokes") == "Electrolyte" else EQ_NAVIER_STOKES
+    eq = cfg.get("eq", "Navier_Stokes")
+    if eq not in _EQ:
+        raise KapselError(f"constitutive_eq {eq!r} is not supported")
+    p.eq = _EQ[eq]
+    p.shear_rate = float(cfg.get("shear_rate", 0.0))
     p.precision = precision
     p.n_particles = len(cfg.get("particles", []))
     p.dx = float(cfg.get("dx", 1.0))
@@ -292,6 +302,15 @@ class Simulation:
     def set_efield(self, e):
         a = np.ascontiguousarray(e, dtype=np.float64)
         self._check(self.L.kapsel_gpu_set_efield(self.h, _ptr(a)))
+
+    def oblique(self) -> dict:
+        """Lees-Edwards state: degree_oblique, Shear_rate_eff, Shear_strain_realized."""
+        a = np.zeros(3)
+        self._check(self.L.kapsel_gpu_get_oblique(self.h, _ptr(a)))
+        return {"degree_oblique": float(a[0]), "shear_rate_eff": float(a[1]), "strain": float(a[2])}
+
+    def set_oblique(self, degree_oblique: float, shear_rate_eff: float):
+        self._check(self.L.kapsel_gpu_set_oblique(self.h, float(degree_oblique), float(shear_rate_eff)))
 
     # ---- routine-level entry points (reference layouts, NX*NY*NZ_ doubles)
     def _padded(self, a):

@@ -35,6 +35,7 @@
 #include "../../include/kapsel_gpu.h"
 #include "electrolyte_kernels.cuh"
 #include "nearcontact_kernels.cuh"
+#include "obl_kernels.cuh"
 #include "particle_kernels.cuh"
 #include "spectral_kernels.cuh"
 #include "zwarp_kernels.cuh"
@@ -193,6 +194,9 @@ struct BoxBase {
   virtual float time_ypass(int small, int reps) = 0;
   virtual void set_ytile(int small) = 0;
   virtual int alloc_el() = 0;
+  virtual int alloc_obl() = 0;
+  virtual int oblique_state(double *out) = 0;
+  virtual int set_oblique_state(double deg, double srate) = 0;
   virtual int init_el() = 0;
   virtual int conc_to_host(double *c) = 0;
   virtual int conc_from_host(const double *c) = 0;
@@ -366,8 +370,10 @@ struct Box : BoxBase {
     const size_t nA = (size_t)g.NX * g.KYc * g.TS;
     const size_t nB = (size_t)g.NX * g.NY * g.TS;
     KCHECK(cudaMalloc(&zeta, sizeof(Cx<R>) * 2 * nz));
-    KCHECK(cudaMalloc(&bufA, sizeof(Cx<R>) * 5 * nA));
-    KCHECK(cudaMalloc(&bufB, sizeof(Cx<R>) * 5 * nB));
+    // the Lees-Edwards advection term carries u and the vorticity: 6 spectra
+    const int nbuf = prm.eq == KAPSEL_EQ_SHEAR_LE ? 6 : 5;
+    KCHECK(cudaMalloc(&bufA, sizeof(Cx<R>) * nbuf * nA));
+    KCHECK(cudaMalloc(&bufB, sizeof(Cx<R>) * nbuf * nB));
     KCHECK(cudaMalloc(&ustar, sizeof(R) * 3 * npts()));
     KCHECK(cudaMalloc(&phiup, sizeof(R) * 4 * npts()));
     KCHECK(cudaMemset(zeta, 0, sizeof(Cx<R>) * 2 * nz));
@@ -534,6 +540,10 @@ struct Box : BoxBase {
       launch_step_el(euler);
       return;
     }
+    if (prm.eq == KAPSEL_EQ_SHEAR_LE) {
+      launch_step_obl(noise, euler);
+      return;
+    }
     int e = 0;
     auto mark = [&]() {
       if (ev) cudaEventRecord(ev[e++], stream);
@@ -590,6 +600,97 @@ struct Box : BoxBase {
       launch_force_to_zeta();
     }
     cudaMemsetAsync(uk_dc, 0, sizeof(double) * 3, stream);
+  }
+
+  // ---- Lees-Edwards sheared branch on the oblique grid -----------------------
+  R *ob6 = nullptr;        // [6][N]: u and vorticity of the advection term, later the force f
+  R *obB = nullptr;        // [3][N]: contravariant u on the oblique grid
+  double *obst = nullptr;  // degree_oblique, Shear_rate_eff, ... (obl_kernels.cuh)
+  OblPar op{};
+  size_t sm_xo6 = 0, sm_xo3 = 0, sm_xof = 0;
+
+  int alloc_obl() override {
+    const size_t N = npts(), nst = OB_PART + 2 * (size_t)OB_RED_BLOCKS;
+    KCHECK(cudaMalloc(&ob6, sizeof(R) * 6 * N));
+    KCHECK(cudaMalloc(&obB, sizeof(R) * 3 * N));
+    KCHECK(cudaMalloc(&obst, sizeof(double) * nst));
+    KCHECK(cudaMemset(ob6, 0, sizeof(R) * 6 * N));
+    KCHECK(cudaMemset(obB, 0, sizeof(R) * 3 * N));
+    KCHECK(cudaMemset(obst, 0, sizeof(double) * nst));
+    const size_t C = sizeof(Cx<R>);
+    sm_xo6 = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)2 * g.NX * 6 * KCX);
+    sm_xo3 = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)2 * g.NX * 3 * KCX);
+    sm_xof = C * (g.NX + (size_t)2 * g.NX * 3 * KCX);
+    if (sm_xo6 > 227 * 1024 || smem_zc > 227 * 1024) return KAPSEL_ERANGE;
+    KCHECK(cudaFuncSetAttribute(k_x_obl_inv<R, KCX, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_xo6));
+    KCHECK(cudaFuncSetAttribute(k_x_obl_inv<R, KCX, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_xo3));
+    KCHECK(cudaFuncSetAttribute(k_x_obl_fwd<R, KCX, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_xof));
+    KCHECK(cudaFuncSetAttribute(k_x_obl_fwd<R, KCX, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_xof));
+    KCHECK(cudaFuncSetAttribute(k_z_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
+    op.shear_rate = prm.shear_rate;
+    op.dt = prm.dt;
+    // ivolume = Ivolume * POW3(DX); s_rate_eff *= ivolume*NY/(NY - 1) (sp_3d_ns.h:175,192)
+    const double LX = g.NX * prm.dx, LY = g.NY * prm.dx, LZ = g.NZ * prm.dx;
+    const double ivolume = (1. / (LX * LY * LZ)) * (prm.dx * prm.dx * prm.dx);
+    op.srate_scale = ivolume * g.NY / (g.NY - 1);
+    op.dx = prm.dx;
+    op.NX = g.NX;
+    op.NY = g.NY;
+    op.NZ = g.NZ;
+    return 0;
+  }
+
+  // Time_evolution_hydro_OBL (sp_3d_ns.cxx:214-390).
+  void launch_step_obl(const double *noise, int euler) {
+    const size_t N = npts();
+    const int pb = 592;
+    // NS_solver_slavedEuler_Shear_OBL: u and omega of the truncated zeta, u x omega,
+    // forward, shear correction, curl and the slaved-Euler step
+    k_x_obl_inv<R, KCX, 6><<<gx(), 256, sm_xo6, stream>>>(g, tw, zeta, uk_dc, obst, bufA);
+    launch_y<true>(g, 6, bufA, bufB);
+    k_z_c2r<R><<<dim3(gz(), 6), 256, smem_zc, stream>>>(g, tw, bufB, ob6, N, g.NZ, PPar{}, nullptr, 0, nullptr);
+    k_obl_cross<R><<<pb, 256, 0, stream>>>(N, ob6, obB);
+    k_z_r2c<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, obB, g.NZ, N, bufB, g.TZ, g.TS);
+    launch_y<false>(g, 3, bufB, bufA);
+    k_x_obl_fwd<R, KCX, 1><<<gx(), 256, sm_xof, stream>>>(g, tw, bufA, zeta, uk_dc, obst);
+    // FIX_CELL on uk_dc, u = Zeta_k2u_k_OBL(zeta, uk_dc), A_k2a
+    k_x_obl_inv<R, KCX, 3><<<gx(), 256, sm_xo3, stream>>>(g, tw, zeta, uk_dc, obst, bufA);
+    launch_y<true>(g, 3, bufA, bufB);
+    k_z_c2r<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, bufB, ob6, N, g.NZ, PPar{}, nullptr, 0, nullptr);
+    // deformation: degree_oblique, grid reset, Cartesian u (ustar), Shear_rate_eff
+    k_obl_degree<<<1, 32, 0, stream>>>(op, obst);
+    k_obl_remap<R><<<pb, 256, 0, stream>>>(op, (const double *)obst, (const R *)ob6, obB);
+    k_obl_to_cart<R><<<pb, 256, 0, stream>>>(op, (const double *)obst, (const R *)obB, ustar);
+    k_obl_srate_partial<R><<<OB_RED_BLOCKS, 256, 0, stream>>>(op, (const R *)ustar, obst);
+    k_obl_srate_final<<<1, 32, 0, stream>>>(op, obst, OB_RED_BLOCKS);
+    if (Np > 0) {
+      k_obl_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, (const double *)obst, status);
+      k_obl_hydro_velocity<R><<<Np, 256, 0, stream>>>(pp, parts, (const R *)ustar, (const int *)cells, noise, euler,
+                                                       (const double *)obst, status);
+      k_obl_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, (const DPart *)parts, (const int *)cells,
+                                                      (const double *)obst, phiup);
+    }
+    // f = up - phi u (Cartesian), u += U2u_oblique(f), forward, Solenoidal_uk_OBL,
+    // contra2co, U_k2zeta_k_OBL
+    k_obl_force<R><<<pb, 256, 0, stream>>>(N, phiup, (const R *)ustar, ob6);
+    k_obl_add_force<R><<<pb, 256, 0, stream>>>(op, (const double *)obst, (const R *)ob6, obB);
+    k_z_r2c<R><<<dim3(gz(), 3), 256, smem_zc, stream>>>(g, tw, obB, g.NZ, N, bufB, g.TZ, g.TS);
+    launch_y<false>(g, 3, bufB, bufA);
+    k_x_obl_fwd<R, KCX, 0><<<gx(), 256, sm_xof, stream>>>(g, tw, bufA, zeta, uk_dc, obst);
+  }
+
+  int oblique_state(double *out) override {
+    if (!obst) return KAPSEL_EINVAL;
+    KCHECK(cudaMemcpyAsync(out, obst, sizeof(double) * 4, cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    return 0;
+  }
+  int set_oblique_state(double deg, double srate) override {
+    if (!obst) return KAPSEL_EINVAL;
+    const double h[2] = {deg, srate};
+    KCHECK(cudaMemcpyAsync(obst + OB_DEG, h, sizeof(h), cudaMemcpyHostToDevice, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    return 0;
   }
 
   // ---- Electrolyte branch (two ion species) --------------------------------
@@ -846,7 +947,10 @@ struct Box : BoxBase {
   int velocity_to_host(double *u) override {
     R *tmp = nullptr;
     KCHECK(cudaMallocAsync(&tmp, sizeof(R) * 3 * npts(), stream));
-    launch_zeta_to_real(tmp, npts(), g.NZ);
+    if (prm.eq == KAPSEL_EQ_SHEAR_LE)
+      KCHECK(cudaMemcpyAsync(tmp, ustar, sizeof(R) * 3 * npts(), cudaMemcpyDeviceToDevice, stream));
+    else
+      launch_zeta_to_real(tmp, npts(), g.NZ);
     std::vector<R> h(3 * npts());
     KCHECK(cudaMemcpyAsync(h.data(), tmp, sizeof(R) * h.size(), cudaMemcpyDeviceToHost, stream));
     KCHECK(cudaFreeAsync(tmp, stream));
@@ -912,6 +1016,9 @@ struct Box : BoxBase {
   int fhydro_host(const double *u0, const double *u1, const double *u2, double *f, double *t) override;
 
   void free_all() override {
+    cudaFree(ob6);
+    cudaFree(obB);
+    cudaFree(obst);
     cudaFree(conc_k);
     cudaFree(rho_k);
     cudaFree(phiq);
@@ -1373,7 +1480,9 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   *out = nullptr;
   for (int d = 0; d < 3; ++d)
     if (p->np_xyz[d] < 4 || p->np_xyz[d] > 9) return KAPSEL_EINVAL;  // 16..512 per axis
-  if (p->eq != KAPSEL_EQ_NAVIER_STOKES && p->eq != KAPSEL_EQ_ELECTROLYTE) return KAPSEL_EINVAL;
+  if (p->eq != KAPSEL_EQ_NAVIER_STOKES && p->eq != KAPSEL_EQ_ELECTROLYTE && p->eq != KAPSEL_EQ_SHEAR_LE)
+    return KAPSEL_EINVAL;
+  if (p->eq == KAPSEL_EQ_SHEAR_LE && !std::isfinite(p->shear_rate)) return KAPSEL_EINVAL;
   if (p->eq == KAPSEL_EQ_ELECTROLYTE && (!(p->dielectric > 0.0) || p->surface_charge == 0.0 || !(p->debye_length > 0.0) ||
                                          !(p->valency_p > 0.0) || !(p->valency_n < 0.0)))
     return KAPSEL_EINVAL;
@@ -1407,6 +1516,8 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   g.nu = p->eta / p->rho;
   g.dt = p->dt;
   for (int d = 0; d < 3; ++d) g.fix_cell[d] = p->fix_cell[d] ? 1 : 0;
+  // the sheared branches always fix the mean y velocity (input.cxx:1555-1557)
+  if (p->eq == KAPSEL_EQ_SHEAR_LE) g.fix_cell[1] = 1;
   g.fp64_exp = p->precision == KAPSEL_FP64 ? 1 : 0;
   g.inv_n = 1.0 / ((double)g.NX * g.NY * g.NZ);
 
@@ -1448,8 +1559,15 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
     const int nmin = std::min(g.NX, std::min(g.NY, g.NZ));
     a_r_cutoff = std::min(nmin * p->dx * .5 / sigma, 2.5);
   }
-  pp.lj_dia = sigma;
-  pp.lj_cut = a_r_cutoff * sigma;
+  // LJ_dia (input.cxx:388-405): SIGMA, or in the sheared branches
+  // MIN((SIGMA + XI)/2^(1/(6(p+1))), SIGMA)
+  double lj_dia = sigma;
+  if (p->eq == KAPSEL_EQ_SHEAR_LE) {
+    const double pw[3] = {1. / 6., 1. / 12., 1. / 18.};
+    lj_dia = std::min((sigma + XI) / std::pow(2., pw[p->lj_powers]), sigma);
+  }
+  pp.lj_dia = lj_dia;
+  pp.lj_cut = a_r_cutoff * lj_dia;
   pp.lj_coeff = 24. * (p->lj_powers + 1) * p->epsilon;
   pp.lc[0] = g.NX / 16;
   pp.lc[1] = g.NY / 16;
@@ -1477,6 +1595,10 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   if (rc) return rc;
   if (p->eq == KAPSEL_EQ_ELECTROLYTE) {
     rc = b->alloc_el();
+    if (rc) return rc;
+  }
+  if (p->eq == KAPSEL_EQ_SHEAR_LE) {
+    rc = b->alloc_obl();
     if (rc) return rc;
   }
   const int np1 = b->Np > 0 ? b->Np : 1;
@@ -1577,6 +1699,19 @@ int kapsel_gpu_init_state(kapsel_ctx *ctx) {
   if (b->prm.eq == KAPSEL_EQ_ELECTROLYTE) {
     int rc = b->init_el();
     if (rc) return rc;
+  }
+  if (b->prm.eq == KAPSEL_EQ_SHEAR_LE && b->Np > 0 && !b->prm.frozen) {
+    // the sheared branches start every particle with v_x = omega_z = 0 after
+    // the initial projection (init_particle.cxx:666-677)
+    std::vector<DPart> h(b->Np);
+    if (cudaMemcpy(h.data(), b->parts, sizeof(DPart) * b->Np, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return KAPSEL_ECUDA;
+    for (DPart &a : h) {
+      a.v[0] = a.v_old[0] = 0.0;
+      a.omega[2] = a.omega_old[2] = 0.0;
+    }
+    if (cudaMemcpy(b->parts, h.data(), sizeof(DPart) * b->Np, cudaMemcpyHostToDevice) != cudaSuccess)
+      return KAPSEL_ECUDA;
   }
   b->ts = 0;
   b->time = 0.0;
@@ -1840,6 +1975,24 @@ int kapsel_gpu_get_stream(kapsel_ctx *ctx, void **stream) {
   if (!ctx || !stream) return KAPSEL_EINVAL;
   *stream = (void *)ctx->box->stream;
   return 0;
+}
+
+int kapsel_gpu_get_oblique(kapsel_ctx *ctx, double *out) {
+  if (!ctx || !out || ctx->box->prm.eq != KAPSEL_EQ_SHEAR_LE) return KAPSEL_EINVAL;
+  double h[4];
+  const int rc = ctx->box->oblique_state(h);
+  if (rc) return rc;
+  out[0] = h[OB_DEG];
+  out[1] = h[OB_SRATE];
+  out[2] = h[OB_STRAIN];
+  return 0;
+}
+
+int kapsel_gpu_set_oblique(kapsel_ctx *ctx, double degree_oblique, double shear_rate_eff) {
+  if (!ctx || ctx->box->prm.eq != KAPSEL_EQ_SHEAR_LE || !std::isfinite(degree_oblique) ||
+      !std::isfinite(shear_rate_eff))
+    return KAPSEL_EINVAL;
+  return ctx->box->set_oblique_state(degree_oblique, shear_rate_eff);
 }
 
 int kapsel_gpu_launches_per_step(kapsel_ctx *ctx) {

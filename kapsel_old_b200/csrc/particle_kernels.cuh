@@ -139,6 +139,28 @@ __device__ __forceinline__ void qnormalize(double *q) {
   for (int i = 0; i < 4; ++i) q[i] *= n;
 }
 
+// MD_solver_orientation_Euler / _AB2 (particle_rotation_solver.h:15-39).
+__device__ __forceinline__ void orientation_update(const PPar &p, DPart &a, int euler) {
+  const double hdt = 0.5 * p.dt;
+  double dq[4];
+  if (euler) {
+    for (int i = 0; i < 4; ++i) a.q_old[i] = a.q[i];
+    const double qw[4] = {0.0, a.omega[0], a.omega[1], a.omega[2]};
+    qprod(qw, a.q, 0.5, dq);
+    for (int i = 0; i < 4; ++i) a.q[i] += dq[i] * p.dt;
+  } else {
+    double wb[3], wbo[3];
+    space2body(a.omega, a.q, wb);
+    space2body(a.omega_old, a.q_old, wbo);
+    for (int d = 0; d < 3; ++d) wb[d] = 3.0 * wb[d] - wbo[d];
+    for (int i = 0; i < 4; ++i) a.q_old[i] = a.q[i];
+    const double qw[4] = {0.0, wb[0], wb[1], wb[2]};
+    qprod(a.q, qw, 0.5, dq);
+    for (int i = 0; i < 4; ++i) a.q[i] += dq[i] * hdt;
+  }
+  qnormalize(a.q);
+}
+
 // MD_solver_position_Euler / _AB2 (particle_solver.cxx:36-88), PBC
 // (periodic_boundary.h:9-15), MD_solver_orientation_Euler / _AB2
 // (particle_rotation_solver.h:15-39).  One thread per particle.
@@ -154,25 +176,7 @@ __device__ __forceinline__ void position_update_one(const PPar &p, DPart *__rest
     a.x[d] = fmod(a.x[d] + p.L[d], p.L[d]);
     if (!(a.x[d] >= 0.0 && a.x[d] < p.L[d])) atomicExch(status, -6);
   }
-  if (p.rotation) {
-    double dq[4];
-    if (euler) {
-      for (int i = 0; i < 4; ++i) a.q_old[i] = a.q[i];
-      const double qw[4] = {0.0, a.omega[0], a.omega[1], a.omega[2]};
-      qprod(qw, a.q, 0.5, dq);
-      for (int i = 0; i < 4; ++i) a.q[i] += dq[i] * p.dt;
-    } else {
-      double wb[3], wbo[3];
-      space2body(a.omega, a.q, wb);
-      space2body(a.omega_old, a.q_old, wbo);
-      for (int d = 0; d < 3; ++d) wb[d] = 3.0 * wb[d] - wbo[d];
-      for (int i = 0; i < 4; ++i) a.q_old[i] = a.q[i];
-      const double qw[4] = {0.0, wb[0], wb[1], wb[2]};
-      qprod(a.q, qw, 0.5, dq);
-      for (int i = 0; i < 4; ++i) a.q[i] += dq[i] * hdt;
-    }
-    qnormalize(a.q);
-  }
+  if (p.rotation) orientation_update(p, a, euler);
 }
 
 

@@ -59,6 +59,9 @@ class RefSim:
         L.kref_resume.argtypes = [ctypes.c_char_p]
         L.kref_time_steps.argtypes = [ctypes.c_int]
         L.kref_time_steps.restype = ctypes.c_double
+        L.kref_oblique.argtypes = [dp]
+        L.kref_set_particle_velocity.argtypes = [ctypes.c_int, dp, dp]
+        L.kref_set_oblique.argtypes = [ctypes.c_double, ctypes.c_double]
         self.cfg = cfg
         self.kv = kv_path or udf.write_udf(os.path.join(self._tmp, "input.kv"), cfg)
         rc = L.kref_init(self.kv.encode())
@@ -117,6 +120,23 @@ class RefSim:
 
     def phi(self):
         return self.field(3)[:, :, : self.NZ]
+
+    def ucp(self):
+        """Lees-Edwards: the Cartesian velocity of the last step (ucp)."""
+        return np.stack([self.field(12 + i)[:, :, : self.NZ] for i in range(3)])
+
+    def oblique(self) -> dict:
+        a = np.zeros(3)
+        self.lib.kref_oblique(self._p(a))
+        return {"degree_oblique": float(a[0]), "shear_rate_eff": float(a[1]), "strain": float(a[2])}
+
+    def set_particle_velocity(self, n: int, v, omega):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        w = np.ascontiguousarray(omega, dtype=np.float64)
+        assert self.lib.kref_set_particle_velocity(int(n), self._p(v), self._p(w)) == 0
+
+    def set_oblique(self, deg: float, srate: float):
+        assert self.lib.kref_set_oblique(float(deg), float(srate)) == 0
 
     def up(self):
         return np.stack([self.field(4 + i)[:, :, : self.NZ] for i in range(3)])

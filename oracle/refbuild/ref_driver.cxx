@@ -20,6 +20,8 @@
 
 extern void (*Time_evolution)(double **zeta, double uk_dc[DIM], double **f, Particle *p, CTime &jikan);
 void Time_evolution_hydro(double **zeta, double uk_dc[DIM], double **f, Particle *p, CTime &jikan);
+void Time_evolution_hydro_OBL(double **zeta, double uk_dc[DIM], double **f, Particle *p, CTime &jikan);
+extern double **ucp;
 /* emitted from sp_3d_ns.cxx by -fkeep-inline-functions */
 void Mem_alloc_var(double **zeta);
 
@@ -44,8 +46,8 @@ int kref_init(const char *kv_path) {
   char *argv[5] = {&a0[0], &aI[0], &aO[0], &aD[0], &aR[0]};
   file_get(5, argv);
   Gourmet_file_io(In_udf, Out_udf, Sum_udf, Def_udf, Ctrl_udf, Res_udf);
-  if (SW_EQ == Shear_Navier_Stokes_Lees_Edwards) return -2; /* not driven here */
-  Time_evolution = Time_evolution_hydro;
+  if (SW_EQ == Shear_Navier_Stokes) return -2; /* not driven here */
+  Time_evolution = SW_EQ == Shear_Navier_Stokes_Lees_Edwards ? Time_evolution_hydro_OBL : Time_evolution_hydro;
 
   MT_seed(GIVEN_SEED, 0);
   Init_fft();
@@ -67,6 +69,16 @@ int kref_init(const char *kv_path) {
     for (int d = 0; d < DIM; d++) g_uk_dc[d] = 0.0;
   }
   if (SW_EQ == Electrolyte) Init_rho_ion(Concentration, g_particles, g_jikan);
+  if (SW_EQ == Shear_Navier_Stokes_Lees_Edwards && !Fixed_particle) {
+    /* the v_x / omega_z reset that Show_parameter applies in the sheared
+       branches (init_particle.cxx:666-677), without its report */
+    for (int n = 0; n < Particle_Number; n++) {
+      g_particles[n].v[0] = 0.0;
+      g_particles[n].v_old[0] = 0.0;
+      g_particles[n].omega[2] = 0.0;
+      g_particles[n].omega_old[2] = 0.0;
+    }
+  }
   g_ready = 1;
   return 0;
 }
@@ -76,8 +88,46 @@ int kref_step(int n) {
   for (int s = 0; s < n; s++) {
     Time_evolution(g_zeta, g_uk_dc, f_particle, g_particles, g_jikan);
     g_jikan.time += g_jikan.dt_fluid;
+    /* main loop bookkeeping of the Lees-Edwards branch (sp_3d_ns.cxx:599-601;
+       Mean_shear_stress only reports) */
+    if (SW_EQ == Shear_Navier_Stokes_Lees_Edwards) Shear_strain_realized += Shear_rate_eff * g_jikan.dt_fluid;
     g_jikan.ts++;
   }
+  return 0;
+}
+
+/* Set the velocity and angular velocity of particle n (and their previous
+   values, as a fresh start has them equal). */
+int kref_set_particle_velocity(int n, const double *v, const double *w) {
+  if (!g_ready || n < 0 || n >= Particle_Number) return -1;
+  for (int d = 0; d < DIM; d++) {
+    g_particles[n].v[d] = g_particles[n].v_old[d] = v[d];
+    g_particles[n].omega[d] = g_particles[n].omega_old[d] = w[d];
+  }
+  return 0;
+}
+
+/* Lees-Edwards state: out = degree_oblique, Shear_rate_eff, Shear_strain_realized. */
+void kref_oblique(double *out) {
+  out[0] = degree_oblique;
+  out[1] = Shear_rate_eff;
+  out[2] = Shear_strain_realized;
+}
+
+/* Set degree_oblique and Shear_rate_eff and rebuild K2/IK2 for the new
+   degree_oblique, as the resume path does (resume.cxx:333-360). */
+int kref_set_oblique(double deg, double srate) {
+  if (!g_ready || SW_EQ != Shear_Navier_Stokes_Lees_Edwards) return -1;
+  degree_oblique = deg;
+  Shear_rate_eff = srate;
+  for (int i = 0; i < NX; i++)
+    for (int j = 0; j < NY; j++)
+      for (int k = 0; k < NZ_; k++) {
+        const int im = (i * NY * NZ_) + (j * NZ_) + k;
+        K2[im] = SQ(WAVE_X * KX_int[im]) + SQ(WAVE_Y * KY_int[im] - WAVE_X * degree_oblique * KX_int[im]) +
+                 SQ(WAVE_Z * KZ_int[im]);
+        IK2[im] = K2[im] > 0.0 ? 1.0 / K2[im] : 0.0;
+      }
   return 0;
 }
 
@@ -98,7 +148,8 @@ void kref_scalars(double *s) {
 int kref_ts(void) { return g_jikan.ts; }
 
 /* Copy a NX*NY*NZ_ field.  which: 0-2 u, 3 phi, 4-6 up, 7-8 zeta, 9-11 f_particle,
-   20+n Concentration[n] (k-space), 30-32 work_v3 */
+   12-14 ucp (Lees-Edwards: the Cartesian velocity of the step), 20+n
+   Concentration[n] (k-space), 30-32 work_v3 */
 int kref_get_field(int which, double *out) {
   double *src = NULL;
   if (which >= 0 && which < 3) src = u[which];
@@ -106,6 +157,7 @@ int kref_get_field(int which, double *out) {
   else if (which >= 4 && which < 7) src = up[which - 4];
   else if (which >= 7 && which < 9) src = g_zeta[which - 7];
   else if (which >= 9 && which < 12) src = f_particle[which - 9];
+  else if (which >= 12 && which < 15 && ucp) src = ucp[which - 12];
   else if (which >= 20 && which < 20 + N_spec && SW_EQ == Electrolyte) src = Concentration[which - 20];
   else if (which >= 30 && which < 33) src = work_v3[which - 30];
   if (!src) return -1;

@@ -4,8 +4,9 @@ TEST INFRASTRUCTURE ONLY (used by tests/golden/make_golden.py, tests and the
 bench's CPU reference arm).  The keys are the dotted UDF paths that
 Gourmet_file_io (input.cxx:438-1818) and the user_specify particle reader
 (init_particle.cxx:226-288) ask for; values mirror the schema in
-Udf/define.udf.  Only the spherical-particle Navier_Stokes and Electrolyte
-branches are produced.
+Udf/define.udf.  Only the spherical-particle Navier_Stokes,
+Shear_Navier_Stokes_Lees_Edwards (DC shear) and Electrolyte branches are
+produced.
 """
 from __future__ import annotations
 
@@ -20,7 +21,8 @@ def spm_udf_lines(cfg: dict) -> list[str]:
     """Return the stand-in UDF lines for one SPM configuration.
 
     cfg keys (all optional except np_xyz and particles):
-      eq: "Navier_Stokes" | "Electrolyte"
+      eq: "Navier_Stokes" | "Shear_Navier_Stokes_Lees_Edwards" | "Electrolyte"
+      shear_rate: Shear_rate of the DC external field (Lees-Edwards)
       np_xyz: (NPX, NPY, NPZ)  -> N = 1<<NP per axis (input.cxx:1392-1397)
       dx, rho, eta, kbt, alpha_v, alpha_o, dt, a, a_xi, mass_ratio,
       gravity_g, gravity_dir ("-X"/"-Y"/"-Z"), epsilon, lj_powers ("12:6"),
@@ -41,9 +43,13 @@ def spm_udf_lines(cfg: dict) -> list[str]:
     put(f"{base}.RHO", float(cfg.get("rho", 1.0)))
     put(f"{base}.ETA", float(cfg.get("eta", 1.0)))
     put(f"{base}.kBT", float(cfg.get("kbt", 0.0)))
-    if eq == "Navier_Stokes":
+    if eq in ("Navier_Stokes", "Shear_Navier_Stokes_Lees_Edwards"):
         put(f"{base}.alpha_v", float(cfg.get("alpha_v", 1.0)))
         put(f"{base}.alpha_o", float(cfg.get("alpha_o", 1.0)))
+        if eq != "Navier_Stokes":
+            # input.cxx:634-645
+            put(f"{base}.External_field.type", "DC")
+            put(f"{base}.External_field.DC.Shear_rate", float(cfg.get("shear_rate", 0.0)))
     else:
         el = cfg["electrolyte"]
         put(f"{base}.Dielectric_cst", float(el["dielectric"]))
@@ -168,6 +174,17 @@ def ns_config(np_xyz, n_particles, seed, a=5.0, a_xi=2.0, kbt=0.0, dt=0.01, min_
         parts.append(p)
     return {"eq": "Navier_Stokes", "np_xyz": tuple(np_xyz), "particles": parts, "a": a, "a_xi": a_xi,
             "kbt": kbt, "dt": dt, "gravity_g": gravity_g, "mass_ratio": mass_ratio, "rotation": rotation}
+
+
+def shear_le_config(np_xyz, n_particles, seed, shear_rate, a=5.0, a_xi=2.0, kbt=0.0, dt=0.01, min_gap=1.0,
+                    rotation="ON"):
+    """A Shear_Navier_Stokes_Lees_Edwards configuration (DC shear) with seeded
+    sphere positions."""
+    cfg = ns_config(np_xyz, n_particles, seed=seed, a=a, a_xi=a_xi, kbt=kbt, dt=dt, min_gap=min_gap,
+                    rotation=rotation)
+    cfg["eq"] = "Shear_Navier_Stokes_Lees_Edwards"
+    cfg["shear_rate"] = float(shear_rate)
+    return cfg
 
 
 def electrolyte_config(np_xyz, n_particles, seed, surface_charge=-100.0, debye=4.0, bjerrum=0.7, kbt=1.0,

@@ -1,0 +1,152 @@
+"""Lees-Edwards sheared step (Time_evolution_hydro_OBL, sp_3d_ns.cxx:214-390)
+on the GPU against the compiled reference (oracle/_ref).
+
+Both sides start from the reference's initial state (zeta, uk_dc and the
+particles are copied to the GPU; the particle velocities are then set on
+both, as the user_specify reader starts them at rest), then step together.
+The cases cover a particle crossing the y boundary (PBC_OBL velocity jump),
+Sekibun stencils
+and an LJ pair across it (stepover / Distance0_OBL), the oblique-grid reset
+when degree_oblique passes 1, and graph replay.
+Tolerances: FP64 <= 1e-10 relative per quantity; degree_oblique exact;
+mixed precision (FP32 fields) velocity <= 1e-5 and particle velocity
+<= 1e-4 relative."""
+import numpy as np
+import pytest
+
+from oracle import ref, spm, udf
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+
+
+def rel(a, b):
+    n = np.linalg.norm(b)
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / (n if n > 0 else 1.0)
+
+
+def _need_ref():
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+
+
+def _cfg(np_xyz=(5, 5, 5), shear_rate=0.05, kbt=0.0):
+    cfg = udf.shear_le_config(np_xyz, 0, seed=0, shear_rate=shear_rate, kbt=kbt)
+    L = [1 << p for p in np_xyz]
+    cfg["particles"] = [
+        # crosses y = 0 in the first step; its stencil straddles the boundary
+        {"x": (8.0, 0.05, 8.0), "v": (0.0, -10.0, 0.0), "omega": (0.0, 0.0, 0.3)},
+        {"x": (L[0] * 0.6, L[1] * 0.5, L[2] * 0.6), "v": (0.0, 0.0, 0.0), "omega": (0.1, 0.0, 0.0)},
+        # LJ partner of the first across y = L (centre distance 10.75 < 2^(1/6) sigma)
+        {"x": (18.7, L[1] - 0.95, 8.0), "v": (0.0, 0.5, 0.0)},
+    ]
+    return cfg
+
+
+def _trunc(zeta_ooura, cfg):
+    base = dict(cfg, eq="Navier_Stokes")
+    S = spm.Spectral(spm.Params(base))
+    z = spm.SpmOracle.from_ooura(zeta_ooura)
+    return spm.SpmOracle.to_ooura(np.stack([S.truncate(z[d]) for d in range(2)]))
+
+
+def _start(cfg, precision=0, oblique=None):
+    import kapsel_old_b200 as kg
+
+    R = ref.RefSim(cfg)
+    for n, p in enumerate(cfg["particles"]):
+        R.set_particle_velocity(n, p.get("v", (0.0, 0.0, 0.0)), p.get("omega", (0.0, 0.0, 0.0)))
+    g = kg.Simulation(cfg, precision=precision)
+    g.set_zeta(R.zeta(), R.uk_dc())
+    st = R.particles()
+    g.set_particle_state(st)
+    if oblique is not None:
+        R.set_oblique(*oblique)
+        g.set_oblique(*oblique)
+    return R, g
+
+
+def _errors(R, g, cfg):
+    o_r, o_g = R.oblique(), g.oblique()
+    pr, pg = R.particles(), g.particles()
+    uo = R.ucp()
+    N = uo[0].size
+    return {
+        "u": rel(g.velocity(), uo),
+        "zeta": rel(g.zeta(), _trunc(R.zeta(), cfg)),
+        "uk_dc": np.abs(g.uk_dc() - R.uk_dc()).max() / (N * max(np.abs(uo).max(), 1e-300)),
+        "x": np.abs(pg["x"] - pr["x"]).max(),
+        "v": rel(pg["v"], pr["v"]),
+        "omega": rel(pg["omega"], pr["omega"]),
+        "f_hydro": rel(pg["f_hydro"], pr["f_hydro"]),
+        "deg": abs(o_g["degree_oblique"] - o_r["degree_oblique"]),
+        "srate": abs(o_g["shear_rate_eff"] - o_r["shear_rate_eff"]) / abs(o_r["shear_rate_eff"]),
+    }
+
+
+@pytest.mark.parametrize("np_xyz", [(5, 5, 5), (6, 5, 5)])
+def test_obl_fp64_matches_reference(np_xyz):
+    _need_ref()
+    cfg = _cfg(np_xyz)
+    R, g = _start(cfg)
+    worst = {}
+    ys = [R.particles()["x"][0, 1]]
+    for s in range(6):
+        R.step(1)
+        g.step(1)
+        ys.append(R.particles()["x"][0, 1])
+        for k, v in _errors(R, g, cfg).items():
+            worst[k] = max(worst.get(k, 0.0), v)
+    # the first particle wrapped through the y boundary (with the shear jump)
+    assert np.abs(np.diff(ys)).max() > (1 << np_xyz[1]) / 2, ys
+    assert worst["deg"] == 0.0, worst
+    for k, v in worst.items():
+        assert v < FP64_TOL, (k, worst)
+
+
+def test_obl_grid_reset_fp64():
+    """degree_oblique passes 1 in the third step: the grid reset (u0 += u1,
+    rows shifted by j - NY/2) and degree_oblique -= 1."""
+    _need_ref()
+    cfg = _cfg()
+    R, g = _start(cfg, oblique=(0.9987, 0.0))
+    worst = {}
+    degs = []
+    for s in range(5):
+        R.step(1)
+        g.step(1)
+        degs.append(g.oblique()["degree_oblique"])
+        for k, v in _errors(R, g, cfg).items():
+            worst[k] = max(worst.get(k, 0.0), v)
+    assert degs[2] < 0.01 < degs[1], degs
+    assert worst["deg"] == 0.0, worst
+    for k, v in worst.items():
+        assert v < FP64_TOL, (k, worst)
+
+
+def test_obl_graph_equals_eager():
+    import kapsel_old_b200 as kg
+
+    cfg = _cfg(kbt=1e-3)
+    a = kg.Simulation(cfg)
+    b = kg.Simulation(cfg)
+    a.step(6)
+    b.step(1)
+    b.step(5, graph=True)
+    assert rel(b.zeta(), a.zeta()) < 1e-13
+    assert rel(b.particles()["v"], a.particles()["v"]) < 1e-13
+    assert b.oblique()["degree_oblique"] == a.oblique()["degree_oblique"]
+
+
+def test_obl_mixed_precision_bound():
+    _need_ref()
+    cfg = _cfg()
+    R, g = _start(cfg, precision=1)
+    for s in range(6):
+        R.step(1)
+        g.step(1)
+    e = _errors(R, g, cfg)
+    assert e["u"] < 1e-5, e
+    assert e["v"] < 1e-4, e
+    assert e["deg"] == 0.0, e
