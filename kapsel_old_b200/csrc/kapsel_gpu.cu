@@ -2689,6 +2689,8 @@ int kapsel_gpu_save_restart(kapsel_ctx *ctx, const char *path) {
   const bool el = b->prm.eq == KAPSEL_EQ_ELECTROLYTE;
   std::vector<double> conc(el ? 2 * plane : 0);
   if (el && (rc = b->conc_to_host(conc.data()))) return rc;
+  double obl[4] = {0.0, 0.0, 0.0, 0.0};
+  if (b->prm.eq == KAPSEL_EQ_SHEAR_LE && (rc = b->oblique_state(obl))) return rc;
   FILE *f = fopen(path, "w");
   if (!f) return KAPSEL_EINVAL;
   fprintf(f, "resume.Calculation = CONTINUE\n");
@@ -2715,7 +2717,7 @@ int kapsel_gpu_save_restart(kapsel_ctx *ctx, const char *path) {
   // inside its step loop, sp_3d_ns.cxx:606-616)
   fprintf(f, "%sjikan.ts = %d\n", kRes, b->ts - 1);
   fprintf(f, "%sjikan.time = %.17g\n", kRes, b->time);
-  fprintf(f, "%soblique.degree_oblique = %.17g\n", kRes, 0.0);
+  fprintf(f, "%soblique.degree_oblique = %.17g\n", kRes, obl[OB_DEG]);
   const bool ok = !ferror(f);
   fclose(f);
   return ok ? 0 : KAPSEL_EINVAL;
@@ -2732,8 +2734,8 @@ int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path) {
   std::vector<double> pv((size_t)std::max(Np, 1) * kNPF * 4, 0.0);
   std::vector<unsigned char> seen((size_t)std::max(Np, 1) * kNPF, 0);
   size_t nz_seen = 0;
-  int ts = -1, have_time = 0, nuk = 0;
-  double time = 0.0;
+  int ts = -1, have_time = 0, nuk = 0, have_deg = 0;
+  double time = 0.0, deg = 0.0;
   FILE *f = fopen(path, "r");
   if (!f) return KAPSEL_EINVAL;
   std::vector<char> line(1 << 12);
@@ -2779,6 +2781,9 @@ int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path) {
     } else if (!strncmp(s, "jikan.time", 10)) {
       time = val;
       have_time = 1;
+    } else if (!strncmp(s, "oblique.degree_oblique", 22)) {
+      deg = val;
+      have_deg = 1;
     }
   }
   fclose(f);
@@ -2816,10 +2821,30 @@ int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path) {
       for (int i = 0; i < 4; ++i) o[(which ? KAPSEL_P_QOLD : KAPSEL_P_Q) + i] = q[i] * (1.0 / nq);
     }
   }
-  int rc = kapsel_gpu_set_zeta(ctx, z.data(), uk.data());
+  int rc = 0;
+  const bool le = b->prm.eq == KAPSEL_EQ_SHEAR_LE;
+  if (le && (!have_deg || !std::isfinite(deg))) return KAPSEL_EINVAL;
+  if (le && b->ts == 0) {
+    // A resumed Lees-Edwards run takes its first step (at jikan.ts = the
+    // saved ts, so AB2 unless that is 0) from the fresh state before the
+    // restore (sp_3d_ns.cxx:547-627) and keeps that step's Shear_rate_eff,
+    // which the record does not hold: a fresh context takes the same
+    // discarded step.
+    if ((rc = b->fill_noise(0))) return rc;
+    b->launch_step(b->noise_dev[0], ts == 0 ? 1 : 0);
+    if ((rc = check_status(b))) return rc;
+  }
+  rc = kapsel_gpu_set_zeta(ctx, z.data(), uk.data());
   if (rc) return rc;
   if (el && (rc = b->conc_from_host(conc.data()))) return rc;
   if (Np > 0 && (rc = kapsel_gpu_set_particle_state(ctx, rec.data()))) return rc;
+  if (le) {
+    // degree_oblique is restored (resume.cxx:333-360; K2 is formed from it on
+    // the fly); Shear_rate_eff keeps its current value (above)
+    double obl[4];
+    if ((rc = b->oblique_state(obl))) return rc;
+    if ((rc = b->set_oblique_state(deg, obl[OB_SRATE]))) return rc;
+  }
   b->ts = ts + 1;
   b->time = time;
   // The reference's resumed run seeds the thermostat stream afresh

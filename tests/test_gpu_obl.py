@@ -150,3 +150,39 @@ def test_obl_mixed_precision_bound():
     assert e["u"] < 1e-5, e
     assert e["v"] < 1e-4, e
     assert e["deg"] == 0.0, e
+
+
+def test_obl_restart_records(tmp_path):
+    """Restart records carry degree_oblique: the GPU resumes a record the
+    reference saved (taking the resumed run's discarded first step, whose
+    Shear_rate_eff the reference keeps) and the reference resumes a GPU
+    record; both continue in step with the reference's resumed run."""
+    _need_ref()
+    import os
+
+    import kapsel_old_b200 as kg
+
+    cfg = _cfg(kbt=1e-3)
+    a = ref.RefSim(cfg)
+    a.set_oblique(0.9987, 0.0)  # passes 1 (grid reset) inside the saved run
+    a.step(5)
+    path = os.path.join(tmp_path, "ref.res")
+    a.save_restart(path)
+    b = ref.RefSim(cfg)
+    b.resume(path)
+    g = kg.Simulation(cfg, precision=kg.FP64)
+    g.load_restart(path)
+    assert g.oblique()["degree_oblique"] == b.oblique()["degree_oblique"] == a.oblique()["degree_oblique"]
+    assert abs(g.oblique()["shear_rate_eff"] - b.oblique()["shear_rate_eff"]) < 1e-12
+    b.step(4)
+    g.step(4)
+    assert rel(g.zeta(), _trunc(b.zeta(), cfg)) < FP64_TOL
+    for k in ("x", "v", "omega"):
+        assert rel(g.particles()[k], b.particles()[k]) < FP64_TOL, k
+    # the GPU's own record, resumed by the reference
+    path2 = os.path.join(tmp_path, "gpu.res")
+    g.save_restart(path2)
+    c = ref.RefSim(cfg)
+    c.resume(path2)
+    assert c.oblique()["degree_oblique"] == g.oblique()["degree_oblique"]
+    assert rel(_trunc(c.zeta(), cfg), g.zeta()) < 1e-14
