@@ -276,6 +276,11 @@ def run_ours(args, rank, world, local_rank):
         s3m.close()
         s3d, _, ms3d = timed(kg.FP64, k2, args.warmup, cfg=c3)
         s3d.close()
+        c6 = workload.shear_le_128_256()
+        s6m, _, ms6m = timed(kg.MIXED, k2, args.warmup, cfg=c6)
+        s6m.close()
+        s6d, _, ms6d = timed(kg.FP64, k2, args.warmup, cfg=c6)
+        s6d.close()
         extra = {
             "plain_64cubed_16_fp64": {"value": round(k2 * world / (ms1 * 1e-3), 2), "unit": UNIT, "steps": k2,
                                       "workload": "64^3, 16 spheres a=5, kBT=0, body force 1e-3 along -z, FP64"},
@@ -283,6 +288,10 @@ def run_ours(args, rank, world, local_rank):
                                         "fp64": round(k2 * world / (ms3d * 1e-3), 2), "unit": UNIT, "steps": k2,
                                         "workload": "128^3, 64 spheres a=5 Z=-100, salt Debye 4, Bjerrum 0.7, "
                                                     "E_x=0.05"},
+            "shear_le_128cubed_256": {"mixed": round(k2 * world / (ms6m * 1e-3), 2),
+                                      "fp64": round(k2 * world / (ms6d * 1e-3), 2), "unit": UNIT, "steps": k2,
+                                      "workload": "128^3, 256 spheres a=5, kBT=1e-3, Lees-Edwards shear rate 0.01 "
+                                                  "(oblique grid)"},
         }
         # batched ensemble: 48 boxes of 4 shapes, one graph launch per step
         boxes = workload.batched()
@@ -352,6 +361,7 @@ def run_ours(args, rank, world, local_rank):
             extra["batched_48_boxes"]["cpu_baseline"] = cpu_baseline_batch(boxes)
             extra["plain_64cubed_16_fp64"]["cpu_baseline"] = cpu_baseline(c1, warmup=1, steps=30)
             extra["electrolyte_128cubed_64"]["cpu_baseline"] = cpu_baseline(c3, warmup=1, steps=4)
+            extra["shear_le_128cubed_256"]["cpu_baseline"] = cpu_baseline(c6, warmup=1, steps=8)
 
     steps_total = args.steps * world
     value = replica_value(args.steps, world, ms_m * 1e-3)

@@ -75,6 +75,16 @@ def electrolyte_128_64() -> dict:
     return cfg
 
 
+def shear_le_128_256() -> dict:
+    """The C2 suspension (128^3, 256 spheres a=5, kBT=1e-3, seed 2) under
+    Lees-Edwards shear (Shear_Navier_Stokes_Lees_Edwards, DC shear rate 0.01;
+    the wall-to-wall velocity difference is 1.28)."""
+    cfg = spm_config((7, 7, 7), 256, seed=2, kbt=1e-3)
+    cfg["eq"] = "Shear_Navier_Stokes_Lees_Edwards"
+    cfg["shear_rate"] = 0.01
+    return cfg
+
+
 BATCH_SHAPES = [(5, 5, 5), (6, 6, 6), (6, 6, 7), (7, 7, 7)]  # 32^3, 64^3, 64x64x128, 128^3
 
 
