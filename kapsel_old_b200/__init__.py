@@ -303,6 +303,26 @@ class Simulation:
         a = np.ascontiguousarray(e, dtype=np.float64)
         self._check(self.L.kapsel_gpu_set_efield(self.h, _ptr(a)))
 
+    def udf_record(self) -> dict:
+        """One Output_udf record of the current state (avs_output.cxx:343-450):
+        E (the reference writes 1.0), t = jikan.ts and, per particle, R, R_raw
+        (unwrapped), v, q, omega, the previous step's f_hydro, torque_hydro and
+        f_r, and zero torque_r, f_slip, torque_slip (spherical, no slip).
+        Nested as the outParticle class of define.udf, for udf_io.write_records."""
+        ts, _ = self.time()
+        p = self.particles()
+        v3 = lambda a: {"x": float(a[0]), "y": float(a[1]), "z": float(a[2])}
+        zero = {"x": 0.0, "y": 0.0, "z": 0.0}
+        parts = []
+        for n in range(self.Np):
+            q = p["q"][n]
+            parts.append({"R": v3(p["x"][n]), "R_raw": v3(p["x_nopbc"][n]), "v": v3(p["v"][n]),
+                          "q": {"q0": float(q[0]), "q1": float(q[1]), "q2": float(q[2]), "q3": float(q[3])},
+                          "omega": v3(p["omega"][n]), "f_hydro": v3(p["f_hydro"][n]),
+                          "torque_hydro": v3(p["torque_hydro"][n]), "f_r": v3(p["fr"][n]),
+                          "torque_r": dict(zero), "f_slip": dict(zero), "torque_slip": dict(zero)})
+        return {"E": 1.0, "t": ts, "Particles": parts}
+
     def oblique(self) -> dict:
         """Lees-Edwards state: degree_oblique, Shear_rate_eff, Shear_strain_realized."""
         a = np.zeros(3)

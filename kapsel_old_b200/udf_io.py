@@ -24,7 +24,7 @@ import math
 import os
 import re
 
-__all__ = ["parse", "read", "flatten", "write", "to_config", "UDFError"]
+__all__ = ["parse", "read", "flatten", "write", "write_records", "read_records", "to_config", "UDFError"]
 
 
 class UDFError(ValueError):
@@ -331,6 +331,50 @@ def write(path: str, data: dict, define_file: str, defs: _Defs | None = None):
     lines.append("\\end{data}")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
+
+
+def write_records(path: str, records: list, define_file: str, header: dict | None = None,
+                  defs: _Defs | None = None):
+    """Write an output UDF: the definitions by ``\\include``, then one
+    ``\\begin{data}`` block per record, values positional in declaration
+    order.  `header` (entry name -> nested value), when given, is record 0:
+    the input values the reference echoes into its output file before the
+    first snapshot (Gourmet_file_io); each later record is one Output_udf
+    call (avs_output.cxx:343-450: E, t, Particles[])."""
+    if defs is None:
+        with open(define_file if os.path.isabs(define_file) else
+                  os.path.join(os.path.dirname(os.path.abspath(path)), define_file)) as f:
+            defs, _ = parse(f.read(), os.path.dirname(os.path.abspath(path)))
+    lines = [f'\\include{{"{os.path.basename(define_file)}"}}', ""]
+    for rec in ([header] if header else []) + list(records):
+        lines.append("\\begin{data}")
+        for fdef in defs.entries:
+            if fdef.name in rec:
+                lines.append(f"{fdef.name}:{_write_value(rec[fdef.name], fdef.typ, fdef.dims, 1)}")
+        lines.append("\\end{data}")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def read_records(path: str) -> list:
+    """Flattened `path -> value` map of every ``\\begin{data}`` block of a
+    UDF file, in order (one per record)."""
+    with open(path) as f:
+        text = f.read()
+    base = os.path.dirname(os.path.abspath(path))
+    defs = _Defs()
+    out = []
+    for name, body in _blocks(text):
+        if name == "include":
+            p = body if os.path.isabs(body) else os.path.join(base, body)
+            with open(p) as g:
+                parse(g.read(), os.path.dirname(p), defs)
+        elif name in ("def", "global_def"):
+            defs.add_block(_tokens(body))
+        elif name == "data":
+            _, data = parse("\\begin{data}" + body + "\\end{data}", base, defs)
+            out.append(flatten(data))
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -60,6 +60,7 @@ class RefSim:
         L.kref_time_steps.argtypes = [ctypes.c_int]
         L.kref_time_steps.restype = ctypes.c_double
         L.kref_oblique.argtypes = [dp]
+        L.kref_output_udf.argtypes = []
         L.kref_set_particle_velocity.argtypes = [ctypes.c_int, dp, dp]
         L.kref_set_oblique.argtypes = [ctypes.c_double, ctypes.c_double]
         self.cfg = cfg
@@ -129,6 +130,24 @@ class RefSim:
         a = np.zeros(3)
         self.lib.kref_oblique(self._p(a))
         return {"degree_oblique": float(a[0]), "shear_rate_eff": float(a[1]), "strain": float(a[2])}
+
+    def output_udf(self):
+        """Output_udf of the current state (appends one record)."""
+        assert self.lib.kref_output_udf() == 0
+
+    def udf_records(self) -> list:
+        """The output records written so far: list of {path: value text},
+        record 0 first (the stand-in manager's "record <n> path = value" lines)."""
+        recs = []
+        with open(self.kv + ".out") as f:
+            for line in f:
+                head, _, val = line.rstrip("\n").partition(" = ")
+                _, n, path = head.split(" ", 2)
+                n = int(n)
+                while len(recs) <= n:
+                    recs.append({})
+                recs[n][path] = val
+        return recs
 
     def set_particle_velocity(self, n: int, v, omega):
         v = np.ascontiguousarray(v, dtype=np.float64)

@@ -96,6 +96,17 @@ int kref_step(int n) {
   return 0;
 }
 
+/* Output_udf of the current state into the output record file (the stand-in
+   manager writes "record <n> path = value" lines to <input>.out, record 0
+   holding the input values Gourmet_file_io echoed); as the step loop calls
+   it (sp_3d_ns.cxx:568-570). */
+int kref_output_udf(void) {
+  if (!g_ready || !ufout) return -1;
+  Output_udf(ufout, Avs_parameters, g_zeta, g_uk_dc, g_particles, g_jikan);
+  ufout->write();
+  return 0;
+}
+
 /* Set the velocity and angular velocity of particle n (and their previous
    values, as a fresh start has them equal). */
 int kref_set_particle_velocity(int n, const double *v, const double *w) {

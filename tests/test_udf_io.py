@@ -121,3 +121,42 @@ def test_write_read_roundtrip(tmp_path):
         assert a.keys() == b.keys()
         for k in a:
             assert a[k] == b[k] or (isinstance(a[k], float) and np.isclose(a[k], b[k], rtol=0, atol=0)), k
+
+
+_OUT_DEFS = """\\begin{def}
+class Vector3d:{x: float, y: float, z: float}
+class Quaternion:{q0: float, q1: float, q2: float, q3: float}
+class outParticle:{R:Vector3d, R_raw:Vector3d, v:Vector3d, q:Quaternion, omega:Vector3d,
+                   f_hydro:Vector3d, torque_hydro:Vector3d, f_r:Vector3d, torque_r:Vector3d,
+                   f_slip:Vector3d, torque_slip:Vector3d}
+E: float
+t: float
+Particles[]: outParticle
+\\end{def}
+"""
+
+
+def test_output_records_round_trip(tmp_path):
+    """write_records / read_records: one data block per Output_udf record,
+    positional in the outParticle declaration order, read back by path."""
+    from kapsel_old_b200 import udf_io
+
+    d = tmp_path / "out_define.udf"
+    d.write_text(_OUT_DEFS)
+    v = lambda a, b, c: {"x": a, "y": b, "z": c}
+    part = lambda s: {"R": v(s, 2 * s, 3.5), "R_raw": v(s + 64, 2 * s, 3.5), "v": v(-s, 0.25, 1e-17),
+                      "q": {"q0": 1.0, "q1": 0.0, "q2": -0.0, "q3": 0.0}, "omega": v(0.0, s, 0.0),
+                      "f_hydro": v(1e5, -2.5e-300, 0.0), "torque_hydro": v(0.1, 0.2, 0.3), "f_r": v(0, 0, -7.0),
+                      "torque_r": v(0, 0, 0), "f_slip": v(0, 0, 0), "torque_slip": v(0, 0, 0)}
+    recs = [{"E": 1.0, "t": 0, "Particles": [part(1.0), part(2.0)]},
+            {"E": 1.0, "t": 100, "Particles": [part(0.125), part(1 / 3)]}]
+    path = tmp_path / "out.udf"
+    udf_io.write_records(str(path), recs, str(d))
+    back = udf_io.read_records(str(path))
+    assert len(back) == 2
+    for r, b in zip(recs, back):
+        flat = udf_io.flatten(r)
+        assert set(flat) == set(b)
+        for k, x in flat.items():
+            assert float(b[k]) == float(x), k
+    assert back[1]["Particles[1].R.x"] == 1 / 3
