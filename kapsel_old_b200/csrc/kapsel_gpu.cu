@@ -239,7 +239,7 @@ struct Box : BoxBase {
   R *phiup = nullptr;     // [4][NX][NY][NZ]
   Cx<R> *twbuf = nullptr;
   Twiddles<R> tw;
-  static constexpr int KCX = sizeof(R) == 4 ? 8 : 4;    // x-pass kz tile
+  static constexpr int KCX = sizeof(R) == 4 ? 4 : 4;    // x-pass kz tile
   static constexpr int KCY = sizeof(R) == 4 ? 32 : 16;  // y-pass kz tile
   size_t smem_xu = 0, smem_xadv = 0, smem_xf = 0, smem_y = 0, smem_zp = 0, smem_zc = 0, smem_zf = 0, smem_zr = 0;
 
@@ -307,16 +307,18 @@ struct Box : BoxBase {
   int zw_setup() {
     using Z = ZL<LM>;
     const size_t line = sizeof(Cx<R>) * Z::RW * Z::LS * ZNW;
-    zw_sm_p = 5 * line;
+    // FP64: the prefetching products kernel; FP32: the direct one
+    zw_sm_p = sizeof(R) == 8 ? sizeof(Cx<R>) * (size_t)ZProd<R, LM>::WARP * ZNW : 5 * line;
     zw_sm_c = 2 * line;
     zw_sm_f = 3 * line;
-    KCHECK(cudaFuncSetAttribute(k_zw_products<R, LM, ZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_p));
+    auto kp = sizeof(R) == 8 ? k_zw_products_pf<R, LM, ZNW> : k_zw_products<R, LM, ZNW>;
+    KCHECK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_p));
     KCHECK(cudaFuncSetAttribute(k_zw_c2r<R, LM, ZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_c));
     KCHECK(cudaFuncSetAttribute(k_zw_force<R, LM, ZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_f));
     int dev = 0, nsm = 0, op = 0, oc = 0, of = 0;
     KCHECK(cudaGetDevice(&dev));
     KCHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    KCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, k_zw_products<R, LM, ZNW>, ZNW * 32, zw_sm_p));
+    KCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, kp, ZNW * 32, zw_sm_p));
     KCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oc, k_zw_c2r<R, LM, ZNW>, ZNW * 32, zw_sm_c));
     KCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&of, k_zw_force<R, LM, ZNW>, ZNW * 32, zw_sm_f));
     const int groups = g.NX * g.NY / Z::RW;
@@ -328,7 +330,8 @@ struct Box : BoxBase {
   }
   template <int LM>
   void zw_products(bool pdl) {
-    launch_k(pdl, k_zw_products<R, LM, ZNW>, dim3(zw_grid_p), dim3(ZNW * 32), zw_sm_p, stream, g, tw, bufB);
+    launch_k(pdl, sizeof(R) == 8 ? k_zw_products_pf<R, LM, ZNW> : k_zw_products<R, LM, ZNW>, dim3(zw_grid_p),
+             dim3(ZNW * 32), zw_sm_p, stream, g, tw, bufB);
   }
   template <int LM>
   void zw_c2r(bool pdl, DPart *pts, int euler) {

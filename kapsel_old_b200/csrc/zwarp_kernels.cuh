@@ -138,7 +138,10 @@ struct Vec2<double> {
 // ---------------------------------------------------------------------------
 // Nonlinear-term centre (as k_z_products): per row group, inverse z of the
 // three velocity components, the five products, forward z (kz < TZ kept).
-// In place on I2.  Warps stride over row groups of RW rows.
+// In place on I2.  Warps stride over row groups of RW rows; five line groups
+// per warp, the input staged in groups 3-4 by plain loads.  Used for FP32
+// fields, whose working set stays in L2 at 128^3: there it beats the
+// prefetching variant below inside the step's launch chain.
 template <typename R, int LM, int NW>
 __global__ void __launch_bounds__(NW * 32) k_zw_products(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ io) {
   using Z = ZL<LM>;
@@ -190,6 +193,106 @@ __global__ void __launch_bounds__(NW * 32) k_zw_products(Geo g, Twiddles<R> tw, 
       for (int i = lane; i < Z::RW * Z::TZ; i += 32) {
         const int rr = i / Z::TZ, k = i - rr * Z::TZ;
         dst[rr * Z::TS + k] = wunpack_r2c<R, LM>(buf + (q * Z::RW + rr) * Z::LS, k, tw.z);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Nonlinear-term centre with prefetch (FP64 fields): as k_zw_products, but
+// each warp owns
+// four line groups and a stage area: while it transforms one row group,
+// cp.async brings the next group's three input rows into the stage.  Four
+// products go through the line groups; the fifth waits in registers and
+// reuses group 0 once the first four are stored.
+template <typename R, int LM>
+struct ZProd {
+  using Z = ZL<LM>;
+  static constexpr int GL = Z::RW * Z::LS;     // one line group
+  static constexpr int SG = 3 * Z::RW * Z::TS;  // staged input of a row group
+  static constexpr int WARP = 4 * GL + SG;      // elements per warp
+  static constexpr int KP = Z::RW * Z::M / 32;  // product elements per lane
+};
+
+template <typename R, int LM, int NW>
+__global__ void __launch_bounds__(NW * 32) k_zw_products_pf(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ io) {
+  using Z = ZL<LM>;
+  using P = ZProd<R, LM>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_begin();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  Cx<R> *buf = reinterpret_cast<Cx<R> *>(smem_raw) + (size_t)warp * P::WARP;
+  Cx<R> *stage = buf + 4 * P::GL;  // [3][RW][TS]
+  Cx<R> wi[Z::N1], wf[Z::N1], wk[Z::KW];
+  wfft_twiddles<R, LM, -1>(tw.m, wi);
+  wfft_twiddles<R, LM, 1>(tw.m, wf);
+  wpre_twiddles<R, LM>(tw.z, wk);
+  const size_t rows = (size_t)g.NX * g.NY;
+  const size_t cstr = rows * Z::TS;
+  const int ngroups = (int)(rows / Z::RW);
+  const int gstride = gridDim.x * NW;
+  const R sc = R(g.inv_n);
+  int grp = blockIdx.x * NW + warp;
+  auto issue = [&](int gq) {
+    const size_t r0 = (size_t)gq * Z::RW;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const Cx<R> *src = io + c * cstr + r0 * Z::TS;
+      for (int i = lane; i < Z::RW * Z::TS; i += 32) cp_async_cx(stage + c * Z::RW * Z::TS + i, src + i);
+    }
+    cp_async_commit();
+  };
+  if (grp < ngroups) issue(grp);
+  for (; grp < ngroups; grp += gstride) {
+    const size_t row0 = (size_t)grp * Z::RW;
+    cp_async_wait_all();
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      for (int rr = 0; rr < Z::RW; ++rr)
+        wpack_c2r<R, LM>(stage + (c * Z::RW + rr) * Z::TS, buf + c * P::GL + rr * Z::LS, wk);
+    __syncwarp();
+    if (grp + gstride < ngroups) issue(grp + gstride);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) wfft<R, LM, -1>(buf + c * P::GL, wi);
+    Cx<R> p4[P::KP];
+#pragma unroll
+    for (int jj = 0; jj < P::KP; ++jj) {
+      const int i = lane + 32 * jj;
+      const int rr = i >> LM, n = rr * Z::LS + zpos<LM>(i & (Z::M - 1));
+      const Cx<R> U1 = buf[n], U2 = buf[P::GL + n], U3 = buf[2 * P::GL + n];
+      const R u1a = U1.x * sc, u1b = U1.y * sc, u2a = U2.x * sc, u2b = U2.y * sc, u3a = U3.x * sc, u3b = U3.y * sc;
+      buf[n] = {u2a * u3a, u2b * u3b};
+      buf[P::GL + n] = {u3a * u1a, u3b * u1b};
+      buf[2 * P::GL + n] = {u1a * u2a, u1b * u2b};
+      buf[3 * P::GL + n] = {(u2a - u3a) * (u2a + u3a), (u2b - u3b) * (u2b + u3b)};
+      p4[jj] = {(u3a - u1a) * (u3a + u1a), (u3b - u1b) * (u3b + u1b)};
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) wfft<R, LM, 1>(buf + q * P::GL, wf);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      Cx<R> *dst = io + q * cstr + row0 * Z::TS;
+      for (int i = lane; i < Z::RW * Z::TZ; i += 32) {
+        const int rr = i / Z::TZ, k = i - rr * Z::TZ;
+        dst[rr * Z::TS + k] = wunpack_r2c<R, LM>(buf + q * P::GL + rr * Z::LS, k, tw.z);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int jj = 0; jj < P::KP; ++jj) {
+      const int i = lane + 32 * jj;
+      buf[(i >> LM) * Z::LS + zpos<LM>(i & (Z::M - 1))] = p4[jj];
+    }
+    __syncwarp();
+    wfft<R, LM, 1>(buf, wf);
+    {
+      Cx<R> *dst = io + 4 * cstr + row0 * Z::TS;
+      for (int i = lane; i < Z::RW * Z::TZ; i += 32) {
+        const int rr = i / Z::TZ, k = i - rr * Z::TZ;
+        dst[rr * Z::TS + k] = wunpack_r2c<R, LM>(buf + rr * Z::LS, k, tw.z);
       }
     }
     __syncwarp();
