@@ -171,3 +171,17 @@ def test_step_mixed_precision_bound():
     w = _compare_run(cfg, 5, 1)
     assert w["u"] < 1e-5, w
     assert w["v"] < 1e-4, w
+
+
+def test_step_mixed_128_against_fp64():
+    """128^3 mixed step (the warp-level y and z kernels) against the FP64
+    path, which the tests above pin to the oracle: same bound as the mixed
+    test at 64^3."""
+    cfg = _cfg((7, 7, 7), 32, seed=5, kbt=1e-3)
+    a = _sim(cfg, 0)
+    b = _sim(cfg, 1)
+    for _ in range(4):
+        a.step(1, graph=True)
+        b.step(1, graph=True)
+    assert rel(b.velocity(), a.velocity()) < 1e-5
+    assert rel(b.particles()["v"], a.particles()["v"]) < 1e-4
