@@ -290,9 +290,12 @@ __global__ void __launch_bounds__(1024) k_particles_hydro_velocity(PPar p, DPart
         rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);
         r[d] = (float)cell[d] * dxf - resf[d];
       }
+      const float ph = prof_phi_f(sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]), rpf, rmf, dxf);
+      // phi is exactly zero beyond a + xi/2 (about half of the Sekibun
+      // points): those terms add zeros, so their loads are skipped
+      if (ph == 0.f) continue;
       const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
       const float ug[3] = {(float)__ldg(u + im), (float)__ldg(u + npts + im), (float)__ldg(u + 2 * npts + im)};
-      const float ph = prof_phi_f(sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]), rpf, rmf, dxf);
       float vr[3] = {0.f, 0.f, 0.f};
       if (p.rotation) {
         vr[0] = wpf[1] * r[2] - wpf[2] * r[1];
@@ -314,10 +317,10 @@ __global__ void __launch_bounds__(1024) k_particles_hydro_velocity(PPar p, DPart
     int rm[3];
     double r[3], dist;
     stencil_point(b, cells + 3 * m, xp, p, rm, r, dist);
-    const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
-    // issue the field loads before the profile exps so they overlap
-    const double ug[3] = {(double)__ldg(u + im), (double)__ldg(u + npts + im), (double)__ldg(u + 2 * npts + im)};
     const double ph = (double)prof_phi<R>(dist, p);
+    if (ph == 0.0) continue;  // a zero term: skip its loads
+    const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
+    const double ug[3] = {(double)__ldg(u + im), (double)__ldg(u + npts + im), (double)__ldg(u + 2 * npts + im)};
     double vr[3] = {0.0, 0.0, 0.0};
     if (p.rotation) {
       vr[0] = wp[1] * r[2] - wp[2] * r[1];
@@ -515,6 +518,7 @@ __global__ void __launch_bounds__(256) k_particles_scatter(PPar p, const DPart *
         r[d] = (float)cell[d] * dxf - resf[d];
       }
       const float ph = prof_phi_f(sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]), rpf, rmf, dxf);
+      if (ph == 0.f) continue;  // adds zeros: no atomics
       float vr[3] = {0.f, 0.f, 0.f};
       if (p.rotation) {
         vr[0] = wpf[1] * r[2] - wpf[2] * r[1];
@@ -535,6 +539,7 @@ __global__ void __launch_bounds__(256) k_particles_scatter(PPar p, const DPart *
     double r[3], dist;
     stencil_point(b, cells + 3 * m, xp, p, rm, r, dist);
     const double ph = (double)prof_phi<R>(dist, p);
+    if (ph == 0.0) continue;  // adds zeros: no atomics
     double vr[3] = {0.0, 0.0, 0.0};
     if (p.rotation) {
       vr[0] = wp[1] * r[2] - wp[2] * r[1];
