@@ -228,6 +228,26 @@ struct BoxBase {
     KCHECK(cudaEventRecord(noise_ev[slot], stream));
     return 0;
   }
+  // The normals of step ts are drawn while the GPU runs step ts-1
+  // (prefill_noise right after its launch); take_noise uses them when they
+  // are there.  The draw order, and so the stream, is unchanged.
+  int noise_pre_ts[2] = {-1, -1};
+  int take_noise(int slot) {
+    if (noise_pre_ts[slot] == ts) {
+      noise_pre_ts[slot] = -1;
+      return 0;
+    }
+    return fill_noise(slot);
+  }
+  int prefill_noise() {
+    const int slot = ts & 1;
+    if (!pp.thermostat || noise_pre_ts[slot] == ts) return 0;
+    const int rc = fill_noise(slot);
+    if (!rc) noise_pre_ts[slot] = ts;
+    return rc;
+  }
+  void drop_prefill() { noise_pre_ts[0] = noise_pre_ts[1] = -1; }
+  DPart *parts_host = nullptr;  // pinned staging of the particle readout
 };
 
 template <typename R>
@@ -1606,6 +1626,7 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   }
   const int np1 = b->Np > 0 ? b->Np : 1;
   if (cudaMalloc(&b->parts, sizeof(DPart) * np1) != cudaSuccess) return KAPSEL_ENOMEM;
+  if (cudaMallocHost(&b->parts_host, sizeof(DPart) * np1) != cudaSuccess) return KAPSEL_ENOMEM;
   if (cudaMemset(b->parts, 0, sizeof(DPart) * np1) != cudaSuccess) return KAPSEL_ECUDA;
   if (cudaMalloc(&b->cells, sizeof(int) * cells.size()) != cudaSuccess) return KAPSEL_ENOMEM;
   if (cudaMemcpy(b->cells, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -1644,6 +1665,7 @@ int kapsel_gpu_destroy(kapsel_ctx *ctx) {
     }
     b->free_all();
     cudaFree(b->parts);
+    cudaFreeHost(b->parts_host);
     cudaFree(b->cells);
     cudaFree(b->uk_dc);
     cudaFree(b->status);
@@ -1718,6 +1740,7 @@ int kapsel_gpu_init_state(kapsel_ctx *ctx) {
   }
   b->ts = 0;
   b->time = 0.0;
+  b->drop_prefill();
   b->initialised = true;
   return 0;
 }
@@ -1737,7 +1760,7 @@ static int step_impl(kapsel_ctx *ctx, int n, bool use_graph) {
   if (!b->initialised) return KAPSEL_ESTATE;
   for (int s = 0; s < n; ++s) {
     const int slot = b->ts & 1;
-    int rc = b->fill_noise(slot);
+    int rc = b->take_noise(slot);
     if (rc) return rc;
     const int euler = b->ts == 0 ? 1 : 0;
     if (use_graph && !euler) {
@@ -1755,6 +1778,7 @@ static int step_impl(kapsel_ctx *ctx, int n, bool use_graph) {
     }
     b->ts += 1;
     b->time += b->prm.dt;
+    if ((rc = b->prefill_noise())) return rc;
   }
   return check_status(b);
 }
@@ -1795,9 +1819,9 @@ int kapsel_gpu_get_velocity(kapsel_ctx *ctx, double *u) {
 int kapsel_gpu_get_particles(kapsel_ctx *ctx, double *out) {
   if (!ctx || (!out && ctx->box->Np > 0)) return KAPSEL_EINVAL;
   BoxBase *b = ctx->box.get();
-  std::vector<DPart> h(b->Np > 0 ? b->Np : 1);
-  if (cudaMemcpyAsync(h.data(), b->parts, sizeof(DPart) * h.size(), cudaMemcpyDeviceToHost, b->stream) !=
-      cudaSuccess)
+  const DPart *h = b->parts_host;  // pinned: a direct DMA, no staging copy
+  if (cudaMemcpyAsync(b->parts_host, b->parts, sizeof(DPart) * std::max(b->Np, 1), cudaMemcpyDeviceToHost,
+                      b->stream) != cudaSuccess)
     return KAPSEL_ECUDA;
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
   for (int n = 0; n < b->Np; ++n) {
@@ -2034,7 +2058,7 @@ int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms) {
   BoxBase *b = ctx->box.get();
   if (!b->initialised) return KAPSEL_ESTATE;
   const int slot = b->ts & 1;
-  int rc = b->fill_noise(slot);
+  int rc = b->take_noise(slot);
   if (rc) return rc;
   cudaEvent_t ev[KAPSEL_N_STEP_KERNELS + 1];
   for (int i = 0; i <= KAPSEL_N_STEP_KERNELS; ++i)
@@ -2130,7 +2154,7 @@ int kapsel_batch_step(kapsel_batch *b, int nsteps) {
     const int euler = first->ts == 0 ? 1 : 0;
     for (int i = 0; i < n; ++i) {
       BoxBase *x = b->boxes[i]->box.get();
-      int rc = x->fill_noise(slot);
+      int rc = x->take_noise(slot);
       if (rc) return rc;
     }
     if (euler) {
@@ -2855,6 +2879,7 @@ int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path) {
   // restore overwrites the state (sp_3d_ns.cxx:547-627), which draws one
   // step of normals: the stream continues after those.
   b->mt.reset(new MT19937(b->prm.mt_seed));
+  b->drop_prefill();
   if (b->pp.thermostat) {
     double pair[2];
     for (int n = 0; n < 3 * Np; ++n) b->mt->gauss2(pair);
