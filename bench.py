@@ -469,7 +469,7 @@ def cpu_baseline_batch(boxes):
             "sample": "one box per shape timed for 2 steps (OpenMP build, all cores), summed over the 48 boxes"}
 
 
-def run_reference(args):
+def run_reference(args, world: int = 1):
     from kapsel_old_b200 import workload
 
     cfg = workload.mixed_128_256()
@@ -480,7 +480,7 @@ def run_reference(args):
         "metric": METRIC,
         "value": cb["value"],
         "unit": UNIT,
-        "n_gpus": 0,
+        "n_gpus": world,  # the launch's N; the work runs on rank 0's host cores (cpu_baseline.cores)
         "steps": steps,
         "warmup": max(1, min(args.warmup, 3)),
         "ms_per_step": round(1000.0 / cb["value"], 3),
@@ -512,7 +512,7 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps(run_reference(args)), flush=True)
+            print(json.dumps(run_reference(args, world)), flush=True)
         return
 
     if world > 1:

@@ -185,3 +185,32 @@ def test_step_mixed_128_against_fp64():
         b.step(1, graph=True)
     assert rel(b.velocity(), a.velocity()) < 1e-5
     assert rel(b.particles()["v"], a.particles()["v"]) < 1e-4
+
+
+def test_thermostat_stream_independent_of_call_pattern():
+    """The normals of step ts are drawn ahead while step ts-1 runs; the
+    stream must not depend on how steps are called: one call, single steps,
+    graph replay and an interleaved per-kernel profiling step all give the
+    same state."""
+    import ctypes
+
+    import kapsel_old_b200 as kg
+
+    cfg = _cfg((5, 5, 5), 4, seed=3, kbt=1e-3)
+    a = _sim(cfg)
+    a.step(7)
+    b = _sim(cfg)
+    for _ in range(7):
+        b.step(1)
+    c = _sim(cfg)
+    c.step(2)
+    c.step(3, graph=True)
+    L = kg.load_library()
+    L.kapsel_gpu_profile_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]
+    ms = (ctypes.c_float * 13)()
+    assert L.kapsel_gpu_profile_step(c.h, ms) == 0
+    c.step(1, graph=True)
+    for s in (b, c):
+        assert s.time()[0] == 7
+        assert rel(s.particles()["v"], a.particles()["v"]) < 1e-13
+        assert rel(s.zeta(), a.zeta()) < 1e-13
