@@ -4,7 +4,7 @@
 // State that changes every step lives in device memory so that the step can
 // be captured into a CUDA graph: ObState[0] = degree_oblique (input.cxx:271),
 // [1] = Shear_rate_eff, [2] = 1 when this step reset the oblique grid,
-// [3] = Shear_strain_realized (sp_3d_ns.cxx:600), [4..] reduction partials.
+// [3] = Shear_strain_realized (sp_3d_ns.cxx:600), [8..] reduction partials.
 //
 // k-space operators (one mode at a time, retained 2/3 box only; the
 // reference truncates zeta at the start of every step, operate_omega.cxx:
