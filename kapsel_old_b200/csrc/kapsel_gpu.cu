@@ -327,8 +327,8 @@ struct Box : BoxBase {
   int zw_setup() {
     using Z = ZL<LM>;
     const size_t line = sizeof(Cx<R>) * Z::RW * Z::LS * ZNW;
-    // FP64: the prefetching products kernel; FP32: the direct one
-    zw_sm_p = sizeof(R) == 8 ? sizeof(Cx<R>) * (size_t)ZProd<R, LM>::WARP * ZNW : 5 * line;
+    // FP64: the prefetching products kernel; FP32: four line groups per warp
+    zw_sm_p = sizeof(R) == 8 ? sizeof(Cx<R>) * (size_t)ZProd<R, LM>::WARP * ZNW : 4 * line;
     zw_sm_c = 2 * line;
     zw_sm_f = 3 * line;
     auto kp = sizeof(R) == 8 ? k_zw_products_pf<R, LM, ZNW> : k_zw_products<R, LM, ZNW>;
@@ -477,13 +477,14 @@ struct Box : BoxBase {
   bool use_pdl = true;
   // warp-level y pass: persistent grid of YNW-warp blocks, two slots per warp
   static constexpr int YNW = 4;
+  static constexpr int YSLOTS = sizeof(R) == 4 ? 1 : 2;
   int yw_occ[2][2] = {{0, 0}, {0, 0}};  // blocks per SM, [inverse][full spectrum]
   int nsm = 0;
   template <bool INV, int LY, bool FULL>
   void yw_launch(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out, bool pdl) {
     using Y = ZL<LY>;
-    auto kern = k_yw_pass<R, INV, LY, FULL, YNW>;
-    const size_t sm = sizeof(Cx<R>) * 2 * Y::RW * Y::LS * YNW;
+    auto kern = k_yw_pass<R, INV, LY, FULL, YNW, YSLOTS>;
+    const size_t sm = sizeof(Cx<R>) * YSLOTS * Y::RW * Y::LS * YNW;
     int &occ = yw_occ[INV ? 1 : 0][FULL ? 1 : 0];
     if (!occ) {
       int dev = 0;

@@ -138,18 +138,20 @@ struct Vec2<double> {
 // ---------------------------------------------------------------------------
 // Nonlinear-term centre (as k_z_products): per row group, inverse z of the
 // three velocity components, the five products, forward z (kz < TZ kept).
-// In place on I2.  Warps stride over row groups of RW rows; five line groups
-// per warp, the input staged in groups 3-4 by plain loads.  Used for FP32
-// fields, whose working set stays in L2 at 128^3: there it beats the
-// prefetching variant below inside the step's launch chain.
+// In place on I2.  Warps stride over row groups of RW rows.  FP32 fields:
+// four line groups per warp (the c2r packing reads the rows straight from
+// global memory, so no stage area), the fifth product waits in registers
+// and reuses group 0 once the first four are stored.  The small per-warp
+// footprint keeps 24 warps per SM resident, which hides the load latency
+// better than a prefetch stage at 16.
 template <typename R, int LM, int NW>
 __global__ void __launch_bounds__(NW * 32) k_zw_products(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ io) {
   using Z = ZL<LM>;
+  constexpr int GL = Z::RW * Z::LS, KP = Z::RW * Z::M / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_begin();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  Cx<R> *buf = reinterpret_cast<Cx<R> *>(smem_raw) + (size_t)warp * 5 * Z::RW * Z::LS;
-  Cx<R> *stage = buf + 3 * Z::RW * Z::LS;  // staged input rows [3][RW][TS]; later product lines 3, 4
+  Cx<R> *buf = reinterpret_cast<Cx<R> *>(smem_raw) + (size_t)warp * 4 * GL;
   Cx<R> wi[Z::N1], wf[Z::N1], wk[Z::KW];
   wfft_twiddles<R, LM, -1>(tw.m, wi);
   wfft_twiddles<R, LM, 1>(tw.m, wf);
@@ -161,38 +163,49 @@ __global__ void __launch_bounds__(NW * 32) k_zw_products(Geo g, Twiddles<R> tw, 
   for (int grp = blockIdx.x * NW + warp; grp < ngroups; grp += gridDim.x * NW) {
     const size_t row0 = (size_t)grp * Z::RW;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const Cx<R> *src = io + c * cstr + row0 * Z::TS;
-      for (int i = lane; i < Z::RW * Z::TS; i += 32) stage[c * Z::RW * Z::TS + i] = src[i];
-    }
-    __syncwarp();
-#pragma unroll
     for (int c = 0; c < 3; ++c)
       for (int rr = 0; rr < Z::RW; ++rr)
-        wpack_c2r<R, LM>(stage + (c * Z::RW + rr) * Z::TS, buf + (c * Z::RW + rr) * Z::LS, wk);
+        wpack_c2r<R, LM>(io + c * cstr + (row0 + rr) * Z::TS, buf + c * GL + rr * Z::LS, wk);
     __syncwarp();
 #pragma unroll
-    for (int c = 0; c < 3; ++c) wfft<R, LM, -1>(buf + c * Z::RW * Z::LS, wi);
-    for (int i = lane; i < Z::RW * Z::M; i += 32) {
-      const int rr = i >> LM, n = zpos<LM>(i & (Z::M - 1));
-      const Cx<R> U1 = buf[rr * Z::LS + n], U2 = buf[(Z::RW + rr) * Z::LS + n];
-      const Cx<R> U3 = buf[(2 * Z::RW + rr) * Z::LS + n];
+    for (int c = 0; c < 3; ++c) wfft<R, LM, -1>(buf + c * GL, wi);
+    Cx<R> p4[KP];
+#pragma unroll
+    for (int jj = 0; jj < KP; ++jj) {
+      const int i = lane + 32 * jj;
+      const int rr = i >> LM, n = rr * Z::LS + zpos<LM>(i & (Z::M - 1));
+      const Cx<R> U1 = buf[n], U2 = buf[GL + n], U3 = buf[2 * GL + n];
       const R u1a = U1.x * sc, u1b = U1.y * sc, u2a = U2.x * sc, u2b = U2.y * sc, u3a = U3.x * sc, u3b = U3.y * sc;
-      buf[rr * Z::LS + n] = {u2a * u3a, u2b * u3b};
-      buf[(Z::RW + rr) * Z::LS + n] = {u3a * u1a, u3b * u1b};
-      buf[(2 * Z::RW + rr) * Z::LS + n] = {u1a * u2a, u1b * u2b};
-      buf[(3 * Z::RW + rr) * Z::LS + n] = {(u2a - u3a) * (u2a + u3a), (u2b - u3b) * (u2b + u3b)};
-      buf[(4 * Z::RW + rr) * Z::LS + n] = {(u3a - u1a) * (u3a + u1a), (u3b - u1b) * (u3b + u1b)};
+      buf[n] = {u2a * u3a, u2b * u3b};
+      buf[GL + n] = {u3a * u1a, u3b * u1b};
+      buf[2 * GL + n] = {u1a * u2a, u1b * u2b};
+      buf[3 * GL + n] = {(u2a - u3a) * (u2a + u3a), (u2b - u3b) * (u2b + u3b)};
+      p4[jj] = {(u3a - u1a) * (u3a + u1a), (u3b - u1b) * (u3b + u1b)};
     }
     __syncwarp();
 #pragma unroll
-    for (int q = 0; q < 5; ++q) wfft<R, LM, 1>(buf + q * Z::RW * Z::LS, wf);
+    for (int q = 0; q < 4; ++q) wfft<R, LM, 1>(buf + q * GL, wf);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) {
+    for (int q = 0; q < 4; ++q) {
       Cx<R> *dst = io + q * cstr + row0 * Z::TS;
       for (int i = lane; i < Z::RW * Z::TZ; i += 32) {
-        const int rr = i / Z::TZ, k = i - rr * Z::TZ;
-        dst[rr * Z::TS + k] = wunpack_r2c<R, LM>(buf + (q * Z::RW + rr) * Z::LS, k, tw.z);
+        const int rr = i / Z::TZ, kk = i - rr * Z::TZ;
+        dst[rr * Z::TS + kk] = wunpack_r2c<R, LM>(buf + q * GL + rr * Z::LS, kk, tw.z);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int jj = 0; jj < KP; ++jj) {
+      const int i = lane + 32 * jj;
+      buf[(i >> LM) * Z::LS + zpos<LM>(i & (Z::M - 1))] = p4[jj];
+    }
+    __syncwarp();
+    wfft<R, LM, 1>(buf, wf);
+    {
+      Cx<R> *dst = io + 4 * cstr + row0 * Z::TS;
+      for (int i = lane; i < Z::RW * Z::TZ; i += 32) {
+        const int rr = i / Z::TZ, kk = i - rr * Z::TZ;
+        dst[rr * Z::TS + kk] = wunpack_r2c<R, LM>(buf + rr * Z::LS, kk, tw.z);
       }
     }
     __syncwarp();
@@ -434,9 +447,10 @@ __global__ void __launch_bounds__(NW * 32) k_zw_force(Geo g, Twiddles<R> tw, R *
 // ---------------------------------------------------------------------------
 // y pass with compile-time NY = 2^LY (as k_y_pass).  A work item is RW
 // consecutive kz columns of one (component, x) plane; each warp of a
-// persistent grid walks its items with two shared-memory slots: while it
-// transforms item k from one slot, cp.async brings item k+1 into the other,
-// so the global-memory latency of the gather overlaps the transform.  The
+// persistent grid walks its items.  NSLOT = 2 (FP64): two shared-memory
+// slots, and while the warp transforms item k from one, cp.async brings item
+// k+1 into the other.  NSLOT = 1 (FP32): one slot, half the footprint and so
+// twice the resident warps, which hide the gather latency better.  The
 // gather lands each element straight at its padded-line position.  FULLY:
 // the retained box spans every ky (the untruncated half spectrum).
 //   inverse: in [c][NX][KYc][TS] -> out [c][NX][NY][TS]
@@ -469,15 +483,16 @@ __device__ __forceinline__ void yw_issue(const Geo &g, const Cx<R> *__restrict__
     }
 }
 
-template <typename R, bool INVERSE, int LY, bool FULLY, int NW>
+template <typename R, bool INVERSE, int LY, bool FULLY, int NW, int NSLOT>
 __global__ void __launch_bounds__(NW * 32) k_yw_pass(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
                                                      Cx<R> *__restrict__ out, int ncomp) {
   using Y = ZL<LY>;
   constexpr int RW = Y::RW, NY = Y::M, SLOT = RW * Y::LS;
+  static_assert(NSLOT == 1 || NSLOT == 2, "slots");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_begin();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  Cx<R> *slots = reinterpret_cast<Cx<R> *>(smem_raw) + (size_t)warp * 2 * SLOT;
+  Cx<R> *slots = reinterpret_cast<Cx<R> *>(smem_raw) + (size_t)warp * NSLOT * SLOT;
   const int nbatch = (g.TZ + RW - 1) / RW;
   const int nitems = ncomp * g.NX * nbatch;
   const int rows_out = INVERSE ? NY : g.KYc;
@@ -485,13 +500,20 @@ __global__ void __launch_bounds__(NW * 32) k_yw_pass(Geo g, Twiddles<R> tw, cons
   wfft_twiddles<R, LY, INVERSE ? -1 : 1>(tw.y, w);
   const int stride = gridDim.x * NW;
   int item = blockIdx.x * NW + warp;
-  if (item < nitems) yw_issue<R, INVERSE, LY, FULLY>(g, in, slots, item, nbatch);
+  if (NSLOT == 2 && item < nitems) yw_issue<R, INVERSE, LY, FULLY>(g, in, slots, item, nbatch);
   cp_async_commit();
   for (int k = 0; item < nitems; ++k, item += stride) {
-    Cx<R> *cur = slots + (k & 1) * SLOT;
-    if (item + stride < nitems) yw_issue<R, INVERSE, LY, FULLY>(g, in, slots + ((k + 1) & 1) * SLOT, item + stride, nbatch);
-    cp_async_commit();
-    cp_async_wait_group<1>();
+    Cx<R> *cur = slots + (NSLOT == 2 ? (k & 1) * SLOT : 0);
+    if (NSLOT == 2) {
+      if (item + stride < nitems)
+        yw_issue<R, INVERSE, LY, FULLY>(g, in, slots + ((k + 1) & 1) * SLOT, item + stride, nbatch);
+      cp_async_commit();
+      cp_async_wait_group<1>();
+    } else {
+      yw_issue<R, INVERSE, LY, FULLY>(g, in, slots, item, nbatch);
+      cp_async_commit();
+      cp_async_wait_all();
+    }
     __syncwarp();
     wfft<R, LY, INVERSE ? -1 : 1>(cur, w);
     const int batch = item % nbatch, plane = item / nbatch;
