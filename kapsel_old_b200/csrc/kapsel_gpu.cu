@@ -329,7 +329,7 @@ struct Box : BoxBase {
     const size_t line = sizeof(Cx<R>) * Z::RW * Z::LS * ZNW;
     // FP64: the prefetching products kernel; FP32: four line groups per warp
     zw_sm_p = sizeof(R) == 8 ? sizeof(Cx<R>) * (size_t)ZProd<R, LM>::WARP * ZNW : 4 * line;
-    zw_sm_c = 2 * line;
+    zw_sm_c = line;
     zw_sm_f = 3 * line;
     auto kp = sizeof(R) == 8 ? k_zw_products_pf<R, LM, ZNW> : k_zw_products<R, LM, ZNW>;
     KCHECK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_p));

@@ -89,7 +89,7 @@ __device__ __forceinline__ void wfft(Cx<R> *buf, const Cx<R> (&w)[ZL<LM>::N1]) {
   __syncwarp();
 }
 
-// c2r packing of one line of A[k], k < TZ (stride-1 staging) into the padded
+// c2r packing of one line of A[k], k < TZ (stride 1, shared or global) into the padded
 // line Z: Z[k] = (A[k] + conj A[M-k]) + i (A[k] - conj A[M-k]) w_NZ^{-k}.
 // wk[j] = w_NZ^{-k} for this lane's k = lane + 32 j.
 template <typename R, int LM>
@@ -331,8 +331,9 @@ __global__ void __launch_bounds__(NW * 32) k_zw_c2r(Geo g, Twiddles<R> tw, const
     return;
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  Cx<R> *buf = reinterpret_cast<Cx<R> *>(smem_raw) + (size_t)warp * 2 * Z::RW * Z::LS;
-  Cx<R> *stage = buf + Z::RW * Z::LS;
+  // one line group per warp: the packing reads the rows straight from global
+  // memory, and the small footprint keeps more warps resident
+  Cx<R> *buf = reinterpret_cast<Cx<R> *>(smem_raw) + (size_t)warp * Z::RW * Z::LS;
   Cx<R> wi[Z::N1], wk[Z::KW];
   wfft_twiddles<R, LM, -1>(tw.m, wi);
   wpre_twiddles<R, LM>(tw.z, wk);
@@ -343,9 +344,7 @@ __global__ void __launch_bounds__(NW * 32) k_zw_c2r(Geo g, Twiddles<R> tw, const
     const int c = task / ngroups;
     const size_t row0 = (size_t)(task - c * ngroups) * Z::RW;
     const Cx<R> *src = in + c * rows * Z::TS + row0 * Z::TS;
-    for (int i = lane; i < Z::RW * Z::TS; i += 32) stage[i] = src[i];
-    __syncwarp();
-    for (int rr = 0; rr < Z::RW; ++rr) wpack_c2r<R, LM>(stage + rr * Z::TS, buf + rr * Z::LS, wk);
+    for (int rr = 0; rr < Z::RW; ++rr) wpack_c2r<R, LM>(src + rr * Z::TS, buf + rr * Z::LS, wk);
     __syncwarp();
     wfft<R, LM, -1>(buf, wi);
     R *dst = out + c * out_cstride + row0 * (size_t)out_pitch;
