@@ -259,7 +259,7 @@ struct Box : BoxBase {
   R *phiup = nullptr;     // [4][NX][NY][NZ]
   Cx<R> *twbuf = nullptr;
   Twiddles<R> tw;
-  static constexpr int KCX = sizeof(R) == 4 ? 4 : 4;    // x-pass kz tile
+  static constexpr int KCX = 4;                         // x-pass kz tile
   static constexpr int KCY = sizeof(R) == 4 ? 32 : 16;  // y-pass kz tile
   size_t smem_xu = 0, smem_xadv = 0, smem_xf = 0, smem_y = 0, smem_zp = 0, smem_zc = 0, smem_zf = 0, smem_zr = 0;
 
