@@ -34,7 +34,6 @@ struct ZL {
   static constexpr int KW = M / 32;                          // k values per lane in pre/post
   static constexpr int LR = L2 > 5 ? 0 : 5 - L2;             // log2(RW)
   static_assert(LM >= 5 && LM <= 8, "line length");
-  static_assert(LM == 8 || 2 * LS >= 3 * TS, "staging fits in two line groups");
 };
 
 template <int LM>
