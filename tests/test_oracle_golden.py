@@ -90,3 +90,24 @@ def test_oracle_solenoidal_idempotent():
     assert rel(b, a) < 1e-13
     div = sum(k * S.fwd(a[d]) for d, k in enumerate((S.kx, S.ky, S.kz)))
     assert np.abs(div).max() < 1e-10 * np.abs(S.fwd(a[0])).max()
+
+
+def test_oracle_phi_volume():
+    """The integral of the smoothed profile over the grid against the sphere
+    volume 4/3 pi a^3 (the mass factor the reference uses,
+    md_force.cxx:334-336): the smooth interface of width xi adds a
+    second-order term, measured 1 + 0.066 (xi/a)^2 for a = 4, 5, 6."""
+    from oracle import udf
+
+    rng = np.random.default_rng(0)
+    excess = []
+    for a in (4.0, 5.0, 6.0):
+        o = spm.SpmOracle(udf.ns_config((5, 5, 5), 1, seed=3, a=a, a_xi=2.0))
+        V = 4.0 / 3.0 * np.pi * a ** 3
+        for _ in range(3):
+            x = np.array([[16.0, 16.0, 16.0]]) + rng.random((1, 3))
+            phi, _ = o.phi_up(x, np.zeros((1, 3)), np.zeros((1, 3)))
+            e = phi.sum() / V - 1.0
+            assert 0.0 < e < 0.1 * (2.0 / a) ** 2, (a, e)
+        excess.append(e)
+    assert excess[0] > excess[1] > excess[2]
