@@ -177,6 +177,9 @@ struct BoxBase {
   double time = 0.0;
   bool initialised = false;
   bool particles_set = false;
+  // bufA holds u_k of the current zeta / uk_dc, left there by the fused last
+  // launch of a Navier-Stokes step; the next step then skips its first launch
+  bool u_spec_ready = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   // learned near-contact correction (off unless a network is attached)
   const kapsel_nc *nc = nullptr;
@@ -202,6 +205,10 @@ struct BoxBase {
   virtual int conc_from_host(const double *c) = 0;
   virtual void launch_step(const double *noise, int euler, cudaEvent_t *ev = nullptr) = 0;
   virtual void launch_init() = 0;
+  // launch the first x pass if bufA does not hold u_k (before a step or a
+  // graph replay); true when the step will leave u_k in bufA again
+  virtual void ensure_u_spec() = 0;
+  virtual bool ends_with_u_spec() const = 0;
   virtual int velocity_to_host(double *u) = 0;
   virtual int zeta_to_host(double *z) = 0;
   virtual int zeta_from_host(const double *z) = 0;
@@ -274,6 +281,8 @@ struct Box : BoxBase {
     KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX, 1, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_xadv));
     KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xf));
+    KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX, LX, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_xf));
     return 0;
   }
   template <int LX>
@@ -284,9 +293,9 @@ struct Box : BoxBase {
   void xa_l(bool pdl) {
     launch_k(pdl, k_x_advect_update<R, KCX, EU, LX>, gx(), dim3(256), smem_xadv, stream, g, tw, bufA, zeta, uk_dc);
   }
-  template <int LX>
-  void xf_l(bool pdl, const Cx<R> *in) {
-    launch_k(pdl, k_x_force_to_zeta<R, KCX, LX>, gx(), dim3(256), smem_xf, stream, g, tw, in, zeta, uk_dc);
+  template <int LX, int NEXTU = 0>
+  void xf_l(bool pdl, Cx<R> *in) {
+    launch_k(pdl, k_x_force_to_zeta<R, KCX, LX, NEXTU>, gx(), dim3(256), smem_xf, stream, g, tw, in, zeta, uk_dc);
   }
   void x_zeta(bool pdl, const Cx<R> *z, const double *u, Cx<R> *out) {
     switch (g.NX) {
@@ -307,13 +316,24 @@ struct Box : BoxBase {
       default: xa_l<EU, 0>(pdl);
     }
   }
-  void x_force(bool pdl, const Cx<R> *in) {
+  void x_force(bool pdl, Cx<R> *in) {
     switch (g.NX) {
       case 32: xf_l<5>(pdl, in); return;
       case 64: xf_l<6>(pdl, in); return;
       case 128: xf_l<7>(pdl, in); return;
       case 256: xf_l<8>(pdl, in); return;
       default: xf_l<0>(pdl, in);
+    }
+  }
+  // the same, followed on each tile by the next step's first x pass (u_k of
+  // the updated zeta into bufA)
+  void x_force_next(bool pdl) {
+    switch (g.NX) {
+      case 32: xf_l<5, 1>(pdl, bufA); return;
+      case 64: xf_l<6, 1>(pdl, bufA); return;
+      case 128: xf_l<7, 1>(pdl, bufA); return;
+      case 256: xf_l<8, 1>(pdl, bufA); return;
+      default: xf_l<0, 1>(pdl, bufA);
     }
   }
 
@@ -453,6 +473,8 @@ struct Box : BoxBase {
     KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
     KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xadv));
     KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xf));
+    KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_xf));
     KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
     KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
     KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
@@ -574,8 +596,11 @@ struct Box : BoxBase {
     };
     const bool pdl = use_pdl && !ev;  // events between launches break the programmatic chain
     const Cx<R> *czeta = zeta;
+    // the fused path starts at the y pass: the previous step's last launch
+    // (or ensure_u_spec) left u_k in bufA; profiling times every launch
+    const bool fused = ends_with_u_spec() && !ev;
     mark();
-    x_zeta(false, czeta, (const double *)uk_dc, bufA);
+    if (!fused) x_zeta(false, czeta, (const double *)uk_dc, bufA);
     mark();
     launch_y<true>(g, 3, bufA, bufB, pdl);
     mark();
@@ -607,10 +632,20 @@ struct Box : BoxBase {
       mark();
       launch_y<false>(g, 3, bufB, bufA, pdl);
       mark();
-      x_force(pdl, (const Cx<R> *)bufA);
+      if (fused)
+        x_force_next(pdl);
+      else
+        x_force(pdl, bufA);
       mark();
     }
   }
+
+  void ensure_u_spec() override {
+    if (!ends_with_u_spec() || u_spec_ready) return;
+    x_zeta(false, zeta, uk_dc, bufA);
+    u_spec_ready = true;
+  }
+  bool ends_with_u_spec() const override { return prm.eq == KAPSEL_EQ_NAVIER_STOKES && Np > 0; }
 
   void launch_init() override {
     // Init_zeta_k gives zeta = 0 and u = 0 (init_fluid.cxx:10-26); the
@@ -1012,6 +1047,7 @@ struct Box : BoxBase {
   }
 
   int zeta_from_host(const double *z) override {
+    u_spec_ready = false;
     const size_t nz = (size_t)g.KXc * g.KYc * g.TS;
     std::vector<Cx<R>> h(2 * nz);
     const int NZ_ = g.NZ + 2;
@@ -1742,6 +1778,7 @@ int kapsel_gpu_init_state(kapsel_ctx *ctx) {
   b->ts = 0;
   b->time = 0.0;
   b->drop_prefill();
+  b->u_spec_ready = false;
   b->initialised = true;
   return 0;
 }
@@ -1763,6 +1800,7 @@ static int step_impl(kapsel_ctx *ctx, int n, bool use_graph) {
     const int slot = b->ts & 1;
     int rc = b->take_noise(slot);
     if (rc) return rc;
+    b->ensure_u_spec();
     const int euler = b->ts == 0 ? 1 : 0;
     if (use_graph && !euler) {
       if (!b->graph[slot]) {
@@ -1777,6 +1815,7 @@ static int step_impl(kapsel_ctx *ctx, int n, bool use_graph) {
     } else {
       b->launch_step(b->noise_dev[slot], euler);
     }
+    b->u_spec_ready = b->ends_with_u_spec();
     b->ts += 1;
     b->time += b->prm.dt;
     if ((rc = b->prefill_noise())) return rc;
@@ -2066,6 +2105,7 @@ int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms) {
     if (cudaEventCreate(&ev[i]) != cudaSuccess) return KAPSEL_ECUDA;
   k_time_gate<<<1, 32, 0, b->stream>>>(2000000ull);  // 2 ms
   b->launch_step(b->noise_dev[slot], b->ts == 0 ? 1 : 0, ev);
+  b->u_spec_ready = false;
   b->ts += 1;
   b->time += b->prm.dt;
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
@@ -2157,6 +2197,7 @@ int kapsel_batch_step(kapsel_batch *b, int nsteps) {
       BoxBase *x = b->boxes[i]->box.get();
       int rc = x->take_noise(slot);
       if (rc) return rc;
+      x->ensure_u_spec();  // on the box's stream, before the graph's ready events
     }
     if (euler) {
       for (int i = 0; i < n; ++i) {
@@ -2192,6 +2233,7 @@ int kapsel_batch_step(kapsel_batch *b, int nsteps) {
     }
     for (int i = 0; i < n; ++i) {
       BoxBase *x = b->boxes[i]->box.get();
+      x->u_spec_ready = x->ends_with_u_spec();
       x->ts += 1;
       x->time += x->prm.dt;
     }

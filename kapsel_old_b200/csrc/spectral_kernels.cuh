@@ -596,8 +596,12 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
 // The velocity before the force is Zeta_k2u of the truncated zeta, so its
 // own U2zeta_k is that zeta again (linearity; parity up to roundoff).
 // in buf [3][NX][KYc][TZ].  grid (KYc, ceil(TZ/KC)).
-template <typename R, int KC, int LX = 0>
-__global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ buf,
+// NEXTU = 1 also does the first launch of the next step on the same tile:
+// u_k = Zeta_k2u_k(zeta, uk_dc) of the updated values and the inverse x
+// transform, written over buf (as k_x_zeta_to_u writes it, with the same
+// arithmetic), so the next step starts at its y pass.
+template <typename R, int KC, int LX = 0, int NEXTU = 0>
+__global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ buf,
                                                          Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_begin();
@@ -607,6 +611,7 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
   Cx<R> *Zs = twx + NXv;          // [2][KXc][KC]
   Cx<R> *Pb = Zs + 2 * g.KXc * KC;  // [NX][3*KC]
   Cx<R> *scr = Pb + NXv * W3;       // FFT scratch
+  __shared__ double ukn[3];         // uk_dc after the update (NEXTU)
   const int iy = blockIdx.x;
   const int kz0 = blockIdx.y * KC;
   const int ncol = min(KC, g.TZ - kz0);
@@ -643,6 +648,8 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
       uk_dc[0] += (double)f0.x;
       uk_dc[1] += (double)f1.x;
       uk_dc[2] += (double)f2.x;
+      if (NEXTU)
+        for (int d = 0; d < 3; ++d) ukn[d] = uk_dc[d];
       continue;  // zeta(k=0) stays 0
     }
     const R K2 = kx * kx + ky * ky + kzr * kzr;
@@ -659,8 +666,45 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
     Cx<R> z0, z1;
     select_zeta(KXi, KYi, w, z0, z1);
     const size_t o = ((size_t)ix * g.KYc + iy) * g.TS + kz;
-    zeta[o] = cadd(Zs[ix * KC + col], z0);
-    zeta[zplane + o] = cadd(Zs[(g.KXc + ix) * KC + col], z1);
+    z0 = cadd(Zs[ix * KC + col], z0);
+    z1 = cadd(Zs[(g.KXc + ix) * KC + col], z1);
+    zeta[o] = z0;
+    zeta[zplane + o] = z1;
+    if (NEXTU) {
+      Zs[ix * KC + col] = z0;
+      Zs[(g.KXc + ix) * KC + col] = z1;
+    }
+  }
+  if (!NEXTU) return;
+  __syncthreads();
+  // the next step's k_x_zeta_to_u on this tile, from the updated Zs / ukn
+  for (int it = threadIdx.x; it < NXv * KC; it += blockDim.x) {
+    const int col = it % KC, i = it / KC;
+    Cx<R> u[3] = {{R(0), R(0)}, {R(0), R(0)}, {R(0), R(0)}};
+    const int KXi = signed_k(i, NXv);
+    if (col < ncol && abs(KXi) < g.TX) {
+      const int ix = KXi >= 0 ? KXi : KXi + g.KXc;
+      const int kz = kz0 + col;
+      const Cx<R> z0 = Zs[ix * KC + col], z1 = Zs[(g.KXc + ix) * KC + col];
+      const R kx = R(g.wave[0] * KXi), kzr = R(g.wave[2] * kz);
+      const R k2 = kx * kx + ky * ky + kzr * kzr;
+      const R ik2 = k2 > R(0) ? R(1) / k2 : R(0);
+      zeta_to_u(KXi, KYi, kx, ky, kzr, ik2, z0, z1, u);
+      if (KXi == 0 && KYi == 0 && kz == 0) {
+        u[0] = {R(ukn[0]), R(0)};
+        u[1] = {R(ukn[1]), R(0)};
+        u[2] = {R(ukn[2]), R(0)};
+      }
+    }
+    Pb[i * W3 + col] = u[0];
+    Pb[i * W3 + KC + col] = u[1];
+    Pb[i * W3 + 2 * KC + col] = u[2];
+  }
+  __syncthreads();
+  fft2_smem<R, -1, W3, LX>(Pb, scr, LXv, 1, W3, twx);
+  for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
+    const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
+    if (col < ncol) buf[(((size_t)c * NXv + x) * g.KYc + iy) * g.TS + kz0 + col] = Pb[x * W3 + c * KC + col];
   }
 }
 
