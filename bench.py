@@ -99,8 +99,8 @@ def sekibun_count(cfg):
 
 def step_bytes_model(cfg, R: int):
     """Compulsory bytes of one step: 40.6 field passes of N*R at 128^3 with
-    256 spheres (stage table in DESIGN.md: 5+7+5 spectral, 0.71 gather,
-    4 phi/up reset, 1.89 scatter, 10 force, 7 zeta update)."""
+    256 spheres (stages: 5+7+5 spectral, 0.71 gather, 4 phi/up reset,
+    1.89 scatter, 10 force, 7 zeta update)."""
     NX, NY, NZ = [1 << p for p in cfg["np_xyz"]]
     N = NX * NY * NZ
     Np = len(cfg["particles"])
@@ -227,6 +227,9 @@ def run_ours(args, rank, world, local_rank):
     # ---- FP64 path, same workload
     sim_d, _, ms_d = timed(kg.FP64, args.steps, args.warmup)
     sim_d.close()
+    # ---- mixed-precision error of the headline configuration over its full
+    # run, against the FP64 GPU path (which the tests pin to the reference)
+    parity = parity_curve(kg, cfg, args.parity_steps) if args.parity_steps > 0 else None
 
     # ---- per-kernel durations (CUDA events between launches on the library stream)
     nker = kg.load_library().kapsel_gpu_launches_per_step(sim_m.h)
@@ -364,6 +367,7 @@ def run_ours(args, rank, world, local_rank):
             extra["shear_le_128cubed_256"]["cpu_baseline"] = cpu_baseline(c6, warmup=1, steps=8)
 
     steps_total = args.steps * world
+    traffic = ncu_traffic(top_name)
     value = replica_value(args.steps, world, ms_m * 1e-3)
     fp64_value = replica_value(args.steps, world, ms_d * 1e-3)
     bstep, passes = step_bytes_model(cfg, 4)
@@ -391,10 +395,13 @@ def run_ours(args, rank, world, local_rank):
         },
         "fp64": {"value": round(fp64_value, 3), "ms_per_step": round(ms_d / args.steps, 5),
                  "mixed_over_fp64": round(value / fp64_value, 3)},
+        "fp64_value": round(fp64_value, 3),
+        "mixed_over_fp64": round(value / fp64_value, 3),
+        "parity": parity,
         "roofline": {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "algorithmic_bytes_per_launch": kb[top_name], "avg_launch_ms": round(float(acc[top]), 5),
-                     "traffic": ncu_traffic(top_name)},
+                     "traffic": traffic[0], "traffic_source": traffic[1]},
         "step_roofline": {"bytes_per_step_model": int(bstep), "field_passes": round(passes, 2),
                           "achieved_gbs": round(bstep / (ms_m / args.steps * 1e-3) / 1e9, 1),
                           "frac": round(bstep / (ms_m / args.steps * 1e-3) / 1e9 / hbm, 4)},
@@ -412,18 +419,52 @@ def run_ours(args, rank, world, local_rank):
 
 # ---------------------------------------------------------------------------
 def ncu_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary
-    (profiles/<kernel without the leading k_>_*.md, line `traffic_bytes_per_launch`), or None."""
+    """DRAM bytes per launch of `kernel` as an ncu capture recorded them in the
+    committed summary (profiles/<kernel without the leading k_>_*.md, line
+    `traffic_bytes_per_launch`), with the summary's name and the build it was
+    captured on (line `captured_at`): (bytes, source) or (None, None).  The
+    figure is not measured by this run."""
     import glob
     import re
 
     stem = kernel[2:] if kernel.startswith("k_") else kernel
     here = os.path.dirname(os.path.abspath(__file__))
     for f in sorted(glob.glob(os.path.join(here, "profiles", f"k_*{stem.replace('z_', 'z*_')}*.md"))):
-        m = re.search(r"\|\s*traffic_bytes_per_launch\s*\|\s*([0-9]+)\s*\|", open(f).read())
+        text = open(f).read()
+        m = re.search(r"\|\s*traffic_bytes_per_launch\s*\|\s*([0-9]+)\s*\|", text)
         if m:
-            return int(m.group(1))
-    return None
+            at = re.search(r"captured_at:\s*(\S+)", text)
+            src = "ncu capture in " + os.path.relpath(f, here) + (f" (build {at.group(1)})" if at else "")
+            return int(m.group(1)), src
+    return None, None
+
+
+def parity_curve(kg, cfg, steps: int, points=(1, 10, 100, 250, 500, 1000, 1500, 2000)):
+    """Mixed-precision state against the FP64 GPU path from the same initial
+    state, both replayed from CUDA graphs: velocity-field relative L2,
+    particle velocity relative L2 and the largest position difference at
+    checkpoints up to `steps`."""
+    import numpy as np
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    a = kg.Simulation(cfg, precision=kg.FP64)
+    b = kg.Simulation(cfg, precision=kg.MIXED)
+    curve, done = [], 0
+    for at in [p for p in points if p <= steps] + ([steps] if steps not in points else []):
+        a.step(at - done, graph=True)
+        b.step(at - done, graph=True)
+        done = at
+        pa, pb = a.particles(), b.particles()
+        curve.append({"step": at, "u_rel_l2": rel(b.velocity(), a.velocity()), "v_rel_l2": rel(pb["v"], pa["v"]),
+                      "x_max_abs": float(np.abs(pb["x_nopbc"] - pa["x_nopbc"]).max())})
+    a.close()
+    b.close()
+    return {"mixed_u_rel_l2": curve[-1]["u_rel_l2"], "mixed_v_rel_l2": curve[-1]["v_rel_l2"],
+            "mixed_x_max_abs": curve[-1]["x_max_abs"], "steps": steps,
+            "against": "FP64 GPU step from the same state (FP64 pinned to the reference <= 1e-10)",
+            "curve": curve}
 
 
 def cpu_baseline(cfg, warmup: int, steps: int, threads: int | None = None):
@@ -504,6 +545,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 64^3 FP64 and electrolyte workloads")
+    ap.add_argument("--parity-steps", type=int, default=2000,
+                    help="steps of the mixed-vs-FP64 error curve (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))

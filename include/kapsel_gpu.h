@@ -233,8 +233,12 @@ int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr);
    with that device current); make that first call before any stream
    capture.  All calls share the one array, so calls that overlap on the GPU
    (different streams or threads at the same time) race; serialise them.
-   The call is asynchronous on `stream`.  No counterpart in the reference:
-   it is an addition of this library. */
+   The call is asynchronous on `stream`: its status covers the arguments
+   and the launch configuration only (a fault while the kernels run shows
+   up at the caller's next synchronising call), and it returns
+   KAPSEL_ECUDA without launching anything when an earlier CUDA error is
+   still pending on the calling thread (that error is left in place).  No
+   counterpart in the reference: it is an addition of this library. */
 int kapsel_gpu_solenoidal_u_noalloc(const int *np_xyz, double dx, const double *u0, const double *u1,
                                     const double *u2, double *o0, double *o1, double *o2, void *stream);
 

@@ -129,7 +129,8 @@ std::vector<int> sekibun(double A, double A_XI, double DX) {
 
 template <typename R, bool INVERSE>
 __global__ void k_col_pass(Geo g, const Cx<R> *twn, int logn, int n, const Cx<R> *in, Cx<R> *out,
-                           long long line_stride, long long elem_stride, int nlines);
+                           long long line_stride, long long elem_stride, int nlines, int lines_per_plane,
+                           long long plane_stride);
 template <typename R>
 __global__ void k_z_c2r_full(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in, R *__restrict__ out, double scale);
 
@@ -562,6 +563,8 @@ struct Box : BoxBase {
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     ytile_small = keep;
+    // the timed passes wrote bufA: it no longer holds u_k of the current zeta
+    u_spec_ready = false;
     return ms / reps;
   }
   void set_ytile(int small) override { ytile_small = small; }
@@ -1126,24 +1129,30 @@ void unpack_real(double *a, const R *h, const Geo &g) {
 template <typename R, bool INVERSE>
 __global__ void k_col_pass(Geo g, const Cx<R> *twn, int logn, int n, const Cx<R> *in,
                                                   Cx<R> *out,
-                                                  long long line_stride, long long elem_stride, int nlines) {
-  // generic batched FFT over lines: element e of line l at l*line_stride + e*elem_stride
+                                                  long long line_stride, long long elem_stride, int nlines,
+                                                  int lines_per_plane, long long plane_stride) {
+  // generic batched FFT over lines: line l = p*lines_per_plane + q starts at
+  // p*plane_stride + q*line_stride, element e at + e*elem_stride
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<R> *tws = reinterpret_cast<Cx<R> *>(smem_raw);
   Cx<R> *B = tws + n;  // [n][16]
   load_twiddles(tws, twn, n);
   const int l0 = blockIdx.x * 16;
+  auto line_base = [&](int l) {
+    const int p = l / lines_per_plane, q = l - p * lines_per_plane;
+    return (long long)p * plane_stride + (long long)q * line_stride;
+  };
   for (int it = threadIdx.x; it < n * 16; it += blockDim.x) {
     const int col = it % 16, e = it / 16;
     Cx<R> v = {R(0), R(0)};
-    if (l0 + col < nlines) v = in[(long long)(l0 + col) * line_stride + (long long)e * elem_stride];
+    if (l0 + col < nlines) v = in[line_base(l0 + col) + (long long)e * elem_stride];
     B[bitrev(e, logn) * 16 + col] = v;
   }
   __syncthreads();
   fft_inplace(B, logn, 16, 1, 16, tws, INVERSE ? -1 : 1);
   for (int it = threadIdx.x; it < n * 16; it += blockDim.x) {
     const int col = it % 16, e = it / 16;
-    if (l0 + col < nlines) out[(long long)(l0 + col) * line_stride + (long long)e * elem_stride] = B[e * 16 + col];
+    if (l0 + col < nlines) out[line_base(l0 + col) + (long long)e * elem_stride] = B[e * 16 + col];
   }
 }
 
@@ -1202,27 +1211,17 @@ struct FullFFT {
     const Geo &g = b.g;
     const int M1 = g.M + 1;
     const size_t sm = sizeof(Cx<R>) * (n + (size_t)n * 16);
-    if (axis == 0) {
-      const int nlines = g.NY * M1;
-      // lines are contiguous (l = y*M1 + kz), element stride NY*M1
-      if (inv)
-        k_col_pass<R, true><<<(nlines + 15) / 16, 256, sm, b.stream>>>(g, twn, logn, n, data, data, 1,
-                                                                         (long long)g.NY * M1, nlines);
-      else
-        k_col_pass<R, false><<<(nlines + 15) / 16, 256, sm, b.stream>>>(g, twn, logn, n, data, data, 1,
-                                                                          (long long)g.NY * M1, nlines);
-    } else {
-      // per x: lines kz (contiguous), element stride M1; run NX launches' worth
-      // as one launch by treating (x, kz) lines with a 2-level index: use a
-      // launch per x (small sizes only on this routine-level path).
-      for (int x = 0; x < g.NX; ++x) {
-        Cx<R> *base = data + (size_t)x * g.NY * M1;
-        if (inv)
-          k_col_pass<R, true><<<(M1 + 15) / 16, 256, sm, b.stream>>>(g, twn, logn, n, base, base, 1, M1, M1);
-        else
-          k_col_pass<R, false><<<(M1 + 15) / 16, 256, sm, b.stream>>>(g, twn, logn, n, base, base, 1, M1, M1);
-      }
-    }
+    // axis 0: lines are contiguous (l = y*M1 + kz), element stride NY*M1;
+    // axis 1: lines (x, kz), kz contiguous within the x-plane, element stride M1
+    const int nlines = axis == 0 ? g.NY * M1 : g.NX * M1;
+    const int lpp = axis == 0 ? nlines : M1;
+    const long long es = axis == 0 ? (long long)g.NY * M1 : M1, ps = axis == 0 ? 0 : (long long)g.NY * M1;
+    if (inv)
+      k_col_pass<R, true><<<(nlines + 15) / 16, 256, sm, b.stream>>>(g, twn, logn, n, data, data, 1, es, nlines,
+                                                                       lpp, ps);
+    else
+      k_col_pass<R, false><<<(nlines + 15) / 16, 256, sm, b.stream>>>(g, twn, logn, n, data, data, 1, es, nlines,
+                                                                        lpp, ps);
   }
 };
 
@@ -2371,6 +2370,9 @@ extern "C" int kapsel_gpu_solenoidal_u_noalloc(const int *np_xyz, double dx, con
   g.wave[1] = 2.0 * M_PI / (g.NY * dx);
   g.wave[2] = 2.0 * M_PI / (g.NZ * dx);
   g.inv_n = 1.0 / ((double)g.NX * g.NY * g.NZ);
+  // an error left on this thread by earlier, unrelated work is not this
+  // call's: report it without launching anything and leave it for its owner
+  if (cudaPeekAtLastError() != cudaSuccess) return KAPSEL_ECUDA;
   void *base = nullptr;
   int rc = noalloc_scratch(&base);
   if (rc) return rc;
@@ -2394,23 +2396,15 @@ extern "C" int kapsel_gpu_solenoidal_u_noalloc(const int *np_xyz, double dx, con
     const int logn = axis == 0 ? g.lx : g.ly;
     const Cx<double> *twn = axis == 0 ? tw.x : tw.y;
     const size_t sm = sizeof(Cx<double>) * (n + (size_t)n * 16);
-    if (axis == 0) {
-      const int nl = g.NY * M1;
-      if (inv)
-        k_col_pass<double, true><<<(nl + 15) / 16, 256, sm, s>>>(g, twn, logn, n, data, data, 1,
-                                                                  (long long)g.NY * M1, nl);
-      else
-        k_col_pass<double, false><<<(nl + 15) / 16, 256, sm, s>>>(g, twn, logn, n, data, data, 1,
-                                                                   (long long)g.NY * M1, nl);
-    } else {
-      for (int x = 0; x < g.NX; ++x) {
-        Cx<double> *b = data + (size_t)x * g.NY * M1;
-        if (inv)
-          k_col_pass<double, true><<<(M1 + 15) / 16, 256, sm, s>>>(g, twn, logn, n, b, b, 1, M1, M1);
-        else
-          k_col_pass<double, false><<<(M1 + 15) / 16, 256, sm, s>>>(g, twn, logn, n, b, b, 1, M1, M1);
-      }
-    }
+    // axis 0 (x): lines (y, kz) contiguous, element stride NY*M1; axis 1 (y):
+    // lines (x, kz), kz contiguous within each x-plane, element stride M1
+    const int nl = axis == 0 ? g.NY * M1 : g.NX * M1;
+    const int lpp = axis == 0 ? nl : M1;
+    const long long es = axis == 0 ? (long long)g.NY * M1 : M1, ps = axis == 0 ? 0 : (long long)g.NY * M1;
+    if (inv)
+      k_col_pass<double, true><<<(nl + 15) / 16, 256, sm, s>>>(g, twn, logn, n, data, data, 1, es, nl, lpp, ps);
+    else
+      k_col_pass<double, false><<<(nl + 15) / 16, 256, sm, s>>>(g, twn, logn, n, data, data, 1, es, nl, lpp, ps);
   };
   const double *in[3] = {u0, u1, u2};
   double *out[3] = {o0, o1, o2};

@@ -57,3 +57,25 @@ def test_batch_msd():
         assert abs(msd[i] - np.mean(np.sum(d * d, axis=1))) <= 1e-12 * max(msd[i], 1e-300)
     assert np.all(msd > 0)
     b.close()
+
+
+def test_batch_autotune_after_stepping_matches_single_boxes():
+    """Boxes stepped on their own before the batch is built: the autotuner's
+    timing passes overwrite the spectrum buffer that a stepped box keeps for
+    its next step, which must then be recomputed, not reused."""
+    import kapsel_old_b200 as kg
+
+    cfgs = _cfgs()
+    batch_sims = [kg.Simulation(c, precision=kg.FP64) for c in cfgs]
+    solo = [kg.Simulation(c, precision=kg.FP64) for c in cfgs]
+    for s in batch_sims + solo:
+        s.step(3)
+    b = kg.Batch(batch_sims, autotune=True)
+    b.step(4)
+    for s in solo:
+        s.step(4)
+    for bs, ss in zip(batch_sims, solo):
+        assert bs.time()[0] == ss.time()[0] == 7
+        assert rel(bs.zeta(), ss.zeta()) < 1e-12
+        assert rel(bs.particles()["v"], ss.particles()["v"]) < 1e-12
+    b.close()

@@ -12,7 +12,21 @@ import subprocess
 import numpy as np
 import pytest
 
-REF = "/root/reference"
+from oracle import ref as _ref
+
+
+def _reference_dir() -> str:
+    """The reference source directory: KAPSEL_REF_SRC, else the one the
+    oracle build recorded (oracle/_ref/source_dir.txt); empty if neither."""
+    d = os.environ.get("KAPSEL_REF_SRC", "")
+    rec = os.path.join(_ref.REF_DIR, "source_dir.txt")
+    if not d and os.path.exists(rec):
+        with open(rec) as f:
+            d = f.read().strip()
+    return d
+
+
+REF = _reference_dir()
 pytestmark = pytest.mark.ref
 
 

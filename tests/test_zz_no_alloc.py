@@ -6,14 +6,18 @@ this entry point; it keeps its work space in a static device array instead
 of calling cudaMalloc.  The test calls it through the C ABI on device buffers
 that the test itself allocates, twice in a row with different inputs, and
 compares each result with the existing allocating entry point
-kapsel_gpu_solenoidal_u on the same fields (relative error <= 1e-12, the
-FP64 tolerance of the other spectral tests).  The file name sorts last so a
+kapsel_gpu_solenoidal_u on the same fields and with the oracle's
+Solenoidal_u (relative error <= 1e-12, the FP64 tolerance of the other
+spectral tests).  The grids include the largest ones the static array
+holds (64^3 and 128x16x128).  The file name sorts last so a
 stop-at-first-failure run has already run every other test.
 """
 import ctypes
 
 import numpy as np
 import pytest
+
+from oracle import spm
 
 pytestmark = pytest.mark.gpu
 
@@ -22,7 +26,7 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
-@pytest.mark.parametrize("np_xyz", [(5, 5, 5), (6, 5, 4)])
+@pytest.mark.parametrize("np_xyz", [(5, 5, 5), (6, 5, 4), (6, 6, 6), (7, 4, 7)])
 def test_noalloc_solenoidal_matches_existing_entry_point(np_xyz):
     import torch
 
@@ -34,6 +38,7 @@ def test_noalloc_solenoidal_matches_existing_entry_point(np_xyz):
     fn.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_double] + [ctypes.c_void_p] * 7
     cfg = {"np_xyz": np_xyz, "particles": []}
     sim = kg.Simulation(cfg, precision=kg.FP64)
+    oracle = spm.Spectral(spm.Params(cfg))
     N = (sim.NX, sim.NY, sim.NZ)
     npx = (ctypes.c_int * 3)(*np_xyz)
     rng = np.random.default_rng(11)
@@ -49,6 +54,7 @@ def test_noalloc_solenoidal_matches_existing_entry_point(np_xyz):
         got = np.stack([t.cpu().numpy() for t in dev_out])
         assert np.isfinite(got).all()
         assert _rel(got, expected) < 1e-12, (call, _rel(got, expected))
+        assert _rel(got, oracle.solenoidal_u(u)) < 1e-12
     sim.close()
 
 
