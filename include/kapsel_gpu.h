@@ -218,6 +218,42 @@ int kapsel_gpu_calc_f_hydro(kapsel_ctx *ctx, const double *u0, const double *u1,
    context's particles; writes fr[n*3]. */
 int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr);
 
+/* Calc_f_Lennard_Jones_shear_cap_primitive_lnk with the minimum-image
+   Distance0 and no cap (md_force.cxx:23-134, md_force.h:75-78): the LJ force
+   alone, cell-list pair multiplicity included; writes fr[n*3]. */
+int kapsel_gpu_calc_lj(kapsel_ctx *ctx, double *fr);
+
+/* Make_phi_particle (make_phi.cxx:180-219; no phi > 1 clamp) for the
+   context's particles: phi as an NX*NY*NZ_ field. */
+int kapsel_gpu_make_phi(kapsel_ctx *ctx, double *phi);
+
+/* NS_solver_slavedEuler (fluid_solver.cxx:328-354): the advection term of the
+   2/3-truncated zeta (Zeta_k2advection_k, operate_omega.cxx:102-113) and the
+   slaved-Euler update of the retained modes, on zeta[2] in the Ooura layout
+   (2*NX*NY*NZ_ doubles, updated in place; the modes outside the 2/3 box keep
+   their values, as in the reference) with the k=0 velocity uk_dc[3].  The
+   context's own fluid state is replaced by the result. */
+int kapsel_gpu_ns_slaved_euler(kapsel_ctx *ctx, double *zeta, const double *uk_dc);
+
+/* MD_solver_position_Euler (euler != 0) / MD_solver_position_AB2
+   (particle_solver.cxx:36-88) on the context's particle state (set it with
+   kapsel_gpu_set_particle_state, read it with kapsel_gpu_get_particles). */
+int kapsel_gpu_md_position(kapsel_ctx *ctx, int euler);
+
+/* MD_solver_velocity_Euler (euler != 0) / MD_solver_velocity_AB2_hydro
+   (particle_solver.cxx:106-147, 247-289) on the context's particle state,
+   with this step's hydrodynamic force and torque given (the f_hydro and
+   torque_hydro that Calc_f_hydro_correct_precision left, n*3 each): Force
+   (LJ + gravity), the velocity update and reset_Forces, after which the
+   records' f_hydro / torque_hydro / fr hold the step's values (the
+   reference's *_previous). */
+int kapsel_gpu_md_velocity(kapsel_ctx *ctx, const double *f_hydro, const double *torque_hydro, int euler);
+
+/* Sets the step counter jikan.ts and time jikan.time (a host program that
+   attaches a context to a run in progress); the thermostat stream keeps its
+   position. */
+int kapsel_gpu_set_time(kapsel_ctx *ctx, int ts, double time);
+
 /* Solenoidal_u on three real fields that are already in device memory,
    packed as NX*NY*NZ doubles each (no NZ_ padding), written to three device
    output fields of the same shape, on `stream` (a cudaStream_t; NULL for the

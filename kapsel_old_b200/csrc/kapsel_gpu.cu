@@ -219,6 +219,8 @@ struct BoxBase {
   virtual int phi_up_host(double *phi, double *up0, double *up1, double *up2) = 0;
   virtual int phi_only_host(double *phi) = 0;  // Make_phi_particle: no clamp
   virtual int fhydro_host(const double *u0, const double *u1, const double *u2, double *f, double *t) = 0;
+  // NS_solver_slavedEuler on a host zeta (Ooura layout): retained modes updated in place
+  virtual int slaved_euler_host(double *z, const double *ukdc) = 0;
   virtual void free_all() = 0;
 
   int fill_noise(int slot) {
@@ -1077,6 +1079,40 @@ struct Box : BoxBase {
   int phi_up_host(double *phi, double *up0, double *up1, double *up2) override;
   int phi_only_host(double *phi) override;
   int fhydro_host(const double *u0, const double *u1, const double *u2, double *f, double *t) override;
+  int slaved_euler_host(double *z, const double *ukdc) override {
+    // NS_solver_slavedEuler (fluid_solver.cxx:328-354): the advection term
+    // of the truncated zeta and the slaved-Euler update of the retained
+    // modes (launches 1-5 of the step); the modes outside the 2/3 box, which
+    // the reference leaves untouched, keep the caller's values
+    if (prm.eq != KAPSEL_EQ_NAVIER_STOKES) return KAPSEL_EINVAL;
+    int rc = zeta_from_host(z);
+    if (rc) return rc;
+    KCHECK(cudaMemcpyAsync(uk_dc, ukdc, sizeof(double) * 3, cudaMemcpyHostToDevice, stream));
+    x_zeta(false, zeta, uk_dc, bufA);
+    launch_y<true>(g, 3, bufA, bufB);
+    zdisp_products(false);
+    launch_y<false>(g, 5, bufB, bufA);
+    x_advect<0>(false);
+    KCHECK(cudaGetLastError());
+    // the update also applied FIX_CELL to the device uk_dc and left u_k of the
+    // new zeta in bufA; neither is the routine's output: restore uk_dc
+    KCHECK(cudaMemcpyAsync(uk_dc, ukdc, sizeof(double) * 3, cudaMemcpyHostToDevice, stream));
+    u_spec_ready = false;
+    const int NZ_ = g.NZ + 2;
+    const size_t plane = (size_t)g.NX * g.NY * NZ_;
+    std::vector<double> full(2 * plane);
+    if ((rc = zeta_to_host(full.data()))) return rc;
+    for (int c = 0; c < 2; ++c)
+      for (int ix = 0; ix < g.KXc; ++ix) {
+        const int i = ix < g.TX ? ix : g.NX + ix - g.KXc;
+        for (int iy = 0; iy < g.KYc; ++iy) {
+          const int j = iy < g.TY ? iy : g.NY + iy - g.KYc;
+          const size_t o = c * plane + ((size_t)i * g.NY + j) * NZ_;
+          memcpy(z + o, full.data() + o, sizeof(double) * 2 * g.TZ);
+        }
+      }
+    return 0;
+  }
 
   void free_all() override {
     cudaFree(ob6);
@@ -1980,10 +2016,11 @@ int kapsel_gpu_calc_f_hydro(kapsel_ctx *ctx, const double *u0, const double *u1,
   return ctx->box->fhydro_host(u0, u1, u2, f, t);
 }
 
-int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr) {
-  // Runs the particle kernel on a copy of the particle state with zero hydro
-  // input is not separable; the LJ + gravity force is recovered from one
-  // velocity update on a scratch copy: fr = fr_prev after an Euler update.
+// Force (particle_solver.h:97-109) without the hydrodynamic part, on a
+// scratch copy of the particle state: the particle kernel runs with no
+// Sekibun points and no thermostat, and fr_prev after its velocity update is
+// the LJ (+ gravity when `gravity`) force of the current positions.
+static int calc_fr_impl(kapsel_ctx *ctx, double *fr, bool gravity) {
   if (!ctx || !fr) return KAPSEL_EINVAL;
   BoxBase *b = ctx->box.get();
   if (b->Np == 0) return 0;
@@ -1993,6 +2030,8 @@ int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr) {
   PPar p = b->pp;
   p.S = 0;           // no hydro gather
   p.thermostat = 0;  // no kick
+  p.frozen = 0;
+  if (!gravity) p.grav = 0.0;
   // u is never read with S == 0
   if (b->prm.precision == KAPSEL_FP64)
     k_particles_hydro_velocity<double><<<b->Np * p.hyd_pcl, p.hyd_threads, 0, b->stream>>>(p, scratch, nullptr, b->cells, nullptr, 1,
@@ -2006,6 +2045,97 @@ int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr) {
   cudaFree(scratch);
   for (int n = 0; n < b->Np; ++n)
     for (int d = 0; d < 3; ++d) fr[3 * n + d] = h[n].fr_prev[d];
+  return 0;
+}
+
+int kapsel_gpu_calc_fr(kapsel_ctx *ctx, double *fr) { return calc_fr_impl(ctx, fr, true); }
+
+int kapsel_gpu_calc_lj(kapsel_ctx *ctx, double *fr) { return calc_fr_impl(ctx, fr, false); }
+
+int kapsel_gpu_make_phi(kapsel_ctx *ctx, double *phi) {
+  if (!ctx || !phi) return KAPSEL_EINVAL;
+  return ctx->box->phi_only_host(phi);
+}
+
+int kapsel_gpu_ns_slaved_euler(kapsel_ctx *ctx, double *zeta, const double *uk_dc) {
+  if (!ctx || !zeta || !uk_dc) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  int rc = b->slaved_euler_host(zeta, uk_dc);
+  if (rc) return rc;
+  b->initialised = true;
+  return check_status(b);
+}
+
+int kapsel_gpu_md_position(kapsel_ctx *ctx, int euler) {
+  if (!ctx) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (b->Np == 0) return 0;
+  if (!b->particles_set) return KAPSEL_ESTATE;
+  PPar p = b->pp;
+  p.frozen = 0;
+  k_particles_position<<<(b->Np + 127) / 128, 128, 0, b->stream>>>(p, b->parts, euler ? 1 : 0, b->status);
+  if (cudaGetLastError() != cudaSuccess) return KAPSEL_ECUDA;
+  return check_status(b);
+}
+
+int kapsel_gpu_md_velocity(kapsel_ctx *ctx, const double *f_hydro, const double *torque_hydro, int euler) {
+  // the particle kernel with no Sekibun points: the given hydrodynamic force
+  // and torque enter through its per-particle correction input (added to an
+  // empty gather), then Force, the velocity update and reset_Forces
+  if (!ctx || (ctx->box->Np > 0 && (!f_hydro || !torque_hydro))) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (b->Np == 0) return 0;
+  if (!b->particles_set) return KAPSEL_ESTATE;
+  std::vector<double> h(6 * (size_t)b->Np);
+  for (int n = 0; n < b->Np; ++n)
+    for (int d = 0; d < 3; ++d) {
+      h[6 * n + d] = f_hydro[3 * n + d];
+      h[6 * n + 3 + d] = torque_hydro[3 * n + d];
+    }
+  double *corr = nullptr;
+  if (cudaMalloc(&corr, sizeof(double) * h.size()) != cudaSuccess) return KAPSEL_ENOMEM;
+  int rc = 0;
+  if (cudaMemcpyAsync(corr, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
+    rc = KAPSEL_ECUDA;
+  PPar p = b->pp;
+  p.S = 0;
+  p.thermostat = 0;
+  p.frozen = 0;
+  if (!rc) {
+    if (b->prm.precision == KAPSEL_FP64)
+      k_particles_hydro_velocity<double><<<b->Np * p.hyd_pcl, p.hyd_threads, 0, b->stream>>>(
+          p, b->parts, nullptr, b->cells, nullptr, euler ? 1 : 0, b->status, b->partial_p, b->arrivals, corr);
+    else
+      k_particles_hydro_velocity<float><<<b->Np * p.hyd_pcl, p.hyd_threads, 0, b->stream>>>(
+          p, b->parts, nullptr, b->cells, nullptr, euler ? 1 : 0, b->status, b->partial_p, b->arrivals, corr);
+    if (cudaGetLastError() != cudaSuccess) rc = KAPSEL_ECUDA;
+  }
+  if (!rc) rc = check_status(b);
+  cudaFree(corr);
+  return rc;
+}
+
+int kapsel_gpu_set_time(kapsel_ctx *ctx, int ts, double time) {
+  if (!ctx || ts < 0) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
+  // normals already drawn for the next step stay the next step's: the
+  // thermostat stream does not move with the step counter
+  const int oslot = b->ts & 1, nslot = ts & 1;
+  const bool pending = b->noise_pre_ts[oslot] == b->ts;
+  b->drop_prefill();
+  if (pending) {
+    if (nslot != oslot) {
+      if (cudaMemcpyAsync(b->noise_dev[nslot], b->noise_dev[oslot], sizeof(double) * 6 * b->Np,
+                          cudaMemcpyDeviceToDevice, b->stream) != cudaSuccess ||
+          cudaEventRecord(b->noise_ev[nslot], b->stream) != cudaSuccess ||
+          cudaStreamSynchronize(b->stream) != cudaSuccess)
+        return KAPSEL_ECUDA;
+    }
+    b->noise_pre_ts[nslot] = ts;
+  }
+  b->ts = ts;
+  b->time = time;
   return 0;
 }
 
