@@ -86,6 +86,11 @@ typedef struct kapsel_params {
      (constitutive_eq.Shear_Navier_Stokes_Lees_Edwards.External_field.DC,
      input.cxx:634-645); ignored by the other branches. */
   double shear_rate;
+  /* Pair searches (LJ forces, the overlap test of the phi/up scatter, the
+     near-contact pairs): 0 chooses by particle count (per-step cell and
+     neighbour lists above 1024 particles, a scan of all particles below),
+     1 always uses the lists, -1 never.  Results do not depend on it. */
+  int neighbor_lists;
 } kapsel_params;
 
 typedef struct kapsel_ctx kapsel_ctx;

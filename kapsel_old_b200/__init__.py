@@ -68,6 +68,7 @@ class _Params(ctypes.Structure):
         ("e_ext", ctypes.c_double * 3),
         ("frozen", ctypes.c_int),
         ("shear_rate", ctypes.c_double),
+        ("neighbor_lists", ctypes.c_int),
     ]
 
 
@@ -112,6 +113,12 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_make_phi_u": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP]),
         "kapsel_gpu_calc_f_hydro": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP, _DP]),
         "kapsel_gpu_calc_fr": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_calc_lj": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_make_phi": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_ns_slaved_euler": (ctypes.c_int, [_VP, _DP, _DP]),
+        "kapsel_gpu_md_position": (ctypes.c_int, [_VP, ctypes.c_int]),
+        "kapsel_gpu_md_velocity": (ctypes.c_int, [_VP, _DP, _DP, ctypes.c_int]),
+        "kapsel_gpu_set_time": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_double]),
         "kapsel_gpu_strerror": (ctypes.c_char_p, [ctypes.c_int]),
         "kapsel_gpu_save_restart": (ctypes.c_int, [_VP, ctypes.c_char_p]),
         "kapsel_gpu_write_avs": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
@@ -171,6 +178,7 @@ def params_from_config(cfg: dict, precision: int = FP64) -> _Params:
         p.fix_cell[d] = 1 if fc[d] else 0
     p.mt_seed = int(cfg.get("mt_seed", 0))
     p.frozen = 1 if cfg.get("frozen", False) else 0
+    p.neighbor_lists = int(cfg.get("neighbor_lists", 0))
     el = cfg.get("electrolyte")
     if el:
         p.dielectric = float(el["dielectric"])

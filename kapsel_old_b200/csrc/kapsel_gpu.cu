@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "../../include/kapsel_gpu.h"
+#include "cell_kernels.cuh"
 #include "electrolyte_kernels.cuh"
 #include "nearcontact_kernels.cuh"
 #include "obl_kernels.cuh"
@@ -193,6 +194,66 @@ struct BoxBase {
   // the pair search and the network, between the position update and the
   // hydrodynamic gather (both launched without programmatic serialization)
   void launch_nearcontact();
+
+  // per-step cell and neighbour lists (cell_kernels.cuh); pp.nbl points at
+  // the lists while they are on
+  bool cl_on = false;
+  CellPar clp{};
+  int *cl_count = nullptr, *cl_start = nullptr, *cl_cursor = nullptr, *cl_list = nullptr, *cl_cellof = nullptr;
+  int *nbl = nullptr;
+  double cl_rlist = 0.0;
+  // (re)build the cell grid for a neighbour range of at least rlist; the
+  // captured step graphs hold the old launch parameters and are dropped
+  int setup_cells(double rlist) {
+    if (Np == 0) return 0;
+    if (cl_on && rlist <= cl_rlist) return 0;
+    for (int s = 0; s < 2; ++s)
+      if (graph[s]) {
+        cudaGraphExecDestroy(graph[s]);
+        graph[s] = nullptr;
+      }
+    cudaFree(cl_count);
+    cudaFree(cl_start);
+    cudaFree(cl_cursor);
+    cl_rlist = rlist;
+    for (int d = 0; d < 3; ++d) {
+      clp.lc[d] = std::max(1, (int)std::floor(pp.L[d] / rlist));
+      clp.inv_cl[d] = clp.lc[d] / pp.L[d];
+    }
+    clp.ncell = clp.lc[0] * clp.lc[1] * clp.lc[2];
+    clp.r2list = rlist * rlist;
+    KCHECK(cudaMalloc(&cl_count, sizeof(int) * clp.ncell));
+    KCHECK(cudaMemset(cl_count, 0, sizeof(int) * clp.ncell));
+    KCHECK(cudaMalloc(&cl_start, sizeof(int) * (clp.ncell + 1)));
+    KCHECK(cudaMalloc(&cl_cursor, sizeof(int) * clp.ncell));
+    if (!cl_list) {
+      KCHECK(cudaMalloc(&cl_list, sizeof(int) * Np));
+      KCHECK(cudaMalloc(&cl_cellof, sizeof(int) * Np));
+      KCHECK(cudaMalloc(&nbl, sizeof(int) * (size_t)Np * (NBL_MAX + 1)));
+      KCHECK(cudaMemset(nbl, 0, sizeof(int) * (size_t)Np * (NBL_MAX + 1)));
+    }
+    pp.nbl = nbl;
+    cl_on = true;
+    return 0;
+  }
+  // the lists of the current positions (five launches), before any kernel
+  // that reads them
+  void launch_cells() {
+    if (!cl_on || Np == 0) return;
+    k_cell_count<<<(Np + 255) / 256, 256, 0, stream>>>(pp, clp, parts, cl_cellof, cl_count);
+    k_cell_scan<<<1, 1024, 0, stream>>>(clp, cl_count, cl_start, cl_cursor);
+    k_cell_fill<<<(Np + 255) / 256, 256, 0, stream>>>(pp, cl_cellof, cl_cursor, cl_list);
+    k_cell_sort<<<(clp.ncell + 255) / 256, 256, 0, stream>>>(clp, cl_start, cl_list);
+    k_neighbor_lists<<<(Np + 127) / 128, 128, 0, stream>>>(pp, clp, parts, cl_start, cl_list, nbl, status);
+  }
+  void free_cells() {
+    cudaFree(cl_count);
+    cudaFree(cl_start);
+    cudaFree(cl_cursor);
+    cudaFree(cl_list);
+    cudaFree(cl_cellof);
+    cudaFree(nbl);
+  }
 
   virtual int alloc() = 0;
   virtual float time_ypass(int small, int reps) = 0;
@@ -624,6 +685,7 @@ struct Box : BoxBase {
     mark();
     if (Np > 0) {
       if (!fuse_pos) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
+      launch_cells();  // neighbour lists of the new positions (large particle counts)
       mark();
       if (nc) launch_nearcontact();  // timed with the position slot when profiling
       launch_k(pdl, k_particles_hydro_velocity<R>, dim3(Np * pp.hyd_pcl), dim3(pp.hyd_threads), 0, stream, pp, parts,
@@ -631,7 +693,7 @@ struct Box : BoxBase {
                nc ? nc_corr : (double *)nullptr);
       mark();
       launch_k(pdl, k_particles_scatter<R>, dim3(Np * PCL), dim3(256), 0, stream, pp, (const DPart *)parts,
-               (const int *)cells, phiup);
+               (const int *)cells, phiup, status);
       mark();
       zdisp_force(pdl);
       mark();
@@ -660,7 +722,8 @@ struct Box : BoxBase {
     cudaMemsetAsync(ustar, 0, sizeof(R) * 3 * npts(), stream);
     cudaMemsetAsync(uk_dc, 0, sizeof(double) * 3, stream);
     if (Np > 0) {
-      k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup);
+      launch_cells();
+      k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup, status);
       launch_force_to_zeta();
     }
     cudaMemsetAsync(uk_dc, 0, sizeof(double) * 3, stream);
@@ -894,6 +957,7 @@ struct Box : BoxBase {
                                                                          KOp{prm.dt, {0, 0, 0}});
     }
     if (Np > 0) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
+    launch_cells();
     // Rescale_solute at the new positions, then the Coulomb force
     el_scatter(0);
     el_surface_scale();
@@ -925,7 +989,7 @@ struct Box : BoxBase {
     if (Np > 0) {
       k_particles_hydro_velocity<R><<<Np * pp.hyd_pcl, pp.hyd_threads, 0, stream>>>(pp, parts, ustar, cells, nullptr, euler, status,
                                                                   partial_p, arrivals);
-      k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup);
+      k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, phiup, status);
       launch_force_to_zeta();
     }
   }
@@ -1375,7 +1439,8 @@ int Box<R>::phi_up_host(double *phi, double *up0, double *up1, double *up2) {
   R *d = nullptr;
   KCHECK(cudaMalloc(&d, sizeof(R) * 4 * npt));
   KCHECK(cudaMemsetAsync(d, 0, sizeof(R) * 4 * npt, stream));
-  if (Np > 0) k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, d);
+  launch_cells();
+  if (Np > 0) k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, d, status);
   k_clamp_phi<R><<<592, 256, 0, stream>>>(npt, d);
   KCHECK(cudaGetLastError());
   std::vector<R> h(4 * npt);
@@ -1393,7 +1458,8 @@ int Box<R>::phi_only_host(double *phi) {
   R *d = nullptr;
   KCHECK(cudaMalloc(&d, sizeof(R) * 4 * npt));
   KCHECK(cudaMemsetAsync(d, 0, sizeof(R) * 4 * npt, stream));
-  if (Np > 0) k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, d);
+  launch_cells();
+  if (Np > 0) k_particles_scatter<R><<<Np * PCL, 256, 0, stream>>>(pp, parts, cells, d, status);
   KCHECK(cudaGetLastError());
   std::vector<R> h(npt);
   KCHECK(cudaMemcpyAsync(h.data(), d, sizeof(R) * npt, cudaMemcpyDeviceToHost, stream));
@@ -1683,6 +1749,7 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   pp.hyd_pcl = 1;
   pp.hyd_threads = b->Np >= 128 ? 512 : 1024;
   if (pp.frozen) pp.thermostat = 0;
+  if (p->neighbor_lists < -1 || p->neighbor_lists > 1) return KAPSEL_EINVAL;
   b->mt.reset(new MT19937(p->mt_seed));
 
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return KAPSEL_ECUDA;
@@ -1707,6 +1774,14 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   cudaMemset(b->uk_dc, 0, sizeof(double) * 3);
   if (cudaMalloc(&b->status, sizeof(int)) != cudaSuccess) return KAPSEL_ENOMEM;
   cudaMemset(b->status, 0, sizeof(int));
+  // neighbour lists: the Navier_Stokes and Electrolyte particle kernels
+  // read them; the range covers the LJ cutoff and two overlapping supports
+  if (b->Np > 0 && p->eq != KAPSEL_EQ_SHEAR_LE &&
+      (p->neighbor_lists == 1 || (p->neighbor_lists == 0 && b->Np > 1024))) {
+    const double rl = std::max(pp.lj_on ? pp.lj_cut : 0.0, 2.0 * (pp.RADIUS + pp.HXI)) * (1.0 + 1e-9);
+    rc = b->setup_cells(rl);
+    if (rc) return rc;
+  }
   if (cudaMalloc(&b->partial_p, sizeof(double) * 18 * HYD_PCL_MAX * np1) != cudaSuccess) return KAPSEL_ENOMEM;
   if (cudaMalloc(&b->arrivals, sizeof(int) * np1) != cudaSuccess) return KAPSEL_ENOMEM;
   cudaMemset(b->arrivals, 0, sizeof(int) * np1);
@@ -1736,6 +1811,7 @@ int kapsel_gpu_destroy(kapsel_ctx *ctx) {
       if (b->noise_ev[s]) cudaEventDestroy(b->noise_ev[s]);
     }
     b->free_all();
+    b->free_cells();
     cudaFree(b->parts);
     cudaFreeHost(b->parts_host);
     cudaFree(b->cells);
@@ -2008,7 +2084,8 @@ int kapsel_gpu_solenoidal_u(kapsel_ctx *ctx, double *u0, double *u1, double *u2)
 }
 int kapsel_gpu_make_phi_u(kapsel_ctx *ctx, double *phi, double *up0, double *up1, double *up2) {
   if (!ctx || !phi || !up0 || !up1 || !up2) return KAPSEL_EINVAL;
-  return ctx->box->phi_up_host(phi, up0, up1, up2);
+  const int rc = ctx->box->phi_up_host(phi, up0, up1, up2);
+  return rc ? rc : check_status(ctx->box.get());
 }
 int kapsel_gpu_calc_f_hydro(kapsel_ctx *ctx, const double *u0, const double *u1, const double *u2, double *f,
                             double *t) {
@@ -2027,6 +2104,7 @@ static int calc_fr_impl(kapsel_ctx *ctx, double *fr, bool gravity) {
   DPart *scratch = nullptr;
   if (cudaMalloc(&scratch, sizeof(DPart) * b->Np) != cudaSuccess) return KAPSEL_ENOMEM;
   cudaMemcpyAsync(scratch, b->parts, sizeof(DPart) * b->Np, cudaMemcpyDeviceToDevice, b->stream);
+  b->launch_cells();
   PPar p = b->pp;
   p.S = 0;           // no hydro gather
   p.thermostat = 0;  // no kick
@@ -2054,7 +2132,8 @@ int kapsel_gpu_calc_lj(kapsel_ctx *ctx, double *fr) { return calc_fr_impl(ctx, f
 
 int kapsel_gpu_make_phi(kapsel_ctx *ctx, double *phi) {
   if (!ctx || !phi) return KAPSEL_EINVAL;
-  return ctx->box->phi_only_host(phi);
+  const int rc = ctx->box->phi_only_host(phi);
+  return rc ? rc : check_status(ctx->box.get());
 }
 
 int kapsel_gpu_ns_slaved_euler(kapsel_ctx *ctx, double *zeta, const double *uk_dc) {
@@ -2097,6 +2176,7 @@ int kapsel_gpu_md_velocity(kapsel_ctx *ctx, const double *f_hydro, const double 
   int rc = 0;
   if (cudaMemcpyAsync(corr, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
     rc = KAPSEL_ECUDA;
+  b->launch_cells();
   PPar p = b->pp;
   p.S = 0;
   p.thermostat = 0;
@@ -2802,6 +2882,11 @@ int kapsel_gpu_set_nearcontact(kapsel_ctx *ctx, const kapsel_nc *nc) {
       return KAPSEL_ENOMEM;
     KCHECK(cudaMemset(b->nc_count, 0, sizeof(int)));
     KCHECK(cudaMemset(b->nc_corr, 0, sizeof(double) * 6 * b->Np));
+  }
+  if (nc && b->cl_on) {
+    // the lists must reach every pair in the trained gap range
+    const int rc = b->setup_cells(std::max(b->cl_rlist, (2.0 * b->pp.RADIUS + nc->sc.gap_hi * nc->sc.a) * (1.0 + 1e-9)));
+    if (rc) return rc;
   }
   b->nc = nc;
   return 0;

@@ -453,7 +453,13 @@ __global__ void __launch_bounds__(128) k_nc_pairs(PPar p, const DPart *__restric
   const int i = blockIdx.x;
   const DPart &a = parts[i];
   const double lo = sc.gap_lo * sc.a, hi = sc.gap_hi * sc.a;
-  for (int j = i + 1 + threadIdx.x; j < p.Np; j += blockDim.x) {
+  // candidates j > i: the neighbour list (sorted; it covers the trained gap
+  // range) or all later particles
+  const int *lst = p.nbl ? p.nbl + (size_t)i * (NBL_MAX + 1) : nullptr;
+  const int ncand = lst ? lst[0] : p.Np - i - 1;
+  for (int t = threadIdx.x; t < ncand; t += blockDim.x) {
+    const int j = lst ? lst[1 + t] : i + 1 + t;
+    if (j <= i) continue;
     const DPart &b = parts[j];
     double d[3];
     for (int k = 0; k < 3; ++k) {

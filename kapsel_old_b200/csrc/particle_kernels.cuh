@@ -38,7 +38,13 @@ struct PPar {
   int frozen;               // positions and velocities held; forces still measured
   int hyd_pcl;              // gather blocks per particle (at most HYD_PCL_MAX)
   int hyd_threads;          // threads per gather block (at most 1024)
+  // per-particle neighbour lists ([Np][NBL_MAX + 1]: count, then indices in
+  // increasing order) built each step for large particle counts; null: the
+  // pair searches scan all particles
+  const int *nbl = nullptr;
 };
+
+constexpr int NBL_MAX = 64;  // neighbours a list holds (more: KAPSEL_ERANGE)
 
 __device__ __forceinline__ double nint_d(double a) {
   // Nint (macro.h:38-46): round half away from zero
@@ -91,18 +97,36 @@ __device__ __forceinline__ StencilBase stencil_base(const double *x, const PPar 
   }
   return b;
 }
-__device__ __forceinline__ void stencil_point(const StencilBase &b, const int *cell, const double *xp, const PPar &p,
-                                              int rm[3], double r[3], double &dist) {
+// Distance (interaction.h:110-133) from the particle centre xp to grid
+// point rm under the minimum image, every operation rounded separately (as
+// the reference's x86 build computes it, and identically wherever it is
+// inlined: the deterministic scatter compares values computed at
+// different sites).
+__device__ __forceinline__ double point_dist(const double *xp, const int rm[3], const PPar &p) {
   double s = 0.0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);  // N is a power of two
-    r[d] = (double)cell[d] * p.DX - b.res[d];
-    double dd = xp[d] - (double)rm[d] * p.DX;
-    dd -= nint_d(dd * p.invL[d]) * p.L[d];
-    s += dd * dd;
+    double dd = __dsub_rn(xp[d], __dmul_rn((double)rm[d], p.DX));
+    dd = __dsub_rn(dd, __dmul_rn(nint_d(__dmul_rn(dd, p.invL[d])), p.L[d]));
+    s = __dadd_rn(s, __dmul_rn(dd, dd));
   }
-  dist = sqrt(s);
+  return __dsqrt_rn(s);
+}
+__device__ __forceinline__ void stencil_point(const StencilBase &b, const int *cell, const double *xp, const PPar &p,
+                                              int rm[3], double r[3], double &dist) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);  // N is a power of two
+    r[d] = __dsub_rn(__dmul_rn((double)cell[d], p.DX), b.res[d]);
+  }
+  dist = point_dist(xp, rm, p);
+}
+// The mixed path's offset of a stencil point from the sphere centre and its
+// length, in float with every operation rounded separately.
+__device__ __forceinline__ float offset_f(const int cell[3], const float resf[3], float dxf, float r[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) r[d] = __fsub_rn(__fmul_rn((float)cell[d], dxf), resf[d]);
+  return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(r[0], r[0]), __fmul_rn(r[1], r[1])), __fmul_rn(r[2], r[2])));
 }
 
 // Neumaier compensated accumulation.
@@ -286,11 +310,8 @@ __global__ void __launch_bounds__(1024) k_particles_hydro_velocity(PPar p, DPart
       int rm[3];
       float r[3];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);
-        r[d] = (float)cell[d] * dxf - resf[d];
-      }
-      const float ph = prof_phi_f(sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]), rpf, rmf, dxf);
+      for (int d = 0; d < 3; ++d) rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);
+      const float ph = prof_phi_f(offset_f(cell, resf, dxf, r), rpf, rmf, dxf);
       // phi is exactly zero beyond a + xi/2 (about half of the Sekibun
       // points): those terms add zeros, so their loads are skipped
       if (ph == 0.f) continue;
@@ -340,7 +361,12 @@ __global__ void __launch_bounds__(1024) k_particles_hydro_velocity(PPar p, DPart
   if (p.lj_on) {
     int mc[3];
     for (int d = 0; d < 3; ++d) mc[d] = (int)(xp[d] / p.lc_r);
-    for (int j = first; j < p.Np; j += stride) {
+    // candidates: the neighbour list (every pair within the LJ cutoff is on
+    // it) or all particles
+    const int *lst = p.nbl ? p.nbl + (size_t)n * (NBL_MAX + 1) : nullptr;
+    const int ncand = lst ? lst[0] : p.Np;
+    for (int t = first; t < ncand; t += stride) {
+      const int j = lst ? lst[1 + t] : t;
       if (j == n) continue;
       const DPart &o = parts[j];
       int mult = 1;
@@ -374,20 +400,19 @@ __global__ void __launch_bounds__(1024) k_particles_hydro_velocity(PPar p, DPart
   }
   KSum acc[9];
   if constexpr (sizeof(R) == 4) {
-    // warp sums (float hydro terms, plain double LJ terms), then a
-    // compensated double sum over the warps
+    // each thread's few hydro terms are summed in float; from the warp
+    // level up every sum is double (warp sums plain, the sum over the warps
+    // compensated)
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-    for (int i = 0; i < 6; ++i)
+    for (int i = 0; i < 6; ++i) a9[i] = (double)f6[i];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) f6[i] += __shfl_xor_sync(0xffffffffu, f6[i], o);
-#pragma unroll
-    for (int i = 6; i < 9; ++i)
+    for (int i = 0; i < 9; ++i)
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) a9[i] += __shfl_xor_sync(0xffffffffu, a9[i], o);
     if (lane == 0)
 #pragma unroll
-      for (int i = 0; i < 9; ++i) sh[(2 * i) * 32 + wid] = i < 6 ? (double)f6[i] : a9[i];
+      for (int i = 0; i < 9; ++i) sh[(2 * i) * 32 + wid] = a9[i];
     __syncthreads();
     if (threadIdx.x < 9) {
       const int i = threadIdx.x;
@@ -485,71 +510,223 @@ __global__ void __launch_bounds__(1024) k_particles_hydro_velocity(PPar p, DPart
     if (!isfinite(a.v[d]) || !isfinite(a.omega[d])) atomicExch(status, -5);
 }
 
-// Make_phi_u_primitive scatter (make_phi.cxx:221-277): phi += phi_i and
-// up += (v + omega x r) phi_i over the Sekibun points of each particle.
-// The phi > 1 clamp is applied by the consumer.  PCL blocks per particle.
+// ---------------------------------------------------------------------------
+// Deterministic phi / phi*u_p scatter.
+//
+// Make_phi_u_primitive (make_phi.cxx:221-277) adds each particle's profile
+// phi_i and phi_i (v_i + omega_i x r) into the fields particle by particle,
+// so where the supports of several particles overlap a point receives its
+// terms in increasing particle index.  Here every point is written by ONE
+// thread, the one of the lowest-index particle whose profile is non-zero
+// there (its "owner"): it adds its own term and then those of the
+// higher-index overlapping particles in index order, and stores the sum.
+// No atomics, no dependence on scheduling: graph and eager runs, and every
+// run, give the same bits, and the FP64 sums are the reference's own order.
+// Every other particle skips the point.  The candidates are the particles
+// whose centre is within 2 (RADIUS + HXI) of this one (minimum image): a
+// point can only be inside two supports if they overlap.  They come from
+// the step's neighbour lists for large particle counts, else from a scan of
+// all particles by every block.
+constexpr int NB_MAX = 64;  // overlapping neighbours per particle (more: KAPSEL_ERANGE)
+
+struct NbShared {
+  double x[3], v[3], w[3], res[3];
+  float resf[3];
+  int xi[3];
+  int idx;
+};
+
+// The overlap candidates of particle n in increasing index order, into nb
+// (at most NB_MAX); returns their count.  All threads of the block call it.
+__device__ int overlap_candidates(const PPar &p, const DPart *__restrict__ parts, int n, NbShared *nb,
+                                  int *__restrict__ status) {
+  __shared__ int wcount[32];
+  __shared__ int total;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double lim = 2.0 * (p.RADIUS + p.HXI), lim2 = lim * lim;
+  const double *xn = parts[n].x;
+  // the neighbour list when there is one (in index order), else all particles
+  const int *lst = p.nbl ? p.nbl + (size_t)n * (NBL_MAX + 1) : nullptr;
+  const int ncand = lst ? lst[0] : p.Np;
+  if (threadIdx.x == 0) total = 0;
+  __syncthreads();
+  for (int base = 0; base < ncand; base += blockDim.x) {
+    const int t = base + threadIdx.x;
+    const int j = t < ncand ? (lst ? lst[1 + t] : t) : -1;
+    bool near = false;
+    if (j >= 0 && j != n) {
+      double s = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        double dd = parts[j].x[d] - xn[d];
+        dd -= nint_d(dd * p.invL[d]) * p.L[d];
+        s += dd * dd;
+      }
+      near = s < lim2;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, near);
+    if (lane == 0) wcount[warp] = __popc(bal);
+    __syncthreads();
+    int pos = total + __popc(bal & ((1u << lane) - 1u));
+    for (int w = 0; w < warp; ++w) pos += wcount[w];
+    if (near && pos < NB_MAX) {
+      const DPart &o = parts[j];
+      NbShared &e = nb[pos];
+      const StencilBase sb = stencil_base(o.x, p);
+      for (int d = 0; d < 3; ++d) {
+        e.x[d] = o.x[d];
+        e.v[d] = o.v[d];
+        e.w[d] = o.omega[d];
+        e.res[d] = sb.res[d];
+        e.resf[d] = (float)sb.res[d];
+        e.xi[d] = sb.xi[d];
+      }
+      e.idx = j;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int w = 0; w < nw; ++w) total += wcount[w];
+    __syncthreads();
+  }
+  if (total > NB_MAX) {
+    if (threadIdx.x == 0) atomicExch(status, -6);
+    return NB_MAX;
+  }
+  return total;
+}
+
+// Sekibun offset of grid point rm from the stencil base of a sphere (the
+// cell index in [-N/2, N/2) that the sphere's own stencil reaches rm with).
+__device__ __forceinline__ void offset_from_base(const int rm[3], const int xi[3], const PPar &p, int cell[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int c = (rm[d] - xi[d]) & (p.N[d] - 1);
+    cell[d] = c >= p.N[d] / 2 ? c - p.N[d] : c;
+  }
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256) k_particles_scatter(PPar p, const DPart *__restrict__ parts,
-                                                           const int *__restrict__ cells, R *__restrict__ phiup) {
+                                                           const int *__restrict__ cells, R *__restrict__ phiup,
+                                                           int *__restrict__ status) {
+  __shared__ NbShared nb[NB_MAX];
   pdl_begin();
   const int n = blockIdx.x / PCL;
   const int stride = PCL * blockDim.x;
   const int first = (blockIdx.x % PCL) * blockDim.x + threadIdx.x;
+  const int nnb = overlap_candidates(p, parts, n, nb, status);
+  int nlow = 0;  // candidates with a lower index come first
+  while (nlow < nnb && nb[nlow].idx < n) ++nlow;
   const DPart &a = parts[n];
   const double xp[3] = {a.x[0], a.x[1], a.x[2]};
   const double vp[3] = {a.v[0], a.v[1], a.v[2]};
   const double wp[3] = {a.omega[0], a.omega[1], a.omega[2]};
   const StencilBase b = stencil_base(xp, p);
   const size_t npts = (size_t)p.N[0] * p.N[1] * p.N[2];
+  const double rsup = p.RADIUS + p.HXI;
   if constexpr (sizeof(R) == 4) {
     // mixed path: offset, distance, phi and phi*(v + omega x r) in float
     const float dxf = (float)p.DX, rpf = (float)(p.RADIUS + p.HXI), rmf = (float)(p.RADIUS - p.HXI);
     const float resf[3] = {(float)b.res[0], (float)b.res[1], (float)b.res[2]};
-    const float vpf[3] = {(float)vp[0], (float)vp[1], (float)vp[2]};
-    const float wpf[3] = {(float)wp[0], (float)wp[1], (float)wp[2]};
-#pragma unroll 2
     for (int m = first; m < p.S; m += stride) {
       const int *cell = cells + 3 * m;
       int rm[3];
       float r[3];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);
-        r[d] = (float)cell[d] * dxf - resf[d];
+      for (int d = 0; d < 3; ++d) rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);
+      const float ph = prof_phi_f(offset_f(cell, resf, dxf, r), rpf, rmf, dxf);
+      if (ph == 0.f) continue;
+      bool own = true;
+      for (int k = 0; k < nlow && own; ++k) {
+        int cj[3];
+        float rj[3];
+        offset_from_base(rm, nb[k].xi, p, cj);
+        const float dj = offset_f(cj, nb[k].resf, dxf, rj);
+        if (dj < rpf && prof_phi_f(dj, rpf, rmf, dxf) != 0.f) own = false;
       }
-      const float ph = prof_phi_f(sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]), rpf, rmf, dxf);
-      if (ph == 0.f) continue;  // adds zeros: no atomics
-      float vr[3] = {0.f, 0.f, 0.f};
-      if (p.rotation) {
-        vr[0] = wpf[1] * r[2] - wpf[2] * r[1];
-        vr[1] = wpf[2] * r[0] - wpf[0] * r[2];
-        vr[2] = wpf[0] * r[1] - wpf[1] * r[0];
+      if (!own) continue;
+      float acc = ph, up[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        float vr = 0.f;
+        if (p.rotation) {
+          const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+          vr = (float)wp[d1] * r[d2] - (float)wp[d2] * r[d1];
+        }
+        up[d] = ((float)vp[d] + vr) * ph;
+      }
+      for (int k = nlow; k < nnb; ++k) {
+        int cj[3];
+        float rj[3];
+        offset_from_base(rm, nb[k].xi, p, cj);
+        const float dj = offset_f(cj, nb[k].resf, dxf, rj);
+        if (!(dj < rpf)) continue;
+        const float phj = prof_phi_f(dj, rpf, rmf, dxf);
+        if (phj == 0.f) continue;
+        acc += phj;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          float vr = 0.f;
+          if (p.rotation) {
+            const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+            vr = (float)nb[k].w[d1] * rj[d2] - (float)nb[k].w[d2] * rj[d1];
+          }
+          up[d] += ((float)nb[k].v[d] + vr) * phj;
+        }
       }
       const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
-      atomicAdd(reinterpret_cast<float *>(phiup) + im, ph);
+      reinterpret_cast<float *>(phiup)[im] = acc;
 #pragma unroll
-      for (int d = 0; d < 3; ++d)
-        atomicAdd(reinterpret_cast<float *>(phiup) + (1 + d) * npts + im, (vpf[d] + vr[d]) * ph);
+      for (int d = 0; d < 3; ++d) reinterpret_cast<float *>(phiup)[(1 + d) * npts + im] = up[d];
     }
     return;
   }
-#pragma unroll 2
   for (int m = first; m < p.S; m += stride) {
     int rm[3];
     double r[3], dist;
     stencil_point(b, cells + 3 * m, xp, p, rm, r, dist);
     const double ph = (double)prof_phi<R>(dist, p);
-    if (ph == 0.0) continue;  // adds zeros: no atomics
-    double vr[3] = {0.0, 0.0, 0.0};
-    if (p.rotation) {
-      vr[0] = wp[1] * r[2] - wp[2] * r[1];
-      vr[1] = wp[2] * r[0] - wp[0] * r[2];
-      vr[2] = wp[0] * r[1] - wp[1] * r[0];
+    if (ph == 0.0) continue;
+    bool own = true;
+    for (int k = 0; k < nlow && own; ++k) {
+      const double dj = point_dist(nb[k].x, rm, p);
+      if (dj < rsup && (double)prof_phi<R>(dj, p) != 0.0) own = false;
+    }
+    if (!own) continue;
+    double acc = ph, up[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double vr = 0.0;
+      if (p.rotation) {
+        const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+        vr = wp[d1] * r[d2] - wp[d2] * r[d1];
+      }
+      up[d] = (vp[d] + vr) * ph;
+    }
+    for (int k = nlow; k < nnb; ++k) {
+      const double dj = point_dist(nb[k].x, rm, p);
+      if (!(dj < rsup)) continue;
+      const double phj = (double)prof_phi<R>(dj, p);
+      if (phj == 0.0) continue;
+      int cj[3];
+      double rj[3];
+      offset_from_base(rm, nb[k].xi, p, cj);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) rj[d] = __dsub_rn(__dmul_rn((double)cj[d], p.DX), nb[k].res[d]);
+      acc += phj;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double vr = 0.0;
+        if (p.rotation) {
+          const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+          vr = nb[k].w[d1] * rj[d2] - nb[k].w[d2] * rj[d1];
+        }
+        up[d] += (nb[k].v[d] + vr) * phj;
+      }
     }
     const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
-    atomicAdd(phiup + im, (R)ph);
+    phiup[im] = (R)acc;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) atomicAdd(phiup + (1 + d) * npts + im, (R)((vp[d] + vr[d]) * ph));
+    for (int d = 0; d < 3; ++d) phiup[(1 + d) * npts + im] = (R)up[d];
   }
 }
 

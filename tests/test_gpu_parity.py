@@ -214,3 +214,51 @@ def test_thermostat_stream_independent_of_call_pattern():
         assert s.time()[0] == 7
         assert rel(s.particles()["v"], a.particles()["v"]) < 1e-13
         assert rel(s.zeta(), a.zeta()) < 1e-13
+
+
+def test_step_mixed_deterministic_graph_equals_eager():
+    """Mixed precision with overlapping sphere supports (gaps down to 0.1):
+    the phi / phi*u_p scatter has one writer per grid point, so graph replay,
+    eager steps and a second eager run give the same bits."""
+    cfg = _cfg((6, 6, 6), 40, seed=3, kbt=1e-3, min_gap=0.1)
+    a = _sim(cfg, 1)
+    b = _sim(cfg, 1)
+    c = _sim(cfg, 1)
+    a.step(6)
+    b.step(6, graph=True)
+    c.step(6)
+    for s in (b, c):
+        assert np.array_equal(a.zeta(), s.zeta())
+        assert np.array_equal(a.uk_dc(), s.uk_dc())
+        for k in ("x", "v", "omega", "f_hydro"):
+            assert np.array_equal(a.particles()[k], s.particles()[k]), k
+
+
+def test_step_fp64_neighbor_lists_match_oracle():
+    """The per-step cell and neighbour lists (used above 1024 particles)
+    forced on at 32^3, where the reference's LJ cell list has 2 cells per
+    axis and meets pairs more than once: FP64 against the oracle."""
+    cfg = _cfg((5, 5, 5), 6, seed=11, kbt=1e-3, min_gap=0.2)
+    cfg["neighbor_lists"] = 1
+    w = _compare_run(cfg, 5, 0)
+    for k, v in w.items():
+        assert v < FP64_TOL, (k, v, w)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_step_neighbor_lists_equal_all_particle_scan(precision):
+    """Dense 64^3 suspension (gaps down to 0.1, LJ and overlapping
+    supports): the step with neighbour lists equals the step that scans all
+    particles (the scatter bit for bit, the LJ sums to roundoff)."""
+    cfg = _cfg((6, 6, 6), 60, seed=8, kbt=1e-3, min_gap=0.1)
+    on, off = dict(cfg, neighbor_lists=1), dict(cfg, neighbor_lists=-1)
+    a, b = _sim(on, precision), _sim(off, precision)
+    a.step(6, graph=True)
+    b.step(6, graph=True)
+    assert rel(a.zeta(), b.zeta()) < 1e-12
+    pa, pb = a.particles(), b.particles()
+    for k in ("x", "v", "omega", "fr"):
+        assert rel(pa[k], pb[k]) < 1e-12, k
+    phi_a, up_a = a.make_phi_u()
+    phi_b, up_b = b.make_phi_u()
+    assert np.array_equal(phi_a, phi_b) and np.array_equal(up_a, up_b)
