@@ -359,6 +359,21 @@ def run_ours(args, rank, world, local_rank):
                 "torque_error_reduction": round(err["torque_plain"] / err["torque_learned"], 2),
                 "workload": "256^3, 2048 spheres a=5 (volume fraction 0.064), min gap 0.05a, kBT=1e-3, mixed; "
                             "network 16-128-128-128-16 SiLU, tcgen05 BF16"}
+            # the same network at the deployment density (volume fraction
+            # 0.27): neighbour lists for the pair searches
+            cd = workload.nearcontact_256_dense()
+            s6a, _, ms6a = timed(kg.MIXED, k5, args.warmup, cfg=cd)
+            s6a.close()
+            s6b, _, ms6b = timed(kg.MIXED, k5, args.warmup, cfg=cd, setup=lambda sm_: ncm.attach(sm_, net))
+            n_corr6 = ncm.corrected_pairs(s6b)
+            s6b.close()
+            extra["nearcontact_256cubed_dense"] = {
+                "plain": round(k5 * world / (ms6a * 1e-3), 2), "learned": round(k5 * world / (ms6b * 1e-3), 2),
+                "unit": UNIT, "steps": k5, "extra_step_time": round(ms6b / ms6a - 1.0, 4),
+                "pairs_corrected_last_step": n_corr6,
+                "force_error_reduction": round(err["force_plain"] / err["force_learned"], 2),
+                "workload": "256^3, 8600 spheres a=5 (volume fraction 0.268), min gap 0.05a, kBT=1e-3, mixed; "
+                            "the network trained above"}
             net.close()
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             extra["batched_48_boxes"]["cpu_baseline"] = cpu_baseline_batch(boxes)
