@@ -283,6 +283,41 @@ int kapsel_gpu_set_time(kapsel_ctx *ctx, int ts, double time);
 int kapsel_gpu_solenoidal_u_noalloc(const int *np_xyz, double dx, const double *u0, const double *u1,
                                     const double *u2, double *o0, double *o1, double *o2, void *stream);
 
+/* ---- UDF files (host only, no GPU needed). ----
+
+   KAPSEL reads its input and writes its records through OCTA's UDFManager
+   (Gourmet_file_io, input.cxx:438-1818; Output_udf avs_output.cxx:343-450;
+   Save_Restart_udf resume.cxx:10-78), which is not part of the reference.
+   kapsel_udf_read parses a UDF file without it: the definition blocks
+   (\begin{def}, \begin{global_def}, files pulled in by \include) and every
+   \begin{data} block, each flattened into one record of `path = value`
+   entries with the paths the reference asks for
+   (constitutive_eq.Navier_Stokes.DX, object_type.spherical_particle.
+   Particle_spec[0].Particle_number, Particles[3].R.x, ...).  An input file
+   has one record; an Output_udf file one per snapshot.  Strings returned
+   stay valid until kapsel_udf_destroy. */
+typedef struct kapsel_udf kapsel_udf;
+int kapsel_udf_read(const char *path, kapsel_udf **out);
+int kapsel_udf_destroy(kapsel_udf *u);
+/* Number of records (data blocks). */
+int kapsel_udf_records(const kapsel_udf *u);
+/* Number of entries of a record; entry i in file order: its path, its
+   value as written (strings without their quotes) and whether it is a
+   string (select values are strings). */
+int kapsel_udf_size(const kapsel_udf *u, int record);
+int kapsel_udf_entry(const kapsel_udf *u, int record, int i, const char **path, const char **text, int *is_string);
+/* A numeric or string value by path (KAPSEL_EINVAL when absent). */
+int kapsel_udf_get_double(const kapsel_udf *u, int record, const char *path, double *value);
+int kapsel_udf_get_string(const kapsel_udf *u, int record, const char *path, const char **text);
+/* kapsel_params of an input file (record 0), one spherical-particle
+   species: the values Gourmet_file_io reads and the automatic time step of
+   Set_global_parameters (input.cxx:316-362).  With user_specify placement
+   the positions (n*3) and quaternions (n*4) go to x and q when they are not
+   NULL and *n_user is the particle count; otherwise *n_user is 0 (the
+   reference places them with rand(): the caller chooses positions).
+   KAPSEL_EINVAL for inputs the library does not model. */
+int kapsel_udf_to_params(const kapsel_udf *u, int precision, kapsel_params *p, double *x, double *q, int *n_user);
+
 /* ---- Host-only helpers (no GPU needed). ---- */
 
 /* n normals (n even) of the thermostat stream Add_random_force_thermostat

@@ -142,6 +142,64 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_DP)
 
 
+def read_udf_native(path: str) -> list:
+    """The records of a UDF file as the library's C++ reader flattens them
+    (kapsel_udf_read): a list of {path: value} dicts, one per data block;
+    numbers as float, strings (and select values) as str."""
+    L = load_library()
+    L.kapsel_udf_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(_VP)]
+    L.kapsel_udf_records.argtypes = [_VP]
+    L.kapsel_udf_size.argtypes = [_VP, ctypes.c_int]
+    L.kapsel_udf_entry.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                   ctypes.POINTER(ctypes.c_char_p), _IP]
+    L.kapsel_udf_destroy.argtypes = [_VP]
+    h = _VP()
+    rc = L.kapsel_udf_read(str(path).encode(), ctypes.byref(h))
+    if rc != 0:
+        raise KapselError(f"kapsel_udf_read({path}) status {rc}")
+    out = []
+    try:
+        for r in range(L.kapsel_udf_records(h)):
+            rec = {}
+            for i in range(L.kapsel_udf_size(h, r)):
+                pth, txt, iss = ctypes.c_char_p(), ctypes.c_char_p(), ctypes.c_int()
+                L.kapsel_udf_entry(h, r, i, ctypes.byref(pth), ctypes.byref(txt), ctypes.byref(iss))
+                t = txt.value.decode()
+                rec[pth.value.decode()] = t if iss.value else float(t)
+            out.append(rec)
+    finally:
+        L.kapsel_udf_destroy(h)
+    return out
+
+
+def params_from_udf_native(path: str, precision: int = FP64):
+    """(kapsel_params, x, q) from an input UDF through the C++ reader
+    (kapsel_udf_to_params); x, q are None unless the file places the
+    particles itself (user_specify)."""
+    L = load_library()
+    L.kapsel_udf_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(_VP)]
+    L.kapsel_udf_to_params.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(_Params), _DP, _DP, _IP]
+    L.kapsel_udf_get_double.argtypes = [_VP, ctypes.c_int, ctypes.c_char_p, _DP]
+    L.kapsel_udf_destroy.argtypes = [_VP]
+    h = _VP()
+    if L.kapsel_udf_read(str(path).encode(), ctypes.byref(h)) != 0:
+        raise KapselError(f"kapsel_udf_read({path}) failed")
+    try:
+        p = _Params()
+        nu = ctypes.c_int()
+        rc = L.kapsel_udf_to_params(h, precision, ctypes.byref(p), None, None, ctypes.byref(nu))
+        if rc != 0:
+            raise KapselError(f"kapsel_udf_to_params status {rc}")
+        x = q = None
+        if nu.value > 0:
+            x = np.zeros((nu.value, 3))
+            q = np.zeros((nu.value, 4))
+            L.kapsel_udf_to_params(h, precision, ctypes.byref(p), _ptr(x), _ptr(q), ctypes.byref(nu))
+        return p, x, q
+    finally:
+        L.kapsel_udf_destroy(h)
+
+
 def params_from_config(cfg: dict, precision: int = FP64) -> _Params:
     """Build kapsel_params from a configuration dict (the UDF values of one
     spherical-particle species; keys as in oracle/udf.py)."""

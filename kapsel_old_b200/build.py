@@ -14,8 +14,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libkapsel_gpu.so")
 
-SOURCES = [os.path.join(CSRC, "kapsel_gpu.cu")]
-DEPS = SOURCES + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
+SOURCES = [os.path.join(CSRC, "kapsel_gpu.cu"), os.path.join(CSRC, "udf_reader.cpp")]
+DEPS = SOURCES + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h", ".cpp"))] + [
     os.path.join(ROOT, "include", "kapsel_gpu.h")]
 
 NVCC_FLAGS = [

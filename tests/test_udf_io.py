@@ -174,3 +174,83 @@ def test_output_records_round_trip(tmp_path):
         for k, x in flat.items():
             assert float(b[k]) == float(x), k
     assert back[1]["Particles[1].R.x"] == 1 / 3
+
+
+# ---- the same checks through the library's C++ reader (kapsel_udf_*), the
+# path a C++ host without OCTA's UDFManager uses
+
+def _same_value(a, b):
+    if isinstance(a, str) or isinstance(b, str):
+        return a == b
+    return float(a) == float(b)
+
+
+def test_native_reader_matches_on_every_example():
+    import kapsel_old_b200 as kg
+    from kapsel_old_b200 import udf_io
+
+    n = 0
+    for p in _examples():
+        py = udf_io.read(p)
+        recs = kg.read_udf_native(p)
+        assert len(recs) == 1, p
+        cx = recs[0]
+        assert cx.keys() == py.keys(), (p, set(cx) ^ set(py))
+        for k in py:
+            assert _same_value(cx[k], py[k]), (p, k, cx[k], py[k])
+        n += 1
+    assert n >= 20
+    g = kg.read_udf_native(os.path.join(REF, "Examples", "02", "gravity.udf"))[0]
+    assert (g["mesh.NPX"], g["mesh.NPY"], g["mesh.NPZ"]) == (8, 8, 9)
+    assert g["gravity.G"] == 980.665 and g["gravity.G_direction"] == "-Z"
+
+
+def test_native_params_match_to_config(tmp_path):
+    import kapsel_old_b200 as kg
+    from kapsel_old_b200 import udf_io
+
+    checked = 0
+    for p in _examples():
+        flat = udf_io.read(p)
+        try:
+            cfg = udf_io.to_config(flat)
+        except udf_io.UDFError:
+            continue
+        prm, x, q = kg.params_from_udf_native(p)
+        ref = kg.params_from_config(cfg, kg.FP64)
+        for f, _ in kg._Params._fields_:
+            a, b = getattr(prm, f), getattr(ref, f)
+            if hasattr(a, "__len__"):
+                a, b = list(a), list(b)
+            if f == "dt":
+                assert abs(a - b) <= 1e-15 * b, (p, f, a, b)
+            else:
+                assert a == b, (p, f, a, b)
+        if x is not None:
+            assert np.array_equal(x, np.array([pp["x"] for pp in cfg["particles"]]))
+        checked += 1
+    assert checked >= 3
+
+
+def test_native_reader_reads_output_records(tmp_path):
+    import kapsel_old_b200 as kg
+    from kapsel_old_b200 import udf_io
+
+    d = tmp_path / "out_define.udf"
+    d.write_text(_OUT_DEFS)
+    v = lambda a, b, c: {"x": a, "y": b, "z": c}
+    part = lambda s: {"R": v(s, 2 * s, 3.5), "R_raw": v(s + 64, 2 * s, 3.5), "v": v(-s, 0.25, 1e-17),
+                      "q": {"q0": 1.0, "q1": 0.0, "q2": -0.0, "q3": 0.0}, "omega": v(0.0, s, 0.0),
+                      "f_hydro": v(1e5, -2.5e-300, 0.0), "torque_hydro": v(0.1, 0.2, 0.3), "f_r": v(0, 0, -7.0),
+                      "torque_r": v(0, 0, 0), "f_slip": v(0, 0, 0), "torque_slip": v(0, 0, 0)}
+    recs = [{"E": 1.0, "t": 0, "Particles": [part(1.0), part(2.0)]},
+            {"E": 1.0, "t": 100, "Particles": [part(0.125), part(1 / 3)]}]
+    path = tmp_path / "out.udf"
+    udf_io.write_records(str(path), recs, str(d))
+    back = kg.read_udf_native(str(path))
+    assert len(back) == 2
+    for r, b in zip(recs, back):
+        flat = udf_io.flatten(r)
+        assert set(flat) == set(b)
+        for k, x in flat.items():
+            assert float(b[k]) == float(x), k
