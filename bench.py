@@ -316,6 +316,7 @@ def run_ours(args, rank, world, local_rank):
             bms += e0.elapsed_time(e1)
         bms = reduce_max(bms, dist)
         msd = batch.msd()
+        chosen = batch.variants()
         batch.close()
         for sm_ in sims:
             sm_.close()
@@ -325,6 +326,8 @@ def run_ours(args, rank, world, local_rank):
             "grid_points_steps_per_s": round(kbat * world * pts / (bms * 1e-3), 1),
             "boxes": len(boxes), "particles": sum(len(c["particles"]) for c in boxes),
             "msd_mean": float(np.mean(msd)),
+            "autotune": [{"shape": list(v[:3]), "z_pass": ["warp", "block"][v[3]],
+                          "y_pass": ["warp", "block wide tile", "block narrow tile"][v[4]]} for v in chosen],
             "workload": "48 boxes from {32^3, 64^3, 64x64x128, 128^3}, 1-64 spheres a in [4,6], kBT=1e-3, mixed"}
         # learned near-contact correction: trained on the GPU from the committed
         # pair set (method runs at a=5 and a=10), then the 256^3 / 2048-sphere

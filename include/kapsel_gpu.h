@@ -189,8 +189,9 @@ int kapsel_gpu_get_concentration(kapsel_ctx *ctx, double *conc);
    launch per step.  The reference runs each box as its own process (one
    main() per UDF); boxes keep their own parameters, particles and thermostat
    streams.  `boxes` must be initialised contexts at the same time step; the
-   batch does not own them.  With autotune != 0 the y-pass tile width is
-   chosen per box shape by timing both variants. */
+   batch does not own them.  With autotune != 0 the z- and y-pass variants
+   are chosen per box shape by timing whole steps of one box of the shape
+   with each variant on a copy of its state (the state is restored). */
 typedef struct kapsel_batch kapsel_batch;
 int kapsel_batch_create(kapsel_ctx *const *boxes, int n, int autotune, kapsel_batch **out);
 int kapsel_batch_step(kapsel_batch *b, int nsteps);
@@ -198,6 +199,15 @@ int kapsel_batch_step(kapsel_batch *b, int nsteps);
    kapsel_batch_create (the R_raw records of Output_udf, avs_output.cxx:361-363). */
 int kapsel_batch_msd(kapsel_batch *b, double *msd);
 int kapsel_batch_get_stream(kapsel_batch *b, void **stream);
+/* The autotuner's choice per box shape, 5 ints each (up to cap shapes):
+   NX, NY, NZ, the z-pass variant (0 warp-level line groups, 1 block-level
+   row tiles) and the y-pass variant (0 warp-level, 1 block-level wide kz
+   tile, 2 block-level narrow kz tile); returns the number of shapes. */
+int kapsel_batch_variants(kapsel_batch *b, int *out, int cap);
+/* Sets the pass variants (as above) of one Navier_Stokes context; results
+   are the same to roundoff, speed differs by shape.  KAPSEL_EINVAL for a
+   variant the shape does not allow. */
+int kapsel_gpu_set_pass_variant(kapsel_ctx *ctx, int zmode, int ymode);
 int kapsel_batch_destroy(kapsel_batch *b);
 
 /* ---- Routine-level entry points on host arrays (reference layouts). ---- */

@@ -468,6 +468,15 @@ class Batch:
         self.L.kapsel_batch_get_stream(self.h, ctypes.byref(sp))
         return sp.value
 
+    def variants(self) -> list:
+        """The autotuner's choice per box shape: (NX, NY, NZ, z variant,
+        y variant); z 0 warp-level / 1 block-level, y 0 warp-level /
+        1 block-level wide tile / 2 block-level narrow tile."""
+        self.L.kapsel_batch_variants.argtypes = [_VP, _IP, ctypes.c_int]
+        buf = (ctypes.c_int * (5 * 64))()
+        n = self.L.kapsel_batch_variants(self.h, buf, 64)
+        return [tuple(buf[5 * i: 5 * i + 5]) for i in range(max(n, 0))]
+
     def close(self):
         if getattr(self, "h", None):
             self.L.kapsel_batch_destroy(self.h)

@@ -256,8 +256,13 @@ struct BoxBase {
   }
 
   virtual int alloc() = 0;
-  virtual float time_ypass(int small, int reps) = 0;
-  virtual void set_ytile(int small) = 0;
+  // pass variants of the batch autotuner: z passes warp-level (0) or
+  // block-level (1); y pass warp-level (0), block-level with the wide (1) or
+  // the narrow (2) kz tile.  time_variant runs `reps` steps of this box's
+  // workload with a variant on a copy of its state and restores the state.
+  virtual float time_variant(int zmode, int ymode, int reps) = 0;
+  virtual void set_variant(int zmode, int ymode) = 0;
+  virtual bool variant_ok(int zmode, int ymode) const = 0;
   virtual int alloc_el() = 0;
   virtual int alloc_obl() = 0;
   virtual int oblique_state(double *out) = 0;
@@ -528,11 +533,14 @@ struct Box : BoxBase {
       else if (g.NX == 128) rc = x_setup<7>();
       else if (g.NX == 256) rc = x_setup<8>();
       if (rc) return rc;
-      if (!zw_ok) rc = 0;
-      else if (g.NZ == 64) rc = zw_setup<5>();
+      if (g.NZ == 64) rc = zw_setup<5>();
       else if (g.NZ == 128) rc = zw_setup<6>();
       else if (g.NZ == 256) rc = zw_setup<7>();
       if (rc) return rc;
+      // warp-level z kernels by default only where they fill the GPU (the
+      // batch autotuner may choose otherwise per box shape)
+      zw_avail = zw;
+      if (!zw_ok) zw = 0;
     }
     KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
     KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xadv));
@@ -559,7 +567,6 @@ struct Box : BoxBase {
   dim3 gy(int nc) const { return dim3(g.NX, nc, (g.TZ + KCY - 1) / KCY); }
   // y-pass tile width: KCY, or KCY/2 when the autotuner found it faster for
   // this box shape (kapsel_batch_create)
-  int ytile_small = 0;
   bool use_pdl = true;
   // warp-level y pass: persistent grid of YNW-warp blocks, two slots per warp
   static constexpr int YNW = 4;
@@ -591,9 +598,11 @@ struct Box : BoxBase {
     else
       yw_launch<INV, LY, false>(gg, nc, in, out, pdl);
   }
+  int ymode = 0;   // y pass variant (time_variant)
+  int zw_avail = 0;  // warp-level z kernels set up for this NZ (their line-length log), else 0
   template <bool INV>
   void launch_y(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out, bool pdl = false) {
-    switch (gg.NY) {
+    if (ymode == 0) switch (gg.NY) {
       case 32: yw<INV, 5>(gg, nc, in, out, pdl); return;
       case 64: yw<INV, 6>(gg, nc, in, out, pdl); return;
       case 128: yw<INV, 7>(gg, nc, in, out, pdl); return;
@@ -602,7 +611,7 @@ struct Box : BoxBase {
     }
     constexpr int K2 = KCY / 2;
     const size_t sm = std::max(smem_y, sm_y_any);
-    if (ytile_small)
+    if (ymode == 2)
       launch_k(pdl, k_y_pass<R, INV, K2>, dim3(g.NX, nc, (gg.TZ + K2 - 1) / K2), dim3(256), sm, stream, gg, tw, in,
                out);
     else
@@ -610,27 +619,69 @@ struct Box : BoxBase {
                in, out);
   }
   size_t sm_y_any = 0;
-  float time_ypass(int small, int reps) override {
-    const int keep = ytile_small;
-    ytile_small = small;
+  bool variant_ok(int zmode, int ymode_) const override {
+    if (prm.eq != KAPSEL_EQ_NAVIER_STOKES || zmode < 0 || zmode > 1 || ymode_ < 0 || ymode_ > 2) return false;
+    if (zmode == 0 && !zw_avail) return false;
+    if (ymode_ == 0 && !(g.NY >= 32 && g.NY <= 256)) return false;
+    return true;
+  }
+  void set_variant(int zmode, int ymode_) override {
+    zw = zmode == 0 ? zw_avail : 0;
+    ymode = ymode_;
+    // the box's captured step graphs hold the previous launches
+    for (int s = 0; s < 2; ++s)
+      if (graph[s]) {
+        cudaGraphExecDestroy(graph[s]);
+        graph[s] = nullptr;
+      }
+  }
+  float time_variant(int zmode, int ymode_, int reps) override {
+    // a copy of the state the steps change (zeta, uk_dc, particles), restored
+    // afterwards; phi/up are all zero again after every step
+    const size_t nz = (size_t)g.KXc * g.KYc * g.TS;
+    Cx<R> *z0 = nullptr;
+    double *u0 = nullptr;
+    DPart *p0 = nullptr;
+    const int np1 = std::max(Np, 1);
+    if (cudaMalloc(&z0, sizeof(Cx<R>) * 2 * nz) != cudaSuccess || cudaMalloc(&u0, sizeof(double) * 3) != cudaSuccess ||
+        cudaMalloc(&p0, sizeof(DPart) * np1) != cudaSuccess) {
+      cudaFree(z0);
+      cudaFree(u0);
+      return -1.f;
+    }
+    cudaMemcpyAsync(z0, zeta, sizeof(Cx<R>) * 2 * nz, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(u0, uk_dc, sizeof(double) * 3, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(p0, parts, sizeof(DPart) * np1, cudaMemcpyDeviceToDevice, stream);
+    const int kz = zw, ky = ymode;
+    zw = zmode == 0 ? zw_avail : 0;
+    ymode = ymode_;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    launch_y<false>(g, 5, bufB, bufA);  // warm
+    u_spec_ready = false;
+    ensure_u_spec();
+    launch_step(noise_dev[0], 0);  // warm
     cudaEventRecord(a, stream);
-    for (int r = 0; r < reps; ++r) launch_y<false>(g, 5, bufB, bufA);
+    for (int r = 0; r < reps; ++r) launch_step(noise_dev[0], 0);
     cudaEventRecord(b, stream);
     cudaEventSynchronize(b);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, a, b);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    ytile_small = keep;
-    // the timed passes wrote bufA: it no longer holds u_k of the current zeta
+    zw = kz;
+    ymode = ky;
+    cudaMemcpyAsync(zeta, z0, sizeof(Cx<R>) * 2 * nz, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(uk_dc, u0, sizeof(double) * 3, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(parts, p0, sizeof(DPart) * np1, cudaMemcpyDeviceToDevice, stream);
+    cudaStreamSynchronize(stream);
+    cudaFree(z0);
+    cudaFree(u0);
+    cudaFree(p0);
+    // the timed steps overwrote bufA: it no longer holds u_k of the current zeta
     u_spec_ready = false;
     return ms / reps;
   }
-  void set_ytile(int small) override { ytile_small = small; }
   int gz() const { return (g.NX * g.NY) / ZROWS; }
 
   // zeta -> u* (real) through launches 1,2,(7); used by the velocity readout
@@ -1590,7 +1641,13 @@ void BoxBase::launch_nearcontact() {
   io.frames = nc_frames;
   io.corr = nc_corr;
   io.sc = nc->sc;
-  nc::k_mlp_tile<false><<<(nc_cap + nc::TILE - 1) / nc::TILE, 128, nc::SMEM_ALLOC, stream>>>(nc->params, io);
+  // a persistent grid of one CTA per SM walks the tiles of however many
+  // pairs the search found (the count is on the device)
+  int nsm = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int tiles = (nc_cap + nc::TILE - 1) / nc::TILE;
+  nc::k_mlp_tile<false><<<std::min(tiles, std::max(nsm, 1)), 128, nc::SMEM_ALLOC, stream>>>(nc->params, io);
 }
 
 struct kapsel_ctx {
@@ -2339,6 +2396,8 @@ struct kapsel_batch {
   cudaEvent_t fork = nullptr, done = nullptr;
   std::vector<cudaEvent_t> ready, join;
   std::vector<std::vector<double>> x0;
+  // the autotuner's choices: NX, NY, NZ, z variant, y variant per shape
+  std::vector<std::vector<int>> variants;
 };
 
 extern "C" {
@@ -2362,22 +2421,33 @@ int kapsel_batch_create(kapsel_ctx *const *boxes, int n, int autotune, kapsel_ba
     if (cudaEventCreateWithFlags(&b->ready[i], cudaEventDisableTiming) != cudaSuccess) return KAPSEL_ECUDA;
     if (cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) != cudaSuccess) return KAPSEL_ECUDA;
   }
-  // autotune: the y-pass tile width per box shape, by timing both variants
+  // autotune: per box shape (and precision, particle count class), the z and
+  // y pass variants, by timing whole steps of the first box of that shape on
+  // a copy of its state
   if (autotune) {
-    std::vector<std::pair<std::vector<int>, int>> chosen;
+    std::vector<std::pair<std::vector<int>, std::pair<int, int>>> chosen;
     for (int i = 0; i < n; ++i) {
       BoxBase *x = b->boxes[i]->box.get();
-      std::vector<int> key = {x->g.NX, x->g.NY, x->g.NZ, x->prm.precision};
-      int pick = -1;
+      if (x->prm.eq != KAPSEL_EQ_NAVIER_STOKES || x->Np == 0) continue;
+      std::vector<int> key = {x->g.NX, x->g.NY, x->g.NZ, x->prm.precision, x->Np > 1024 ? 1 : 0};
+      int zp = -1, yp = -1;
       for (auto &c : chosen)
-        if (c.first == key) pick = c.second;
-      if (pick < 0) {
-        const float t0 = x->time_ypass(0, 10), t1 = x->time_ypass(1, 10);
-        pick = t1 < t0 ? 1 : 0;
-        chosen.push_back({key, pick});
+        if (c.first == key) zp = c.second.first, yp = c.second.second;
+      if (zp < 0) {
+        float best = 0.f;
+        for (int zm = 0; zm < 2; ++zm)
+          for (int ym = 0; ym < 3; ++ym) {
+            if (!x->variant_ok(zm, ym)) continue;
+            const float t = x->time_variant(zm, ym, 5);
+            if (t > 0.f && (zp < 0 || t < best)) best = t, zp = zm, yp = ym;
+          }
+        if (zp < 0) continue;
+        chosen.push_back({key, {zp, yp}});
       }
-      x->set_ytile(pick);
+      x->set_variant(zp, yp);
     }
+    b->variants.clear();
+    for (auto &c : chosen) b->variants.push_back({c.first[0], c.first[1], c.first[2], c.second.first, c.second.second});
   }
   // initial unwrapped positions for the mean-square displacement
   for (int i = 0; i < n; ++i) {
@@ -2473,6 +2543,24 @@ int kapsel_batch_msd(kapsel_batch *b, double *msd) {
     msd[i] = x->Np > 0 ? acc / x->Np : 0.0;
   }
   return 0;
+}
+
+int kapsel_gpu_set_pass_variant(kapsel_ctx *ctx, int zmode, int ymode) {
+  if (!ctx) return KAPSEL_EINVAL;
+  BoxBase *x = ctx->box.get();
+  if (!x->variant_ok(zmode, ymode)) return KAPSEL_EINVAL;
+  if (cudaStreamSynchronize(x->stream) != cudaSuccess) return KAPSEL_ECUDA;
+  x->set_variant(zmode, ymode);
+  x->u_spec_ready = false;
+  return 0;
+}
+
+int kapsel_batch_variants(kapsel_batch *b, int *out, int cap) {
+  if (!b || cap < 0 || (cap > 0 && !out)) return KAPSEL_EINVAL;
+  const int n = (int)b->variants.size();
+  for (int i = 0; i < n && i < cap; ++i)
+    for (int k = 0; k < 5; ++k) out[5 * i + k] = b->variants[i][k];
+  return n;
 }
 
 int kapsel_batch_get_stream(kapsel_batch *b, void **stream) {

@@ -238,8 +238,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tile(const float *__restrict__ p
   extern __shared__ __align__(128) unsigned char sm[];
   const int t = threadIdx.x, w = t >> 5;
   const int n = io.n >= 0 ? io.n : min(*io.n_dev, io.n_cap);
-  const int row0 = blockIdx.x * TILE;
-  if (row0 >= n) return;
+  if (blockIdx.x * TILE >= n) return;
   const uint32_t sm0 = smem_u32(sm);
   const uint32_t bar = sm0 + S_BAR;
   float *sb = reinterpret_cast<float *>(sm + S_B);
@@ -254,15 +253,6 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tile(const float *__restrict__ p
     const int off = i < HID ? OB1 + i : i < 2 * HID ? OB2 + i - HID : i < 3 * HID ? OB3 + i - 2 * HID : OB4 + i - 3 * HID;
     sb[i] = params[off];
     sdb[i] = 0.f;
-  }
-  const int row = row0 + t;
-  const bool valid = row < n;
-  const int src = valid ? (io.idx ? io.idx[row] : row) : 0;
-  {
-    float xv[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) xv[i] = valid ? io.x[(size_t)src * IN + i] : 0.f;
-    st_row16(sm, S_X, t, 0, IN, xv);
   }
   if (t == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
@@ -311,6 +301,23 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tile(const float *__restrict__ p
       st_row16(sm, dst, t, c0, HID, v);
     }
   };
+
+  // The CTA loops over row tiles (a grid smaller than the tile count keeps
+  // the weights and the tensor memory of one CTA for several tiles): the
+  // previous tile's MMAs and tensor-memory reads have all completed when the
+  // next tile's input is staged.
+  for (int tile = blockIdx.x; ok && tile * TILE < n; tile += gridDim.x) {
+  const int row0 = tile * TILE;
+  const int row = row0 + t;
+  const bool valid = row < n;
+  const int src = valid ? (io.idx ? io.idx[row] : row) : 0;
+  {
+    float xv[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) xv[i] = valid ? io.x[(size_t)src * IN + i] : 0.f;
+    st_row16(sm, S_X, t, 0, IN, xv);
+  }
+  to_mma();
 
   // ---- forward
   if (t == 0) { tc_fence_after(); gemm(tm + 0, sm0, S_X, IN, false, S_W1, IN, false, 128, HID, IN); }
@@ -431,8 +438,11 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tile(const float *__restrict__ p
         const int off =
             i < HID ? OB1 + i : i < 2 * HID ? OB2 + i - HID : i < 3 * HID ? OB3 + i - 2 * HID : OB4 + i - 3 * HID;
         atomicAdd(io.grad + off, sdb[i]);
+        sdb[i] = 0.f;
       }
+    __syncthreads();
   }
+  }  // tiles
 
   if (!ok && t == 0) atomicExch(io.status, NC_ETIMEOUT);
   tc_fence_before();
@@ -457,22 +467,34 @@ __global__ void __launch_bounds__(128) k_nc_pairs(PPar p, const DPart *__restric
   // range) or all later particles
   const int *lst = p.nbl ? p.nbl + (size_t)i * (NBL_MAX + 1) : nullptr;
   const int ncand = lst ? lst[0] : p.Np - i - 1;
-  for (int t = threadIdx.x; t < ncand; t += blockDim.x) {
-    const int j = lst ? lst[1 + t] : i + 1 + t;
-    if (j <= i) continue;
-    const DPart &b = parts[j];
-    double d[3];
-    for (int k = 0; k < 3; ++k) {
-      d[k] = b.x[k] - a.x[k];
-      d[k] -= nint_d(d[k] * p.invL[k]) * p.L[k];
+  const int lane = threadIdx.x & 31;
+  // every lane of a warp takes the same number of turns, so that the pairs a
+  // warp finds take their slots with one atomic per warp
+  for (int base = 0; base < ncand; base += blockDim.x) {
+    const int t = base + threadIdx.x;
+    const int j = t < ncand ? (lst ? lst[1 + t] : i + 1 + t) : -1;
+    double d[3], gap = -1.0;
+    bool keep = false;
+    if (j > i) {
+      const DPart &b = parts[j];
+      for (int k = 0; k < 3; ++k) {
+        d[k] = b.x[k] - a.x[k];
+        d[k] -= nint_d(d[k] * p.invL[k]) * p.L[k];
+      }
+      gap = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) - 2.0 * p.RADIUS;
+      keep = gap >= lo && gap <= hi;
     }
-    const double gap = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) - 2.0 * p.RADIUS;
-    if (!(gap >= lo && gap <= hi)) continue;
-    const int s = atomicAdd(count, 1);
+    const unsigned found = __ballot_sync(0xffffffffu, keep);
+    int first = 0;
+    if (lane == 0 && found) first = atomicAdd(count, __popc(found));
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (!keep) continue;
+    const int s = first + __popc(found & ((1u << lane) - 1u));
     if (s >= cap) {
       atomicExch(status, -6);
       continue;
     }
+    const DPart &b = parts[j];
     double e[9];
     nc_frame(d, e);
     nc_features(sc, gap, e, a.v, b.v, a.omega, b.omega, feat + (size_t)s * IN);

@@ -79,3 +79,31 @@ def test_batch_autotune_after_stepping_matches_single_boxes():
         assert rel(bs.zeta(), ss.zeta()) < 1e-12
         assert rel(bs.particles()["v"], ss.particles()["v"]) < 1e-12
     b.close()
+
+
+def test_batch_pass_variants_match():
+    """Every z / y pass variant the autotuner may choose gives the same step
+    (FP64, to roundoff) as the default one, on a box whose shape allows all
+    of them (64x64x128)."""
+    import kapsel_old_b200 as kg
+
+    cfg = udf.ns_config((6, 6, 7), 5, seed=24, a=5.0, kbt=1e-3)
+    ref = kg.Simulation(cfg, precision=kg.FP64)
+    ref.step(4)
+    for zmode in (0, 1):
+        for ymode in (0, 1, 2):
+            s = kg.Simulation(cfg, precision=kg.FP64)
+            _set_variant(s, zmode, ymode)
+            s.step(4)
+            assert rel(s.zeta(), ref.zeta()) < 1e-12, (zmode, ymode)
+            assert rel(s.particles()["v"], ref.particles()["v"]) < 1e-12, (zmode, ymode)
+            s.close()
+    ref.close()
+
+
+def _set_variant(sim, zmode, ymode):
+    import ctypes
+
+    fn = sim.L.kapsel_gpu_set_pass_variant
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    assert fn(sim.h, zmode, ymode) == 0

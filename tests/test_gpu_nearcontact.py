@@ -58,6 +58,7 @@ def test_network_forward_matches_oracle(n):
     y = net.forward(x)
     ref, _, _ = mlp.forward(p, x, "bf16")
     scale = np.abs(ref).max()
+    print(f"forward n={n}: max |y-ref|/scale {np.abs(y - ref).max() / scale:.2e}, rel L2 {rel(y, ref):.2e}")
     assert np.abs(y - ref).max() <= 2e-2 * scale, (np.abs(y - ref).max(), scale)
     # and the exact network within bf16 accuracy
     ref64, _, _ = mlp.forward(p.astype(np.float64), x.astype(np.float64), "fp64")
@@ -76,6 +77,8 @@ def test_network_gradient_matches_oracle(n):
     gr, lr = mlp.gradient(p, x, y, w, "bf16")
     assert abs(loss - lr) <= 1e-3 * abs(lr)
     G, R = mlp.unpack(g), mlp.unpack(gr)
+    print(f"gradient n={n}: loss rel {abs(loss - lr) / abs(lr):.2e}, " + ", ".join(
+        f"{k} {np.linalg.norm(G[k] - R[k]) / np.linalg.norm(R[k]):.2e}" for k in R))
     for k in R:
         e = np.linalg.norm(G[k] - R[k]) / np.linalg.norm(R[k])
         assert e < 3e-2, (k, e)
