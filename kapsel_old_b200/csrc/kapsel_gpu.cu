@@ -326,6 +326,20 @@ struct BoxBase {
   DPart *parts_host = nullptr;  // pinned staging of the particle readout
 };
 
+// threads per block of the x passes of the Navier-Stokes step (multiples of
+// 32 up to 256); the block-level transforms divide their work over them
+#ifndef KAPSEL_XZ_THREADS
+#define KAPSEL_XZ_THREADS 256
+#endif
+#ifndef KAPSEL_XADV_THREADS
+#define KAPSEL_XADV_THREADS 256
+#endif
+#ifndef KAPSEL_XFORCE_THREADS
+#define KAPSEL_XFORCE_THREADS 256
+#endif
+constexpr int kXZThreads = KAPSEL_XZ_THREADS, kXAdvThreads = KAPSEL_XADV_THREADS,
+              kXForceThreads = KAPSEL_XFORCE_THREADS;
+
 template <typename R>
 struct Box : BoxBase {
   Cx<R> *zeta = nullptr;  // [2][KXc][KYc][TS]
@@ -356,15 +370,15 @@ struct Box : BoxBase {
   }
   template <int LX>
   void xz_l(bool pdl, const Cx<R> *z, const double *u, Cx<R> *out) {
-    launch_k(pdl, k_x_zeta_to_u<R, KCX, LX>, gx(), dim3(256), smem_xu, stream, g, tw, z, u, out);
+    launch_k(pdl, k_x_zeta_to_u<R, KCX, LX>, gx(), dim3(kXZThreads), smem_xu, stream, g, tw, z, u, out);
   }
   template <int EU, int LX>
   void xa_l(bool pdl) {
-    launch_k(pdl, k_x_advect_update<R, KCX, EU, LX>, gx(), dim3(256), smem_xadv, stream, g, tw, bufA, zeta, uk_dc);
+    launch_k(pdl, k_x_advect_update<R, KCX, EU, LX>, gx(), dim3(kXAdvThreads), smem_xadv, stream, g, tw, bufA, zeta, uk_dc);
   }
   template <int LX, int NEXTU = 0>
   void xf_l(bool pdl, Cx<R> *in) {
-    launch_k(pdl, k_x_force_to_zeta<R, KCX, LX, NEXTU>, gx(), dim3(256), smem_xf, stream, g, tw, in, zeta, uk_dc);
+    launch_k(pdl, k_x_force_to_zeta<R, KCX, LX, NEXTU>, gx(), dim3(kXForceThreads), smem_xf, stream, g, tw, in, zeta, uk_dc);
   }
   void x_zeta(bool pdl, const Cx<R> *z, const double *u, Cx<R> *out) {
     switch (g.NX) {
@@ -577,7 +591,7 @@ struct Box : BoxBase {
   void yw_launch(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out, bool pdl) {
     using Y = ZL<LY>;
     auto kern = k_yw_pass<R, INV, LY, FULL, YNW, YSLOTS>;
-    const size_t sm = sizeof(Cx<R>) * YSLOTS * Y::RW * Y::LS * YNW;
+    const size_t sm = sizeof(Cx<R>) * YSLOTS * Y::RW * YLines<R, LY>::LS * YNW;
     int &occ = yw_occ[INV ? 1 : 0][FULL ? 1 : 0];
     if (!occ) {
       int dev = 0;

@@ -41,6 +41,28 @@ __device__ __forceinline__ int zpos(int j) {
   return j + (j >> ZL<LM>::L2);
 }
 
+// Placement of the RW lines of a warp batch in shared memory: line l starts
+// at base(l).  The z passes use l*LS.  The y pass uses a stride and an order
+// of the lines chosen for its element size so that its strided gather and
+// scatter (four kz columns of consecutive rows per half warp) and the
+// transform phases hit distinct banks (a search over strides and orders,
+// counting wavefronts of every access of the pass: 268 -> 219 per work item
+// for 128-point float lines, 684 -> 368 for double).
+struct ZLines {
+  template <int LM>
+  __device__ __forceinline__ static int base(int l) { return l * ZL<LM>::LS; }
+};
+template <typename R, int LY>
+struct YLines {
+  static constexpr bool F = sizeof(R) == 4;
+  static constexpr int LS = LY == 6 ? (F ? 76 : 74) : LY == 7 ? (F ? 148 : 146) : LY == 8 ? (F ? 280 : 276)
+                                                                                        : ZL<LY>::LS;
+  // line order as 4-bit fields: (1,3,2,0) for float, (3,2,1,0) for double
+  static constexpr unsigned PERM = (LY == 6 || LY == 7) ? (F ? 0x0231u : 0x0123u) : 0x76543210u;
+  template <int LM>
+  __device__ __forceinline__ static int base(int l) { return (int)((PERM >> (4 * l)) & 15u) * LS; }
+};
+
 // Phase-1 twiddles of this lane: w_M^(SIGN t k1), t = lane mod N2.
 template <typename R, int LM, int SIGN>
 __device__ __forceinline__ void wfft_twiddles(const Cx<R> *__restrict__ twm, Cx<R> (&w)[ZL<LM>::N1]) {
@@ -51,13 +73,13 @@ __device__ __forceinline__ void wfft_twiddles(const Cx<R> *__restrict__ twm, Cx<
 
 // In-place transform of RW lines (line l at buf + l*LS, padded layout),
 // natural order in and out; ends with __syncwarp.
-template <typename R, int LM, int SIGN>
+template <typename R, int LM, int SIGN, typename LB = ZLines>
 __device__ __forceinline__ void wfft(Cx<R> *buf, const Cx<R> (&w)[ZL<LM>::N1]) {
   using Z = ZL<LM>;
   const int lane = threadIdx.x & 31;
   {
     const int l = lane >> Z::L2, t = lane & (Z::N2 - 1);
-    Cx<R> *p = buf + l * Z::LS + t;
+    Cx<R> *p = buf + LB::template base<LM>(l) + t;
     Cx<R> v[Z::N1];
 #pragma unroll
     for (int n1 = 0; n1 < Z::N1; ++n1) v[n1] = p[n1 * (Z::N2 + 1)];
@@ -72,7 +94,7 @@ __device__ __forceinline__ void wfft(Cx<R> *buf, const Cx<R> (&w)[ZL<LM>::N1]) {
 #pragma unroll
   for (int q = 0; q < Z::IT2; ++q) {
     const int i = lane + 32 * q, l = i >> Z::L1, k1 = i & (Z::N1 - 1);
-    const Cx<R> *p = buf + l * Z::LS + k1 * (Z::N2 + 1);
+    const Cx<R> *p = buf + LB::template base<LM>(l) + k1 * (Z::N2 + 1);
 #pragma unroll
     for (int n2 = 0; n2 < Z::N2; ++n2) y[q][n2] = p[n2];
   }
@@ -81,7 +103,7 @@ __device__ __forceinline__ void wfft(Cx<R> *buf, const Cx<R> (&w)[ZL<LM>::N1]) {
   for (int q = 0; q < Z::IT2; ++q) {
     const int i = lane + 32 * q, l = i >> Z::L1, k1 = i & (Z::N1 - 1);
     dft_small<R, SIGN>(y[q], Z::N2);
-    Cx<R> *p = buf + l * Z::LS;
+    Cx<R> *p = buf + LB::template base<LM>(l);
 #pragma unroll
     for (int k2 = 0; k2 < Z::N2; ++k2) p[zpos<LM>(k1 + Z::N1 * k2)] = y[q][k2];
   }
@@ -412,21 +434,33 @@ __global__ void __launch_bounds__(NW * 32) k_zw_force(Geo g, Twiddles<R> tw, R *
   const size_t rows = (size_t)g.NX * g.NY;
   const size_t npts = rows * Z::NZ;
   const int ngroups = (int)(rows / Z::RW);
-  constexpr int NI = Z::RW * Z::M / 32;  // element pairs per lane, one at a time (7 loads in flight)
+  constexpr int NI = Z::RW * Z::M / 32;  // element pairs per lane
   for (int grp = blockIdx.x * NW + warp; grp < ngroups; grp += gridDim.x * NW) {
     const size_t row0 = (size_t)grp * Z::RW;
+    // phi first, all of the lane's element pairs at once: where phi is zero
+    // up is zero too and f = up - phi u* = 0, so up and u* are read only
+    // where a particle's profile reaches (about an eighth of the points at
+    // a solid fraction of 0.14); the rest of the pass is unchanged
+    V2 ph[NI];
+#pragma unroll
+    for (int h = 0; h < NI; ++h)
+      ph[h] = *reinterpret_cast<const V2 *>(phiup + row0 * Z::NZ + 2 * (size_t)(lane + 32 * h));
 #pragma unroll 1
     for (int h = 0; h < NI; ++h) {
       const int i = lane + 32 * h;
       const size_t o = row0 * Z::NZ + 2 * (size_t)i;
-      const V2 ph = *reinterpret_cast<const V2 *>(phiup + o);
       V2 up[3], us[3];
+      if (ph[h].x != R(0) || ph[h].y != R(0)) {
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        up[d] = *reinterpret_cast<const V2 *>(phiup + (1 + d) * npts + o);
-        us[d] = *reinterpret_cast<const V2 *>(ustar + d * npts + o);
+        for (int d = 0; d < 3; ++d) {
+          up[d] = *reinterpret_cast<const V2 *>(phiup + (1 + d) * npts + o);
+          us[d] = *reinterpret_cast<const V2 *>(ustar + d * npts + o);
+        }
+      } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) up[d] = us[d] = V2{R(0), R(0)};
       }
-      zw_force_item<R, LM>(buf, phiup, npts, row0, i, ph, up, us);
+      zw_force_item<R, LM>(buf, phiup, npts, row0, i, ph[h], up, us);
     }
     __syncwarp();
 #pragma unroll
@@ -459,6 +493,7 @@ template <typename R, bool INVERSE, int LY, bool FULLY>
 __device__ __forceinline__ void yw_issue(const Geo &g, const Cx<R> *__restrict__ in, Cx<R> *slot, int item,
                                          int nbatch) {
   using Y = ZL<LY>;
+  using YL = YLines<R, LY>;
   constexpr int RW = Y::RW, NY = Y::M;
   constexpr int TYc = FULLY ? NY / 2 + 1 : (NY + 2) / 3, KYc = FULLY ? NY : 2 * TYc - 1;
   constexpr int RIN = INVERSE ? KYc : NY;
@@ -470,7 +505,7 @@ __device__ __forceinline__ void yw_issue(const Geo &g, const Cx<R> *__restrict__
   for (int i = lane; i < RIN * RW; i += 32) {
     const int r = i >> Y::LR, col = i & (RW - 1);
     const int j = INVERSE ? (r < TYc ? r : NY + r - KYc) : r;
-    Cx<R> *d = slot + col * Y::LS + zpos<LY>(j);
+    Cx<R> *d = slot + YL::template base<LY>(col) + zpos<LY>(j);
     if (col < ncols)
       cp_async_cx(d, src + (size_t)r * g.TS + col);
     else
@@ -479,15 +514,20 @@ __device__ __forceinline__ void yw_issue(const Geo &g, const Cx<R> *__restrict__
   if (INVERSE)
     for (int i = lane; i < (NY - KYc) * RW; i += 32) {
       const int j = TYc + (i >> Y::LR), col = i & (RW - 1);
-      slot[col * Y::LS + zpos<LY>(j)] = zero;
+      slot[YL::template base<LY>(col) + zpos<LY>(j)] = zero;
     }
 }
 
+// blocks of the y pass resident per SM that the register budget must allow
+#ifndef KAPSEL_YW_MINB
+#define KAPSEL_YW_MINB 1
+#endif
 template <typename R, bool INVERSE, int LY, bool FULLY, int NW, int NSLOT>
-__global__ void __launch_bounds__(NW * 32) k_yw_pass(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
+__global__ void __launch_bounds__(NW * 32, KAPSEL_YW_MINB) k_yw_pass(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
                                                      Cx<R> *__restrict__ out, int ncomp) {
   using Y = ZL<LY>;
-  constexpr int RW = Y::RW, NY = Y::M, SLOT = RW * Y::LS;
+  using YL = YLines<R, LY>;
+  constexpr int RW = Y::RW, NY = Y::M, SLOT = RW * YL::LS;
   static_assert(NSLOT == 1 || NSLOT == 2, "slots");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_begin();
@@ -515,14 +555,14 @@ __global__ void __launch_bounds__(NW * 32) k_yw_pass(Geo g, Twiddles<R> tw, cons
       cp_async_wait_all();
     }
     __syncwarp();
-    wfft<R, LY, INVERSE ? -1 : 1>(cur, w);
+    wfft<R, LY, INVERSE ? -1 : 1, YL>(cur, w);
     const int batch = item % nbatch, plane = item / nbatch;
     const int col0 = batch * RW, ncols = min(RW, g.TZ - col0);
     Cx<R> *dst = out + (size_t)plane * rows_out * g.TS + col0;
     for (int i = lane; i < rows_out * RW; i += 32) {
       const int r = i >> Y::LR, col = i & (RW - 1);
       const int j = INVERSE ? r : full_from_compact(r, g.TY, g.KYc, NY);
-      if (col < ncols) dst[(size_t)r * g.TS + col] = cur[col * Y::LS + zpos<LY>(j)];
+      if (col < ncols) dst[(size_t)r * g.TS + col] = cur[YL::template base<LY>(col) + zpos<LY>(j)];
     }
     __syncwarp();
   }
