@@ -304,34 +304,54 @@ __global__ void __launch_bounds__(1024) k_particles_hydro_velocity(PPar p, DPart
     const float resf[3] = {(float)b.res[0], (float)b.res[1], (float)b.res[2]};
     const float vpf[3] = {(float)vp[0], (float)vp[1], (float)vp[2]};
     const float wpf[3] = {(float)wp[0], (float)wp[1], (float)wp[2]};
-#pragma unroll 2
-    for (int m = first; m < p.S; m += stride) {
-      const int *cell = cells + 3 * m;
-      int rm[3];
-      float r[3];
+    // GB of the thread's points at a time: their geometry and phi first,
+    // then all their velocity loads, then the sums (in the same point
+    // order), so that the scattered loads of a batch are in flight together
+    constexpr int GB = 4;
+    for (int m0 = first; m0 < p.S; m0 += GB * stride) {
+      float ph[GB], r[GB][3];
+      size_t im[GB];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);
-      const float ph = prof_phi_f(offset_f(cell, resf, dxf, r), rpf, rmf, dxf);
-      // phi is exactly zero beyond a + xi/2 (about half of the Sekibun
-      // points): those terms add zeros, so their loads are skipped
-      if (ph == 0.f) continue;
-      const size_t im = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
-      const float ug[3] = {(float)__ldg(u + im), (float)__ldg(u + npts + im), (float)__ldg(u + 2 * npts + im)};
-      float vr[3] = {0.f, 0.f, 0.f};
-      if (p.rotation) {
-        vr[0] = wpf[1] * r[2] - wpf[2] * r[1];
-        vr[1] = wpf[2] * r[0] - wpf[0] * r[2];
-        vr[2] = wpf[0] * r[1] - wpf[1] * r[0];
-      }
-      float fp[3];
+      for (int k = 0; k < GB; ++k) {
+        const int m = m0 + k * stride;
+        ph[k] = 0.f;
+        im[k] = 0;
+        if (m < p.S) {
+          const int *cell = cells + 3 * m;
+          int rm[3];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        fp[d] = ((vpf[d] + vr[d]) - ug[d]) * ph;
-        f6[d] += fp[d];
+          for (int d = 0; d < 3; ++d) rm[d] = (b.xi[d] + cell[d] + p.N[d]) & (p.N[d] - 1);
+          // phi is exactly zero beyond a + xi/2 (about half of the Sekibun
+          // points): those terms add zeros, so their loads are skipped
+          ph[k] = prof_phi_f(offset_f(cell, resf, dxf, r[k]), rpf, rmf, dxf);
+          im[k] = ((size_t)rm[0] * p.N[1] + rm[1]) * p.N[2] + rm[2];
+        }
       }
-      f6[3] += r[1] * fp[2] - r[2] * fp[1];
-      f6[4] += r[2] * fp[0] - r[0] * fp[2];
-      f6[5] += r[0] * fp[1] - r[1] * fp[0];
+      float ug[GB][3];
+#pragma unroll
+      for (int k = 0; k < GB; ++k)
+        if (ph[k] != 0.f)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) ug[k][d] = (float)__ldg(u + d * npts + im[k]);
+#pragma unroll
+      for (int k = 0; k < GB; ++k) {
+        if (ph[k] == 0.f) continue;
+        float vr[3] = {0.f, 0.f, 0.f};
+        if (p.rotation) {
+          vr[0] = wpf[1] * r[k][2] - wpf[2] * r[k][1];
+          vr[1] = wpf[2] * r[k][0] - wpf[0] * r[k][2];
+          vr[2] = wpf[0] * r[k][1] - wpf[1] * r[k][0];
+        }
+        float fp[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          fp[d] = ((vpf[d] + vr[d]) - ug[k][d]) * ph[k];
+          f6[d] += fp[d];
+        }
+        f6[3] += r[k][1] * fp[2] - r[k][2] * fp[1];
+        f6[4] += r[k][2] * fp[0] - r[k][0] * fp[2];
+        f6[5] += r[k][0] * fp[1] - r[k][1] * fp[0];
+      }
     }
   } else
   for (int m = first; m < p.S; m += stride) {

@@ -4,10 +4,12 @@ resistance mode against the SPM oracle, the per-step correction hook, and
 the gain of the trained network over the plain method on the committed pair
 set (tests/golden/nearcontact_pairs.npz, generated by make_nearcontact.py).
 
-Tolerances: network output within 2e-2 of the output scale and gradients
-within 3e-2 relative L2 per tensor against the bf16-emulating oracle (the
-kernels sum in a different order and may round an activation to the other
-bf16 neighbour); frozen-mode forces <= 1e-10 relative (FP64 path).
+Tolerances: network output within 5e-4 of the output scale (1e-4
+relative L2) and gradients within 1e-3 relative L2 per tensor (loss 1e-5)
+against the bf16-emulating oracle, about ten times the differences
+measured on B200 (the kernels sum in a different order and may round an
+activation to the other bf16 neighbour); frozen-mode forces <= 1e-10
+relative (FP64 path).
 """
 import os
 
@@ -58,8 +60,9 @@ def test_network_forward_matches_oracle(n):
     y = net.forward(x)
     ref, _, _ = mlp.forward(p, x, "bf16")
     scale = np.abs(ref).max()
-    print(f"forward n={n}: max |y-ref|/scale {np.abs(y - ref).max() / scale:.2e}, rel L2 {rel(y, ref):.2e}")
-    assert np.abs(y - ref).max() <= 2e-2 * scale, (np.abs(y - ref).max(), scale)
+    # measured on B200: max 4e-5 of the scale, rel L2 1.3e-5 (n=300)
+    assert np.abs(y - ref).max() <= 5e-4 * scale, (np.abs(y - ref).max(), scale)
+    assert rel(y, ref) <= 1e-4, rel(y, ref)
     # and the exact network within bf16 accuracy
     ref64, _, _ = mlp.forward(p.astype(np.float64), x.astype(np.float64), "fp64")
     assert np.abs(y - ref64).max() <= 5e-2 * np.abs(ref64).max()
@@ -75,13 +78,12 @@ def test_network_gradient_matches_oracle(n):
     net = _net(p)
     g, loss = net.gradient(x, y, w)
     gr, lr = mlp.gradient(p, x, y, w, "bf16")
-    assert abs(loss - lr) <= 1e-3 * abs(lr)
+    # measured on B200: loss 1e-7 relative, gradients <= 8.5e-5 relative L2
+    assert abs(loss - lr) <= 1e-5 * abs(lr)
     G, R = mlp.unpack(g), mlp.unpack(gr)
-    print(f"gradient n={n}: loss rel {abs(loss - lr) / abs(lr):.2e}, " + ", ".join(
-        f"{k} {np.linalg.norm(G[k] - R[k]) / np.linalg.norm(R[k]):.2e}" for k in R))
     for k in R:
         e = np.linalg.norm(G[k] - R[k]) / np.linalg.norm(R[k])
-        assert e < 3e-2, (k, e)
+        assert e < 1e-3, (k, e)
     # rows 12..15 carry no loss: no gradient on their weights
     assert np.all(G["W4"][12:] == 0) and np.all(G["b4"][12:] == 0)
 
