@@ -198,6 +198,10 @@ struct BoxBase {
   // per-step cell and neighbour lists (cell_kernels.cuh); pp.nbl points at
   // the lists while they are on
   bool cl_on = false;
+  // overlap candidates of each particle as bit words ([Np][32]), written by
+  // the gather for the scatter of the same step (at most 1024 particles,
+  // without neighbour lists); null otherwise
+  unsigned *ovl = nullptr;
   CellPar clp{};
   int *cl_count = nullptr, *cl_start = nullptr, *cl_cursor = nullptr, *cl_list = nullptr, *cl_cellof = nullptr;
   int *nbl = nullptr;
@@ -253,6 +257,7 @@ struct BoxBase {
     cudaFree(cl_list);
     cudaFree(cl_cellof);
     cudaFree(nbl);
+    cudaFree(ovl);
   }
 
   virtual int alloc() = 0;
@@ -755,10 +760,10 @@ struct Box : BoxBase {
       if (nc) launch_nearcontact();  // timed with the position slot when profiling
       launch_k(pdl, k_particles_hydro_velocity<R>, dim3(Np * pp.hyd_pcl), dim3(pp.hyd_threads), 0, stream, pp, parts,
                (const R *)ustar, (const int *)cells, noise, euler, status, partial_p, arrivals,
-               nc ? nc_corr : (double *)nullptr);
+               nc ? nc_corr : (double *)nullptr, ovl);
       mark();
       launch_k(pdl, k_particles_scatter<R>, dim3(Np * PCL), dim3(256), 0, stream, pp, (const DPart *)parts,
-               (const int *)cells, phiup, status);
+               (const int *)cells, phiup, status, (const unsigned *)ovl);
       mark();
       zdisp_force(pdl);
       mark();
@@ -1852,6 +1857,10 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
     const double rl = std::max(pp.lj_on ? pp.lj_cut : 0.0, 2.0 * (pp.RADIUS + pp.HXI)) * (1.0 + 1e-9);
     rc = b->setup_cells(rl);
     if (rc) return rc;
+  }
+  if (b->Np > 0 && b->Np <= 1024 && !b->cl_on && pp.hyd_pcl == 1) {
+    if (cudaMalloc(&b->ovl, sizeof(unsigned) * 32 * (size_t)b->Np) != cudaSuccess) return KAPSEL_ENOMEM;
+    cudaMemset(b->ovl, 0, sizeof(unsigned) * 32 * (size_t)b->Np);
   }
   if (cudaMalloc(&b->partial_p, sizeof(double) * 18 * HYD_PCL_MAX * np1) != cudaSuccess) return KAPSEL_ENOMEM;
   if (cudaMalloc(&b->arrivals, sizeof(int) * np1) != cudaSuccess) return KAPSEL_ENOMEM;

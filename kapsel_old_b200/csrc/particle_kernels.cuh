@@ -274,7 +274,8 @@ __global__ void __launch_bounds__(1024) k_particles_hydro_velocity(PPar p, DPart
                                                                   int *__restrict__ status,
                                                                   double *__restrict__ partial,
                                                                   int *__restrict__ arrivals,
-                                                                  double *__restrict__ nc_corr = nullptr) {
+                                                                  double *__restrict__ nc_corr = nullptr,
+                                                                  unsigned *__restrict__ ovl = nullptr) {
   __shared__ double sh[2 * 9 * 32];
   __shared__ int last;
   pdl_begin();
@@ -418,6 +419,27 @@ __global__ void __launch_bounds__(1024) k_particles_hydro_velocity(PPar p, DPart
       }
     }
   }
+  if (ovl && p.hyd_pcl == 1 && !p.nbl) {
+    // the overlap candidates of this particle for the scatter that follows
+    // (centre distance below 2 (RADIUS + HXI)), as a bit per particle: one
+    // word per 32 candidates, written by the warp that tested them
+    const double lim = 2.0 * (p.RADIUS + p.HXI), lim2 = lim * lim;
+    for (int base = 0; base < p.Np; base += blockDim.x) {
+      const int j = base + threadIdx.x;
+      bool near = false;
+      if (j < p.Np && j != n) {
+        double s2 = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          double dd = parts[j].x[d] - xp[d];
+          dd -= nint_d(dd * p.invL[d]) * p.L[d];
+          s2 += dd * dd;
+        }
+        near = s2 < lim2;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, near);
+      if ((threadIdx.x & 31) == 0 && base + (threadIdx.x & ~31) < p.Np) ovl[(size_t)n * 32 + (j >> 5)] = bal;
+    }
+  }
   KSum acc[9];
   if constexpr (sizeof(R) == 4) {
     // each thread's few hydro terms are summed in float; from the warp
@@ -558,6 +580,48 @@ struct NbShared {
 
 // The overlap candidates of particle n in increasing index order, into nb
 // (at most NB_MAX); returns their count.  All threads of the block call it.
+__device__ void fill_candidate(const PPar &p, const DPart *__restrict__ parts, int j, NbShared &e) {
+  const DPart &o = parts[j];
+  const StencilBase sb = stencil_base(o.x, p);
+  for (int d = 0; d < 3; ++d) {
+    e.x[d] = o.x[d];
+    e.v[d] = o.v[d];
+    e.w[d] = o.omega[d];
+    e.res[d] = sb.res[d];
+    e.resf[d] = (float)sb.res[d];
+    e.xi[d] = sb.xi[d];
+  }
+  e.idx = j;
+}
+
+// The same list from the bit words the gather kernel left (ovl, at most
+// 1024 particles): warp 0 orders the set bits with a prefix sum.
+__device__ int overlap_from_bits(const PPar &p, const DPart *__restrict__ parts, int n, const unsigned *ovl,
+                                 NbShared *nb, int *__restrict__ status) {
+  __shared__ int total_b;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    const unsigned word = lane * 32 < p.Np ? ovl[(size_t)n * 32 + lane] : 0u;
+    const int c = __popc(word);
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    int pos = incl - c;
+    for (unsigned w = word; w; w &= w - 1, ++pos)
+      if (pos < NB_MAX) fill_candidate(p, parts, lane * 32 + __ffs(w) - 1, nb[pos]);
+    if (lane == 31) total_b = incl;
+  }
+  __syncthreads();
+  if (total_b > NB_MAX) {
+    if (threadIdx.x == 0) atomicExch(status, -6);
+    return NB_MAX;
+  }
+  return total_b;
+}
+
 __device__ int overlap_candidates(const PPar &p, const DPart *__restrict__ parts, int n, NbShared *nb,
                                   int *__restrict__ status) {
   __shared__ int wcount[32];
@@ -588,20 +652,7 @@ __device__ int overlap_candidates(const PPar &p, const DPart *__restrict__ parts
     __syncthreads();
     int pos = total + __popc(bal & ((1u << lane) - 1u));
     for (int w = 0; w < warp; ++w) pos += wcount[w];
-    if (near && pos < NB_MAX) {
-      const DPart &o = parts[j];
-      NbShared &e = nb[pos];
-      const StencilBase sb = stencil_base(o.x, p);
-      for (int d = 0; d < 3; ++d) {
-        e.x[d] = o.x[d];
-        e.v[d] = o.v[d];
-        e.w[d] = o.omega[d];
-        e.res[d] = sb.res[d];
-        e.resf[d] = (float)sb.res[d];
-        e.xi[d] = sb.xi[d];
-      }
-      e.idx = j;
-    }
+    if (near && pos < NB_MAX) fill_candidate(p, parts, j, nb[pos]);
     __syncthreads();
     if (threadIdx.x == 0)
       for (int w = 0; w < nw; ++w) total += wcount[w];
@@ -627,13 +678,14 @@ __device__ __forceinline__ void offset_from_base(const int rm[3], const int xi[3
 template <typename R>
 __global__ void __launch_bounds__(256) k_particles_scatter(PPar p, const DPart *__restrict__ parts,
                                                            const int *__restrict__ cells, R *__restrict__ phiup,
-                                                           int *__restrict__ status) {
+                                                           int *__restrict__ status,
+                                                           const unsigned *__restrict__ ovl = nullptr) {
   __shared__ NbShared nb[NB_MAX];
   pdl_begin();
   const int n = blockIdx.x / PCL;
   const int stride = PCL * blockDim.x;
   const int first = (blockIdx.x % PCL) * blockDim.x + threadIdx.x;
-  const int nnb = overlap_candidates(p, parts, n, nb, status);
+  const int nnb = ovl ? overlap_from_bits(p, parts, n, ovl, nb, status) : overlap_candidates(p, parts, n, nb, status);
   int nlow = 0;  // candidates with a lower index come first
   while (nlow < nnb && nb[nlow].idx < n) ++nlow;
   const DPart &a = parts[n];
