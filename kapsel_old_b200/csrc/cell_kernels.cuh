@@ -109,15 +109,22 @@ __global__ void k_cell_sort(CellPar c, const int *__restrict__ start, int *__res
 
 // Neighbour list of each particle: count, then up to NBL_MAX indices in
 // increasing order, of the particles within the list range (minimum image).
-// More neighbours than NBL_MAX: KAPSEL_ERANGE in the status word.
-__global__ void k_neighbor_lists(PPar p, CellPar c, const DPart *__restrict__ parts, const int *__restrict__ start,
-                                 const int *__restrict__ list, int *__restrict__ nbl, int *__restrict__ status) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= p.Np) return;
-  const double *xn = parts[n].x;
+// More neighbours than NBL_MAX: KAPSEL_ERANGE in the status word.  One warp
+// per particle: the lanes test a cell's members together and append the
+// hits in cell order (ballot), then each lane places its entries by rank.
+constexpr int NBL_WARPS = 4;  // particles per block
+__global__ void __launch_bounds__(NBL_WARPS * 32) k_neighbor_lists(PPar p, CellPar c, const DPart *__restrict__ parts,
+                                                                   const int *__restrict__ start,
+                                                                   const int *__restrict__ list, int *__restrict__ nbl,
+                                                                   int *__restrict__ status) {
+  __shared__ int cand[NBL_WARPS][NBL_MAX];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n = blockIdx.x * NBL_WARPS + warp;
+  if (n >= p.Np) return;  // a whole warp: no later block-wide barrier
+  int *cw = cand[warp];
+  const double xn[3] = {parts[n].x[0], parts[n].x[1], parts[n].x[2]};
   int ci[3];
   cell_coords(xn, c, ci);
-  int *out = nbl + (size_t)n * (NBL_MAX + 1) + 1;
   int cnt = 0;
   for (int ox = -1; ox <= 1; ++ox) {
     // each distinct neighbouring cell once (fewer than 3 cells on an axis)
@@ -130,38 +137,46 @@ __global__ void k_neighbor_lists(PPar p, CellPar c, const DPart *__restrict__ pa
         if ((c.lc[2] == 1 && oz != 0) || (c.lc[2] == 2 && oz == -1)) continue;
         const int cz = (ci[2] + oz + c.lc[2]) % c.lc[2];
         const int cell = (cx * c.lc[1] + cy) * c.lc[2] + cz;
-        for (int k = start[cell]; k < start[cell + 1]; ++k) {
-          const int j = list[k];
-          if (j == n) continue;
-          double s = 0.0;
+        const int b = start[cell], e = start[cell + 1];
+        for (int k0 = b; k0 < e; k0 += 32) {
+          const int k = k0 + lane;
+          int j = -1;
+          bool hit = false;
+          if (k < e) {
+            j = list[k];
+            if (j != n) {
+              double s = 0.0;
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            double dd = parts[j].x[d] - xn[d];
-            dd -= nint_d(dd * p.invL[d]) * p.L[d];
-            s += dd * dd;
+              for (int d = 0; d < 3; ++d) {
+                double dd = parts[j].x[d] - xn[d];
+                dd -= nint_d(dd * p.invL[d]) * p.L[d];
+                s += dd * dd;
+              }
+              hit = s < c.r2list;
+            }
           }
-          if (s < c.r2list) {
-            if (cnt < NBL_MAX) out[cnt] = j;
-            ++cnt;
-          }
+          const unsigned bal = __ballot_sync(0xffffffffu, hit);
+          const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+          if (hit && pos < NBL_MAX) cw[pos] = j;
+          cnt += __popc(bal);
         }
       }
     }
   }
+  __syncwarp();
   if (cnt > NBL_MAX) {
-    atomicExch(status, -6);
+    if (lane == 0) atomicExch(status, -6);
     cnt = NBL_MAX;
   }
-  for (int i = 1; i < cnt; ++i) {
-    const int v = out[i];
-    int k = i - 1;
-    while (k >= 0 && out[k] > v) {
-      out[k + 1] = out[k];
-      --k;
-    }
-    out[k + 1] = v;
+  // increasing index order: each entry's rank among the distinct indices
+  int *out = nbl + (size_t)n * (NBL_MAX + 1);
+  for (int q = lane; q < cnt; q += 32) {
+    const int v = cw[q];
+    int r = 0;
+    for (int t = 0; t < cnt; ++t) r += cw[t] < v;
+    out[1 + r] = v;
   }
-  out[-1] = cnt;
+  if (lane == 0) out[0] = cnt;
 }
 
 }  // namespace kapsel

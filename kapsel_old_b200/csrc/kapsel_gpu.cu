@@ -248,7 +248,8 @@ struct BoxBase {
     k_cell_scan<<<1, 1024, 0, stream>>>(clp, cl_count, cl_start, cl_cursor);
     k_cell_fill<<<(Np + 255) / 256, 256, 0, stream>>>(pp, cl_cellof, cl_cursor, cl_list);
     k_cell_sort<<<(clp.ncell + 255) / 256, 256, 0, stream>>>(clp, cl_start, cl_list);
-    k_neighbor_lists<<<(Np + 127) / 128, 128, 0, stream>>>(pp, clp, parts, cl_start, cl_list, nbl, status);
+    k_neighbor_lists<<<(Np + NBL_WARPS - 1) / NBL_WARPS, NBL_WARPS * 32, 0, stream>>>(pp, clp, parts, cl_start,
+                                                                                   cl_list, nbl, status);
   }
   void free_cells() {
     cudaFree(cl_count);
@@ -1666,7 +1667,7 @@ void BoxBase::launch_nearcontact() {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int tiles = (nc_cap + nc::TILE - 1) / nc::TILE;
-  nc::k_mlp_tile<false><<<std::min(tiles, std::max(nsm, 1)), 128, nc::SMEM_ALLOC, stream>>>(nc->params, io);
+  nc::k_mlp_tile<false><<<std::min(tiles, std::max(nsm, 1)), 256, nc::SMEM_ALLOC, stream>>>(nc->params, io);
 }
 
 struct kapsel_ctx {
@@ -2825,7 +2826,7 @@ int kapsel_nc_forward(kapsel_nc *nc, const float *x, int n, float *y) {
   io.n = n;
   io.out = dy;
   io.status = nc->status;
-  nc::k_mlp_tile<false><<<(n + nc::TILE - 1) / nc::TILE, 128, nc::SMEM_ALLOC, nc->stream>>>(nc->params, io);
+  nc::k_mlp_tile<false><<<(n + nc::TILE - 1) / nc::TILE, 256, nc::SMEM_ALLOC, nc->stream>>>(nc->params, io);
   KCHECK(cudaGetLastError());
   KCHECK(cudaMemcpyAsync(y, dy, sizeof(float) * nc::OUT * n, cudaMemcpyDeviceToHost, nc->stream));
   cudaFreeAsync(dx, nc->stream);

@@ -233,10 +233,16 @@ struct TileIO {
 
 // Forward (TRAIN=false) or forward + backward with gradient accumulation.
 // Loss = inv_n * sum_rows sum_c colw[c] (O[c] - y[c])^2.
+// Inference runs 256 threads: two per row (TMEM lane), each taking half of
+// the hidden columns in the epilogues (warps w and w+4 read the same 32
+// tensor-memory lanes); training runs 128, one per row.
 template <bool TRAIN>
-__global__ void __launch_bounds__(128, 1) k_mlp_tile(const float *__restrict__ params, TileIO io) {
+__global__ void __launch_bounds__(TRAIN ? 128 : 256, 1) k_mlp_tile(const float *__restrict__ params, TileIO io) {
   extern __shared__ __align__(128) unsigned char sm[];
   const int t = threadIdx.x, w = t >> 5;
+  const int r = t & (TILE - 1);             // row of the tile (TMEM lane)
+  const int h = TRAIN ? 0 : t >> 7;          // column half of the epilogues
+  constexpr int HC = TRAIN ? HID : HID / 2;  // hidden columns per thread
   const int n = io.n >= 0 ? io.n : min(*io.n_dev, io.n_cap);
   if (blockIdx.x * TILE >= n) return;
   const uint32_t sm0 = smem_u32(sm);
@@ -269,7 +275,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tile(const float *__restrict__ p
   __syncthreads();
   tc_fence_after();
   const uint32_t tm = *reinterpret_cast<volatile uint32_t *>(sm + S_TADDR);
-  const uint32_t lane_tm = tm + ((uint32_t)(w * 32) << 16);  // this warp's 32 lanes
+  const uint32_t lane_tm = tm + ((uint32_t)((w & 3) * 32) << 16);  // this warp's 32 lanes
   uint32_t phase = 0;
   bool ok = true;
 
@@ -290,7 +296,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tile(const float *__restrict__ p
   };
   // hidden-layer epilogue: A = silu(Z + b) -> blocked bf16
   auto fwd_hidden = [&](uint32_t zc, const float *b, uint32_t dst) {
-    for (int c0 = 0; c0 < HID; c0 += 16) {
+    for (int c0 = h * HC; c0 < (h + 1) * HC; c0 += 16) {
       float v[16];
       tmem_ld16(lane_tm + zc + c0, v);
 #pragma unroll
@@ -298,7 +304,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tile(const float *__restrict__ p
         const float z = v[i] + b[c0 + i];
         v[i] = z * sigm(z);
       }
-      st_row16(sm, dst, t, c0, HID, v);
+      st_row16(sm, dst, r, c0, HID, v);
     }
   };
 
@@ -308,14 +314,14 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tile(const float *__restrict__ p
   // next tile's input is staged.
   for (int tile = blockIdx.x; ok && tile * TILE < n; tile += gridDim.x) {
   const int row0 = tile * TILE;
-  const int row = row0 + t;
+  const int row = row0 + r;
   const bool valid = row < n;
   const int src = valid ? (io.idx ? io.idx[row] : row) : 0;
-  {
+  if (h == 0) {
     float xv[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) xv[i] = valid ? io.x[(size_t)src * IN + i] : 0.f;
-    st_row16(sm, S_X, t, 0, IN, xv);
+    st_row16(sm, S_X, r, 0, IN, xv);
   }
   to_mma();
 
@@ -331,7 +337,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tile(const float *__restrict__ p
   if (ok) { fwd_hidden(256, sb + 2 * HID, S_A3); to_mma(); }
   if (ok && t == 0) gemm(tm + 384, sm0, S_A3, HID, false, S_W4, HID, false, 128, OUT, HID);
   if (ok) ok = sync_mma();
-  if (ok) {
+  if (ok && h == 0) {
     float o[16];
     tmem_ld16(lane_tm + 384, o);
 #pragma unroll
