@@ -144,3 +144,33 @@ def test_mixed_128cubed_256_2000_steps_against_fp64():
         assert e["u"] < 1e-4 and e["v"] < 1e-3 and e["x"] < 1e-5, curve
     print("mixed vs FP64, 128^3/256:", "; ".join(f"{c['step']}: u {c['u']:.1e} v {c['v']:.1e} x {c['x']:.1e}"
                                                   for c in curve))
+
+
+def test_electrolyte_128cubed_64_fp64_3_steps_against_reference():
+    """The charged-colloid configuration (128^3, 64 spheres, Z = -100, salt
+    with Debye length 4, Bjerrum length 0.7, E_x = 0.05) in FP64 against the
+    compiled reference for 3 steps: zeta and the ion concentrations on the
+    retained modes, particle positions and velocities, <= 1e-10."""
+    _need_ref()
+    import kapsel_old_b200 as kg
+
+    cfg = workload.electrolyte_128_64()
+    R = ref.RefSim(cfg)
+    g = kg.Simulation(cfg, precision=kg.FP64)
+    S = spm.Spectral(spm.Params(dict(cfg, eq="Navier_Stokes")))
+
+    def trunc(a):
+        z = spm.SpmOracle.from_ooura(a)
+        return spm.SpmOracle.to_ooura(np.stack([S.truncate(z[c]) for c in range(len(z))]))
+
+    for s in range(1, 4):
+        R.step(1)
+        g.step(1, graph=True)
+        conc_ref = trunc(np.stack([R.field(20), R.field(21)]))
+        e = {"zeta": rel(g.zeta(), trunc(R.zeta())), "conc": rel(g.concentration(), conc_ref)}
+        pg, pr = g.particles(), R.particles()
+        e["x"] = np.abs(pg["x"] - pr["x"]).max()
+        e["v"] = rel(pg["v"], pr["v"])
+        e["f_hydro"] = rel(pg["f_hydro"], pr["f_hydro"])
+        for k, v in e.items():
+            assert v < FP64_TOL, (s, k, v, e)
