@@ -55,6 +55,17 @@ def peaks():
 # ---------------------------------------------------------------------------
 # algorithmic bytes of each launch (compulsory reads + writes of the stored
 # operands; complex values 2R, real values R bytes)
+# profiling slots of a step (kapsel_gpu_profile_step), labelled with the
+# kernel names the library reports; repeated kernels get the suffixes below
+SLOT_SUFFIX = {3: "#5", 5: "#2", 11: "#3"}
+# y-pass variants of the batch autotuner (kapsel_batch_variants)
+Y_VARIANTS = ["warp", "block wide tile", "block narrow tile", "warp, fused y/z planes"]
+
+
+def slot_labels(names):
+    return [(n + SLOT_SUFFIX.get(i, "")) if n else "" for i, n in enumerate(names)]
+
+
 def kernel_bytes(cfg, R: int):
     NX, NY, NZ = [1 << p for p in cfg["np_xyz"]]
     T = [(n + 2) // 3 for n in (NX, NY, NZ)]
@@ -81,6 +92,9 @@ def kernel_bytes(cfg, R: int):
         "k_z_force": 7 * N * R + 3 * I2,
         "k_y_pass<fwd>#3": 3 * I2 + 3 * I1,
         "k_x_force_to_zeta": 3 * I1 + 2 * zeta,
+        # fused y/z plane kernels: the y pass's intermediate stays on chip
+        "k_yzw_c2r": 3 * I1 + 3 * N * R,
+        "k_zyw_force": 7 * N * R + 3 * I1,
     }
 
 
@@ -243,12 +257,13 @@ def run_ours(args, rank, world, local_rank):
         sim_m._check(L.kapsel_gpu_profile_step(sim_m.h, buf))
         acc += np.frombuffer(buf, dtype=np.float32)
     acc /= prof_steps
-    names = list(kernel_bytes(cfg, 4).keys())
-    # profiling slots: the 13 kernels of a step, each launched on its own (in
-    # the timed graph the position update runs inside the k_z_c2r launch)
+    names = slot_labels(sim_m.step_kernel_names())
+    # profiling slots: the kernels of a step, each launched on its own (in
+    # the timed graph the position update runs inside the c2r launch); a slot
+    # with no launch (a y pass inside a fused y/z kernel) is left out
     nslot = len(names)
-    shares = {names[i]: float(acc[i]) for i in range(nslot)}
-    top = max(range(nslot), key=lambda i: acc[i])
+    shares = {names[i]: float(acc[i]) for i in range(nslot) if names[i]}
+    top = max((i for i in range(nslot) if names[i]), key=lambda i: acc[i])
     kb = kernel_bytes(cfg, 4)
     top_name = names[top]
     achieved = kb[top_name] / (acc[top] * 1e-3) / 1e9
@@ -327,7 +342,7 @@ def run_ours(args, rank, world, local_rank):
             "boxes": len(boxes), "particles": sum(len(c["particles"]) for c in boxes),
             "msd_mean": float(np.mean(msd)),
             "autotune": [{"shape": list(v[:3]), "z_pass": ["warp", "block"][v[3]],
-                          "y_pass": ["warp", "block wide tile", "block narrow tile"][v[4]]} for v in chosen],
+                          "y_pass": Y_VARIANTS[v[4]]} for v in chosen],
             "workload": "48 boxes from {32^3, 64^3, 64x64x128, 128^3}, 1-64 spheres a in [4,6], kBT=1e-3, mixed"}
         # learned near-contact correction: trained on the GPU from the committed
         # pair set (method runs at a=5 and a=10), then the 256^3 / 2048-sphere

@@ -202,7 +202,10 @@ int kapsel_batch_get_stream(kapsel_batch *b, void **stream);
 /* The autotuner's choice per box shape, 5 ints each (up to cap shapes):
    NX, NY, NZ, the z-pass variant (0 warp-level line groups, 1 block-level
    row tiles) and the y-pass variant (0 warp-level, 1 block-level wide kz
-   tile, 2 block-level narrow kz tile); returns the number of shapes. */
+   tile, 2 block-level narrow kz tile, 3 warp-level with the inverse y + z
+   c2r and the force's z + y passes fused over (component, x) planes held in
+   shared memory; 3 needs z variant 0, NY = 32..128 and particles); returns
+   the number of shapes. */
 int kapsel_batch_variants(kapsel_batch *b, int *out, int cap);
 /* Sets the pass variants (as above) of one Navier_Stokes context; results
    are the same to roundoff, speed differs by shape.  KAPSEL_EINVAL for a
@@ -347,6 +350,10 @@ int kapsel_sekibun_cells(double a, double a_xi, double dx, int *out, int cap);
 #define KAPSEL_N_STEP_KERNELS 13
 int kapsel_gpu_launches_per_step(kapsel_ctx *ctx);
 const char *kapsel_gpu_kernel_name(int i);
+/* The kernel of timing slot i for this context's pass variants: with the
+   fused y/z plane kernels (pass variant y = 3) slot 6 is k_yzw_c2r, slot 10
+   k_zyw_force, and slots 5 and 11 are empty ("", no launch). */
+const char *kapsel_gpu_step_kernel_name(kapsel_ctx *ctx, int i);
 
 /* The context's CUDA stream (a cudaStream_t), for recording events around
    its work. */

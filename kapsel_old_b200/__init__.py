@@ -120,6 +120,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_md_velocity": (ctypes.c_int, [_VP, _DP, _DP, ctypes.c_int]),
         "kapsel_gpu_set_time": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_double]),
         "kapsel_gpu_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+        "kapsel_gpu_step_kernel_name": (ctypes.c_char_p, [_VP, ctypes.c_int]),
         "kapsel_gpu_save_restart": (ctypes.c_int, [_VP, ctypes.c_char_p]),
         "kapsel_gpu_write_avs": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
         "kapsel_gpu_load_restart": (ctypes.c_int, [_VP, ctypes.c_char_p]),
@@ -298,6 +299,11 @@ class Simulation:
         f = self.L.kapsel_gpu_step_graph if graph else self.L.kapsel_gpu_step
         self._check(f(self.h, int(n)))
 
+    def step_kernel_names(self) -> list:
+        """The kernel of each profiling slot (kapsel_gpu_profile_step) for
+        this context's pass variants; "" for a slot with no launch."""
+        return [self.L.kapsel_gpu_step_kernel_name(self.h, i).decode() for i in range(13)]
+
     def time(self):
         ts = ctypes.c_int()
         t = ctypes.c_double()
@@ -471,7 +477,8 @@ class Batch:
     def variants(self) -> list:
         """The autotuner's choice per box shape: (NX, NY, NZ, z variant,
         y variant); z 0 warp-level / 1 block-level, y 0 warp-level /
-        1 block-level wide tile / 2 block-level narrow tile."""
+        1 block-level wide tile / 2 block-level narrow tile / 3 warp-level
+        with the fused y/z plane kernels."""
         self.L.kapsel_batch_variants.argtypes = [_VP, _IP, ctypes.c_int]
         buf = (ctypes.c_int * (5 * 64))()
         n = self.L.kapsel_batch_variants(self.h, buf, 64)

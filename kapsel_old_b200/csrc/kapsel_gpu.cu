@@ -39,6 +39,7 @@
 #include "obl_kernels.cuh"
 #include "particle_kernels.cuh"
 #include "spectral_kernels.cuh"
+#include "yz_kernels.cuh"
 #include "zwarp_kernels.cuh"
 
 using namespace kapsel;
@@ -269,6 +270,8 @@ struct BoxBase {
   virtual float time_variant(int zmode, int ymode, int reps) = 0;
   virtual void set_variant(int zmode, int ymode) = 0;
   virtual bool variant_ok(int zmode, int ymode) const = 0;
+  // the step runs the fused y/z plane kernels (k_yzw_c2r, k_zyw_force)
+  virtual bool fused_yz() const { return false; }
   virtual int alloc_el() = 0;
   virtual int alloc_obl() = 0;
   virtual int oblique_state(double *out) = 0;
@@ -345,6 +348,13 @@ struct BoxBase {
 #endif
 constexpr int kXZThreads = KAPSEL_XZ_THREADS, kXAdvThreads = KAPSEL_XADV_THREADS,
               kXForceThreads = KAPSEL_XFORCE_THREADS;
+
+// warps per block of the fused y/z plane kernels (FP32 fields; 4 measured
+// faster than 6 and 8 at 128^3: three 64 KB blocks per SM hold all 384
+// planes in one wave)
+#ifndef KAPSEL_YZ_NW
+#define KAPSEL_YZ_NW 4
+#endif
 
 template <typename R>
 struct Box : BoxBase {
@@ -455,7 +465,67 @@ struct Box : BoxBase {
     zw_grid_c = std::min((3 * groups + ZNW - 1) / ZNW, std::max(oc, 1) * nsm);
     zw_grid_f = std::min((groups + ZNW - 1) / ZNW, std::max(of, 1) * nsm);
     zw = LM;
+    yz_ly = 0;
+    if (g.KYc < g.NY) {
+      if (g.NY == 32) return yz_setup<5, LM>();
+      if (g.NY == 64) return yz_setup<6, LM>();
+      if (g.NY == 128) return yz_setup<7, LM>();
+    }
     return 0;
+  }
+
+  // fused y/z plane kernels (pass variant ymode 3): the inverse to u* and the
+  // rigidity force as one launch each, for NY = 2^yz_ly (0: not available)
+  static constexpr int YZNW = sizeof(R) == 4 ? KAPSEL_YZ_NW : 4;  // warps per block
+  int yz_ly = 0;
+  size_t yz_sm = 0;
+  unsigned *plane_count = nullptr;  // [NX] readers of phi per x plane (k_zyw_force)
+  template <int LY, int LM>
+  int yz_setup() {
+    const size_t sm = YZ<R, LY, LM>::smem(YZNW);
+    if (sm > 227 * 1024) return 0;
+    KCHECK(cudaFuncSetAttribute(k_yzw_c2r<R, LY, LM, false, YZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sm));
+    KCHECK(cudaFuncSetAttribute(k_zyw_force<R, LY, LM, false, YZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sm));
+    yz_sm = sm;
+    yz_ly = LY;
+    return 0;
+  }
+  template <int LY, int LM>
+  void yz_c2r_l(bool pdl, DPart *pts, int euler) {
+    const int posblk = pts ? (Np + YZNW * 32 - 1) / (YZNW * 32) : 0;
+    launch_k(pdl, k_yzw_c2r<R, LY, LM, false, YZNW>, dim3(3 * g.NX + posblk), dim3(YZNW * 32), yz_sm, stream, g, tw,
+             (const Cx<R> *)bufA, ustar, npts(), g.NZ, 3 * g.NX, pp, pts, euler, status);
+  }
+  template <int LY, int LM>
+  void zy_force_l(bool pdl) {
+    launch_k(pdl, k_zyw_force<R, LY, LM, false, YZNW>, dim3(3 * g.NX), dim3(YZNW * 32), yz_sm, stream, g, tw, phiup,
+             (const R *)ustar, bufA, plane_count);
+  }
+  // bufA (x real, ky compact) -> u*, with the position update in extra blocks
+  template <int LM>
+  void yz_c2r_m(bool pdl, DPart *pts, int euler) {
+    if (yz_ly == 5) yz_c2r_l<5, LM>(pdl, pts, euler);
+    else if (yz_ly == 6) yz_c2r_l<6, LM>(pdl, pts, euler);
+    else yz_c2r_l<7, LM>(pdl, pts, euler);
+  }
+  void yz_c2r(bool pdl, DPart *pts, int euler) {
+    if (zw == 5) yz_c2r_m<5>(pdl, pts, euler);
+    else if (zw == 6) yz_c2r_m<6>(pdl, pts, euler);
+    else yz_c2r_m<7>(pdl, pts, euler);
+  }
+  // phi/up, u* -> force spectra in bufA (x real, ky compact)
+  template <int LM>
+  void zy_force_m(bool pdl) {
+    if (yz_ly == 5) zy_force_l<5, LM>(pdl);
+    else if (yz_ly == 6) zy_force_l<6, LM>(pdl);
+    else zy_force_l<7, LM>(pdl);
+  }
+  void zy_force(bool pdl) {
+    if (zw == 5) zy_force_m<5>(pdl);
+    else if (zw == 6) zy_force_m<6>(pdl);
+    else zy_force_m<7>(pdl);
   }
   template <int LM>
   void zw_products(bool pdl) {
@@ -508,6 +578,8 @@ struct Box : BoxBase {
     KCHECK(cudaMalloc(&bufB, sizeof(Cx<R>) * nbuf * nB));
     KCHECK(cudaMalloc(&ustar, sizeof(R) * 3 * npts()));
     KCHECK(cudaMalloc(&phiup, sizeof(R) * 4 * npts()));
+    KCHECK(cudaMalloc(&plane_count, sizeof(unsigned) * g.NX));
+    KCHECK(cudaMemset(plane_count, 0, sizeof(unsigned) * g.NX));
     KCHECK(cudaMemset(zeta, 0, sizeof(Cx<R>) * 2 * nz));
     KCHECK(cudaMemset(ustar, 0, sizeof(R) * 3 * npts()));
     KCHECK(cudaMemset(phiup, 0, sizeof(R) * 4 * npts()));
@@ -561,6 +633,10 @@ struct Box : BoxBase {
       // batch autotuner may choose otherwise per box shape)
       zw_avail = zw;
       if (!zw_ok) zw = 0;
+      // FP32: the fused y/z plane kernels wherever the warp-level z kernels
+      // run (128^3 mixed step 0.200 -> 0.189 ms); FP64 planes (90 KB at
+      // 128^3) leave one block per SM and run slower than the separate passes
+      if (sizeof(R) == 4 && zw && yz_ly) ymode = 3;
     }
     KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
     KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xadv));
@@ -622,7 +698,7 @@ struct Box : BoxBase {
   int zw_avail = 0;  // warp-level z kernels set up for this NZ (their line-length log), else 0
   template <bool INV>
   void launch_y(const Geo &gg, int nc, const Cx<R> *in, Cx<R> *out, bool pdl = false) {
-    if (ymode == 0) switch (gg.NY) {
+    if (ymode == 0 || ymode == 3) switch (gg.NY) {
       case 32: yw<INV, 5>(gg, nc, in, out, pdl); return;
       case 64: yw<INV, 6>(gg, nc, in, out, pdl); return;
       case 128: yw<INV, 7>(gg, nc, in, out, pdl); return;
@@ -640,9 +716,10 @@ struct Box : BoxBase {
   }
   size_t sm_y_any = 0;
   bool variant_ok(int zmode, int ymode_) const override {
-    if (prm.eq != KAPSEL_EQ_NAVIER_STOKES || zmode < 0 || zmode > 1 || ymode_ < 0 || ymode_ > 2) return false;
+    if (prm.eq != KAPSEL_EQ_NAVIER_STOKES || zmode < 0 || zmode > 1 || ymode_ < 0 || ymode_ > 3) return false;
     if (zmode == 0 && !zw_avail) return false;
-    if (ymode_ == 0 && !(g.NY >= 32 && g.NY <= 256)) return false;
+    if ((ymode_ == 0 || ymode_ == 3) && !(g.NY >= 32 && g.NY <= 256)) return false;
+    if (ymode_ == 3 && (zmode != 0 || !yz_ly || Np == 0)) return false;
     return true;
   }
   void set_variant(int zmode, int ymode_) override {
@@ -747,12 +824,18 @@ struct Box : BoxBase {
     mark();
     x_advect<0>(pdl);
     mark();
-    launch_y<true>(g, 3, bufA, bufB, pdl);
+    // ymode 3: the inverse y and z c2r as one launch (k_yzw_c2r), and the
+    // force's z and y passes as one (k_zyw_force); their y slots stay empty
+    const bool yzf = fused_yz();
+    if (!yzf) launch_y<true>(g, 3, bufA, bufB, pdl);
     mark();
     // u* and, in extra blocks, the particle positions (a launch of their own
     // when profiling, so that each launch is timed separately)
     const bool fuse_pos = Np > 0 && !ev;
-    zdisp_c2r(pdl, fuse_pos ? parts : (DPart *)nullptr, euler);
+    if (yzf)
+      yz_c2r(pdl, fuse_pos ? parts : (DPart *)nullptr, euler);
+    else
+      zdisp_c2r(pdl, fuse_pos ? parts : (DPart *)nullptr, euler);
     mark();
     if (Np > 0) {
       if (!fuse_pos) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
@@ -766,9 +849,12 @@ struct Box : BoxBase {
       launch_k(pdl, k_particles_scatter<R>, dim3(Np * PCL), dim3(256), 0, stream, pp, (const DPart *)parts,
                (const int *)cells, phiup, status, (const unsigned *)ovl);
       mark();
-      zdisp_force(pdl);
+      if (yzf)
+        zy_force(pdl);
+      else
+        zdisp_force(pdl);
       mark();
-      launch_y<false>(g, 3, bufB, bufA, pdl);
+      if (!yzf) launch_y<false>(g, 3, bufB, bufA, pdl);
       mark();
       if (fused)
         x_force_next(pdl);
@@ -784,6 +870,7 @@ struct Box : BoxBase {
     u_spec_ready = true;
   }
   bool ends_with_u_spec() const override { return prm.eq == KAPSEL_EQ_NAVIER_STOKES && Np > 0; }
+  bool fused_yz() const override { return prm.eq == KAPSEL_EQ_NAVIER_STOKES && ymode == 3 && zw && yz_ly && Np > 0; }
 
   void launch_init() override {
     // Init_zeta_k gives zeta = 0 and u = 0 (init_fluid.cxx:10-26); the
@@ -1272,6 +1359,7 @@ struct Box : BoxBase {
     cudaFree(ustar);
     cudaFree(phiup);
     cudaFree(twbuf);
+    cudaFree(plane_count);
   }
 };
 
@@ -2379,6 +2467,16 @@ const char *kapsel_gpu_kernel_name(int i) {
   return (i >= 0 && i < KAPSEL_N_STEP_KERNELS) ? kKernelNames[i] : "";
 }
 
+const char *kapsel_gpu_step_kernel_name(kapsel_ctx *ctx, int i) {
+  if (i < 0 || i >= KAPSEL_N_STEP_KERNELS) return "";
+  if (ctx && ctx->box->fused_yz()) {
+    if (i == 5 || i == 11) return "";  // y passes inside the fused launches
+    if (i == 6) return "k_yzw_c2r";
+    if (i == 10) return "k_zyw_force";
+  }
+  return kKernelNames[i];
+}
+
 int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms) {
   // A short timed gate kernel holds the stream while the host enqueues the
   // step with an event between consecutive launches, so on the device the
@@ -2460,7 +2558,7 @@ int kapsel_batch_create(kapsel_ctx *const *boxes, int n, int autotune, kapsel_ba
       if (zp < 0) {
         float best = 0.f;
         for (int zm = 0; zm < 2; ++zm)
-          for (int ym = 0; ym < 3; ++ym) {
+          for (int ym = 0; ym < 4; ++ym) {
             if (!x->variant_ok(zm, ym)) continue;
             const float t = x->time_variant(zm, ym, 5);
             if (t > 0.f && (zp < 0 || t < best)) best = t, zp = zm, yp = ym;
