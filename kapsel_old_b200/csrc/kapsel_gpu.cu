@@ -109,6 +109,25 @@ int ilog2(int n) {
     }                                                        \
   } while (0)
 
+// Lets `kern` take all the dynamic shared memory a block may opt in to
+// (`need` bytes must fit).  The limit is one value per kernel function,
+// shared by every context of the process: set to one box shape's size it
+// would refuse the same kernel's launches for a larger shape created
+// earlier.  Occupancy follows the shared memory a launch asks for, not
+// this limit.
+template <typename K>
+cudaError_t allow_smem(K kern, size_t need) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa;
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kern);
+  if (e != cudaSuccess) return e;
+  const size_t lim = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+  if (need > lim) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim);
+}
+
 // Sekibun stencil offsets (Particle_domain, profile.cxx:25-74): points with
 // |(i,j,k) DX| < RADIUS + HXI + 1.7321 DX, scanned i, j, k from -nh to nh.
 std::vector<int> sekibun(double A, double A_XI, double DX) {
@@ -374,14 +393,11 @@ struct Box : BoxBase {
   // x passes with compile-time NX for NX = 32..256 (the runtime-NX kernels otherwise)
   template <int LX>
   int x_setup() {
-    KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R, KCX, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
-    KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX, 0, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_xadv));
-    KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX, 1, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_xadv));
-    KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX, LX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xf));
-    KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX, LX, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_xf));
+    KCHECK(allow_smem(k_x_zeta_to_u<R, KCX, LX>, smem_xu));
+    KCHECK(allow_smem(k_x_advect_update<R, KCX, 0, LX>, smem_xadv));
+    KCHECK(allow_smem(k_x_advect_update<R, KCX, 1, LX>, smem_xadv));
+    KCHECK(allow_smem(k_x_force_to_zeta<R, KCX, LX>, smem_xf));
+    KCHECK(allow_smem(k_x_force_to_zeta<R, KCX, LX, 1>, smem_xf));
     return 0;
   }
   template <int LX>
@@ -451,9 +467,9 @@ struct Box : BoxBase {
     zw_sm_c = line;
     zw_sm_f = 3 * line;
     auto kp = sizeof(R) == 8 ? k_zw_products_pf<R, LM, ZNW> : k_zw_products<R, LM, ZNW>;
-    KCHECK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_p));
-    KCHECK(cudaFuncSetAttribute(k_zw_c2r<R, LM, ZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_c));
-    KCHECK(cudaFuncSetAttribute(k_zw_force<R, LM, ZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zw_sm_f));
+    KCHECK(allow_smem(kp, zw_sm_p));
+    KCHECK(allow_smem(k_zw_c2r<R, LM, ZNW>, zw_sm_c));
+    KCHECK(allow_smem(k_zw_force<R, LM, ZNW>, zw_sm_f));
     int dev = 0, nsm = 0, op = 0, oc = 0, of = 0;
     KCHECK(cudaGetDevice(&dev));
     KCHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -484,10 +500,8 @@ struct Box : BoxBase {
   int yz_setup() {
     const size_t sm = YZ<R, LY, LM>::smem(YZNW);
     if (sm > 227 * 1024) return 0;
-    KCHECK(cudaFuncSetAttribute(k_yzw_c2r<R, LY, LM, false, YZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sm));
-    KCHECK(cudaFuncSetAttribute(k_zyw_force<R, LY, LM, false, YZNW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sm));
+    KCHECK(allow_smem(k_yzw_c2r<R, LY, LM, false, YZNW>, sm));
+    KCHECK(allow_smem(k_zyw_force<R, LY, LM, false, YZNW>, sm));
     yz_sm = sm;
     yz_ly = LY;
     return 0;
@@ -638,24 +652,23 @@ struct Box : BoxBase {
       // 128^3) leave one block per SM and run slower than the separate passes
       if (sizeof(R) == 4 && zw && yz_ly) ymode = 3;
     }
-    KCHECK(cudaFuncSetAttribute(k_x_zeta_to_u<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xu));
-    KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xadv));
-    KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xf));
-    KCHECK(cudaFuncSetAttribute(k_x_force_to_zeta<R, KCX, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_xf));
-    KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
-    KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
-    KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
-    KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
-    KCHECK(cudaFuncSetAttribute(k_z_products<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zp));
-    KCHECK(cudaFuncSetAttribute(k_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
-    KCHECK(cudaFuncSetAttribute(k_z_r2c_full<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zr));
-    KCHECK(cudaFuncSetAttribute(k_z_force<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zf));
+    KCHECK(allow_smem(k_x_zeta_to_u<R, KCX>, smem_xu));
+    KCHECK(allow_smem(k_x_advect_update<R, KCX>, smem_xadv));
+    KCHECK(allow_smem(k_x_force_to_zeta<R, KCX>, smem_xf));
+    KCHECK(allow_smem(k_x_force_to_zeta<R, KCX, 0, 1>, smem_xf));
+    KCHECK(allow_smem(k_y_pass<R, true, KCY>, smem_y));
+    KCHECK(allow_smem(k_y_pass<R, false, KCY>, smem_y));
+    KCHECK(allow_smem(k_y_pass<R, true, KCY / 2>, smem_y));
+    KCHECK(allow_smem(k_y_pass<R, false, KCY / 2>, smem_y));
+    KCHECK(allow_smem(k_z_products<R>, smem_zp));
+    KCHECK(allow_smem(k_z_c2r<R>, smem_zc));
+    KCHECK(allow_smem(k_z_r2c_full<R>, smem_zr));
+    KCHECK(allow_smem(k_z_force<R>, smem_zf));
     const int nmax = std::max(g.NX, g.NY);
     const int smem_col = (int)(C * ((size_t)nmax + (size_t)nmax * 16));
-    KCHECK(cudaFuncSetAttribute(k_col_pass<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_col));
-    KCHECK(cudaFuncSetAttribute(k_col_pass<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_col));
-    KCHECK(cudaFuncSetAttribute(k_z_c2r_full<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zr));
+    KCHECK(allow_smem(k_col_pass<R, true>, smem_col));
+    KCHECK(allow_smem(k_col_pass<R, false>, smem_col));
+    KCHECK(allow_smem(k_z_c2r_full<R>, smem_zr));
     return 0;
   }
 
@@ -679,7 +692,7 @@ struct Box : BoxBase {
       int dev = 0;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      allow_smem(kern, sm);
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, YNW * 32, sm);
       occ = std::max(occ, 1);
     }
@@ -907,11 +920,11 @@ struct Box : BoxBase {
     sm_xo3 = C * (g.NX + (size_t)2 * g.KXc * KCX + (size_t)2 * g.NX * 3 * KCX);
     sm_xof = C * (g.NX + (size_t)2 * g.NX * 3 * KCX);
     if (sm_xo6 > 227 * 1024 || smem_zc > 227 * 1024) return KAPSEL_ERANGE;
-    KCHECK(cudaFuncSetAttribute(k_x_obl_inv<R, KCX, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_xo6));
-    KCHECK(cudaFuncSetAttribute(k_x_obl_inv<R, KCX, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_xo3));
-    KCHECK(cudaFuncSetAttribute(k_x_obl_fwd<R, KCX, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_xof));
-    KCHECK(cudaFuncSetAttribute(k_x_obl_fwd<R, KCX, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_xof));
-    KCHECK(cudaFuncSetAttribute(k_z_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_zc));
+    KCHECK(allow_smem(k_x_obl_inv<R, KCX, 6>, sm_xo6));
+    KCHECK(allow_smem(k_x_obl_inv<R, KCX, 3>, sm_xo3));
+    KCHECK(allow_smem(k_x_obl_fwd<R, KCX, 1>, sm_xof));
+    KCHECK(allow_smem(k_x_obl_fwd<R, KCX, 0>, sm_xof));
+    KCHECK(allow_smem(k_z_r2c<R>, smem_zc));
     op.shear_rate = prm.shear_rate;
     op.dt = prm.dt;
     // ivolume = Ivolume * POW3(DX); s_rate_eff *= ivolume*NY/(NY - 1) (sp_3d_ns.h:175,192)
@@ -1030,21 +1043,20 @@ struct Box : BoxBase {
     sm_y_any = sm_el;
     if (sm_el > 227 * 1024) return KAPSEL_ERANGE;
     const int sm = (int)sm_el;
-    KCHECK(cudaFuncSetAttribute(k_x_inv_op<R, KCX, XI_IDENT, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_x_inv_op<R, KCX, XI_IDENT, 3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_x_inv_op<R, KCX, XI_GRADPSI, 1, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_x_inv_op<R, KCX, XI_GRADDIFF, 1, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_x_fwd_op<R, KCX, XF_STORE, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_x_fwd_op<R, KCX, XF_CONCUPD, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_x_fwd_op<R, KCX, XF_GRADPSI_FULL, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_z_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_y_pass<R, true, KCY / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_y_pass<R, false, KCY / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    KCHECK(cudaFuncSetAttribute(k_x_advect_update<R, KCX, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_xadv));
+    KCHECK(allow_smem(k_x_inv_op<R, KCX, XI_IDENT, 2, 2>, sm));
+    KCHECK(allow_smem(k_x_inv_op<R, KCX, XI_IDENT, 3, 3>, sm));
+    KCHECK(allow_smem(k_x_inv_op<R, KCX, XI_GRADPSI, 1, 3>, sm));
+    KCHECK(allow_smem(k_x_inv_op<R, KCX, XI_GRADDIFF, 1, 3>, sm));
+    KCHECK(allow_smem(k_x_fwd_op<R, KCX, XF_STORE, 1>, sm));
+    KCHECK(allow_smem(k_x_fwd_op<R, KCX, XF_CONCUPD, 3>, sm));
+    KCHECK(allow_smem(k_x_fwd_op<R, KCX, XF_GRADPSI_FULL, 1>, sm));
+    KCHECK(allow_smem(k_z_r2c<R>, sm));
+    KCHECK(allow_smem(k_z_c2r<R>, sm));
+    KCHECK(allow_smem(k_y_pass<R, true, KCY>, sm));
+    KCHECK(allow_smem(k_y_pass<R, false, KCY>, sm));
+    KCHECK(allow_smem(k_y_pass<R, true, KCY / 2>, sm));
+    KCHECK(allow_smem(k_y_pass<R, false, KCY / 2>, sm));
+    KCHECK(allow_smem(k_x_advect_update<R, KCX, 1>, smem_xadv));
     return 0;
   }
 
@@ -1727,10 +1739,8 @@ static int nc_smem_setup() {
   static std::once_flag once;
   static int rc = 0;
   std::call_once(once, []() {
-    if (cudaFuncSetAttribute(nc::k_mlp_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)nc::SMEM_ALLOC) != cudaSuccess ||
-        cudaFuncSetAttribute(nc::k_mlp_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)nc::SMEM_ALLOC) != cudaSuccess)
+    if (allow_smem(nc::k_mlp_tile<false>, nc::SMEM_ALLOC) != cudaSuccess ||
+        allow_smem(nc::k_mlp_tile<true>, nc::SMEM_ALLOC) != cudaSuccess)
       rc = KAPSEL_ECUDA;
   });
   return rc;

@@ -136,3 +136,32 @@ def test_fused_yz_planes_bitwise(shape, n, precision):
     assert np.array_equal(a.velocity(), b.velocity())
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_larger_box_created_before_smaller_one(precision):
+    """The dynamic shared-memory limit of a kernel is one value per process:
+    a box created after a larger one must not lower it below what the larger
+    box's launches ask for (64x64x128 with the block-level z passes, then
+    32^3), alone and in a batch built largest box first."""
+    import kapsel_old_b200 as kg
+
+    prec = kg.FP64 if precision == "fp64" else kg.MIXED
+    big = udf.ns_config((6, 6, 7), 6, seed=26, a=5.0, kbt=1e-3)
+    small = udf.ns_config((5, 5, 5), 2, seed=27, a=4.5, kbt=1e-3)
+    a = kg.Simulation(big, precision=prec)
+    b = kg.Simulation(small, precision=prec)
+    a.step(3)
+    b.step(3)
+    c = kg.Simulation(big, precision=prec)
+    c.step(3)
+    assert np.array_equal(a.zeta(), c.zeta())
+    sims = [kg.Simulation(cfg, precision=prec) for cfg in (big, big, small, small)]
+    solo = kg.Simulation(big, precision=prec)
+    bt = kg.Batch(sims, autotune=True)
+    bt.step(4)
+    solo.step(4)
+    assert rel(sims[0].zeta(), solo.zeta()) < (1e-12 if precision == "fp64" else 1e-5)
+    bt.close()
+    for s in sims + [a, b, c, solo]:
+        s.close()
