@@ -447,6 +447,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, warmup=1, steps=min(args.steps, 12))
+        # the serial build (the oracle) on one core, reported beside it
+        line["cpu_baseline_serial"] = cpu_baseline(cfg, warmup=1, steps=min(args.steps, 8), serial=True)
     return line
 
 
@@ -500,12 +502,14 @@ def parity_curve(kg, cfg, steps: int, points=(1, 10, 100, 250, 500, 1000, 1500, 
             "curve": curve}
 
 
-def cpu_baseline(cfg, warmup: int, steps: int, threads: int | None = None):
-    """Reference CPU timing on the host cores (oracle/_ref; else the numpy port)."""
+def cpu_baseline(cfg, warmup: int, steps: int, threads: int | None = None, serial: bool = False):
+    """Reference CPU timing on the host cores (oracle/_ref; else the numpy port):
+    the OpenMP build on all cores, or with `serial` the serial build (the
+    oracle) on one core."""
     from oracle import ref, udf
 
-    threads = threads or os.cpu_count() or 1
-    exe = os.path.join(ref.REF_DIR, "kapsel_ref_omp")
+    threads = 1 if serial else (threads or os.cpu_count() or 1)
+    exe = os.path.join(ref.REF_DIR, "kapsel_ref" if serial else "kapsel_ref_omp")
     if os.path.exists(exe):
         with tempfile.TemporaryDirectory() as td:
             kv = udf.write_udf(os.path.join(td, "in.kv"), cfg)
@@ -513,9 +517,10 @@ def cpu_baseline(cfg, warmup: int, steps: int, threads: int | None = None):
             out = subprocess.run([exe, kv, str(warmup), str(steps)], capture_output=True, text=True, env=env,
                                  timeout=900)
             d = json.loads(out.stdout.strip().splitlines()[-1])
+        build = "serial build, one core" if serial else "OpenMP loops"
         return {"value": round(1.0 / d["s_per_step"], 4), "unit": UNIT, "cores": threads, "kind": "reference",
                 "sample": f"{steps} steps of the same workload after {warmup} warm-up, "
-                          f"unmodified KAPSEL sources (OpenMP loops, Ooura FFT), wall clock"}
+                          f"unmodified KAPSEL sources ({build}, Ooura FFT), wall clock"}
     from oracle import spm
 
     o = spm.SpmOracle(cfg)
