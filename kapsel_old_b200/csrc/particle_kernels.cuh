@@ -750,8 +750,7 @@ __global__ void __launch_bounds__(256) k_particles_scatter(PPar p, const DPart *
 #pragma unroll
       for (int d = 0; d < 3; ++d) reinterpret_cast<float *>(phiup)[(1 + d) * npts + im] = up[d];
     }
-    return;
-  }
+  } else
   for (int m = first; m < p.S; m += stride) {
     int rm[3];
     double r[3], dist;

@@ -136,14 +136,26 @@ __global__ void __launch_bounds__(NW * 32) k_zyw_force(Geo g, Twiddles<R> tw, R 
   {
     Cx<R> wf[Z::N1];
     wfft_twiddles<R, LM, 1>(tw.m, wf);
-    for (int grp = warp; grp < P::NG; grp += NW) {
-      const size_t row0 = row_base + (size_t)grp * Z::RW;
-      // all of the lane's loads first (phi, then up and u* where phi is
-      // non-zero), so that they are in flight together
-      V2 ph[NI], up[NI], us[NI];
+    // phi of the warp's next row group is loaded while the current one is
+    // transformed
+    V2 ph_next[NI];
+    if (warp < P::NG)
 #pragma unroll
       for (int h = 0; h < NI; ++h)
-        ph[h] = *reinterpret_cast<const V2 *>(phiup + row0 * Z::NZ + 2 * (size_t)(lane + 32 * h));
+        ph_next[h] = *reinterpret_cast<const V2 *>(phiup + (row_base + (size_t)warp * Z::RW) * Z::NZ +
+                                                   2 * (size_t)(lane + 32 * h));
+    for (int grp = warp; grp < P::NG; grp += NW) {
+      const size_t row0 = row_base + (size_t)grp * Z::RW;
+      // all of the lane's loads first (up and u* where phi is non-zero), so
+      // that they are in flight together
+      V2 ph[NI], up[NI], us[NI];
+#pragma unroll
+      for (int h = 0; h < NI; ++h) ph[h] = ph_next[h];
+      if (grp + NW < P::NG)
+#pragma unroll
+        for (int h = 0; h < NI; ++h)
+          ph_next[h] = *reinterpret_cast<const V2 *>(phiup + (row0 + (size_t)NW * Z::RW) * Z::NZ +
+                                                     2 * (size_t)(lane + 32 * h));
 #pragma unroll
       for (int h = 0; h < NI; ++h) {
         const size_t o = row0 * Z::NZ + 2 * (size_t)(lane + 32 * h);
