@@ -65,10 +65,34 @@ __global__ void __launch_bounds__(NW * 32) k_yzw_c2r(Geo g, Twiddles<R> tw, cons
   {
     Cx<R> w[Y::N1];
     wfft_twiddles<R, LY, -1>(tw.y, w);
+    // the warp's next batch of kz columns is loaded into registers while the
+    // current one is transformed (the elements of yw_issue, same placement)
+    constexpr int TYc = FULLY ? P::NY / 2 + 1 : (P::NY + 2) / 3, KYc = FULLY ? P::NY : 2 * TYc - 1;
+    constexpr int NL = (KYc * Y::RW + 31) / 32;
+    const Cx<R> zero = {R(0), R(0)};
+    Cx<R> pre[NL];
+    auto load_batch = [&](int b) {
+      const int col0 = b * Y::RW, ncols = min(Y::RW, Z::TZ - col0);
+      const Cx<R> *src = in + (size_t)pl * KYc * g.TS + col0;
+#pragma unroll
+      for (int q = 0; q < NL; ++q) {
+        const int i = lane + 32 * q, r = i >> Y::LR, col = i & (Y::RW - 1);
+        pre[q] = (i < KYc * Y::RW && col < ncols) ? src[(size_t)r * g.TS + col] : zero;
+      }
+    };
+    if (warp < P::NB) load_batch(warp);
     for (int b = warp; b < P::NB; b += NW) {
-      yw_issue<R, true, LY, FULLY>(g, in, slot, pl * P::NB + b, P::NB);
-      cp_async_commit();
-      cp_async_wait_all();
+#pragma unroll
+      for (int q = 0; q < NL; ++q) {
+        const int i = lane + 32 * q, r = i >> Y::LR, col = i & (Y::RW - 1);
+        const int j = r < TYc ? r : P::NY + r - KYc;
+        if (i < KYc * Y::RW) slot[YL::template base<LY>(col) + zpos<LY>(j)] = pre[q];
+      }
+      for (int i = lane; i < (P::NY - KYc) * Y::RW; i += 32) {
+        const int j = TYc + (i >> Y::LR), col = i & (Y::RW - 1);
+        slot[YL::template base<LY>(col) + zpos<LY>(j)] = zero;
+      }
+      if (b + NW < P::NB) load_batch(b + NW);
       __syncwarp();
       wfft<R, LY, -1, YL>(slot, w);
       const int col0 = b * Y::RW, ncols = min(Y::RW, Z::TZ - col0);
