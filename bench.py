@@ -275,9 +275,12 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
+    # every step: the next step's thermostat normals drawn on the host and
+    # copied up, the graph step, and the particle records copied back
+    # (kapsel_gpu_step_graph_particles: one host synchronisation per step)
     for _ in range(args.steps):
-        sim_m._check(L.kapsel_gpu_step_graph(sim_m.h, 1))
-        sim_m._check(L.kapsel_gpu_get_particles(sim_m.h, rec.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        sim_m._check(L.kapsel_gpu_step_graph_particles(sim_m.h, 1,
+                                                       rec.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
     torch.cuda.synchronize()
     e2e_s = reduce_max(time.perf_counter() - t0, dist)
     sim_m.close()

@@ -132,6 +132,12 @@ int kapsel_gpu_get_velocity(kapsel_ctx *ctx, double *u);
 
 /* Particle records, n_particles * KAPSEL_P_STRIDE doubles. */
 int kapsel_gpu_get_particles(kapsel_ctx *ctx, double *out);
+/* kapsel_gpu_step_graph(ctx, n) followed by kapsel_gpu_get_particles(ctx,
+   out) with one host synchronisation instead of two: one pass of the
+   reference main loop (sp_3d_ns.cxx:547-594, Output_udf of the particles
+   every GTS steps, Time_evolution) with GTS = n.  Same status codes; the
+   records are filled also when the status is non-zero. */
+int kapsel_gpu_step_graph_particles(kapsel_ctx *ctx, int n, double *out);
 int kapsel_gpu_set_particle_state(kapsel_ctx *ctx, const double *in);
 
 /* Restart records.  save writes the state that Save_Restart_udf

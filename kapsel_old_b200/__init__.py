@@ -121,6 +121,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_set_time": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_double]),
         "kapsel_gpu_strerror": (ctypes.c_char_p, [ctypes.c_int]),
         "kapsel_gpu_step_kernel_name": (ctypes.c_char_p, [_VP, ctypes.c_int]),
+        "kapsel_gpu_step_graph_particles": (ctypes.c_int, [_VP, ctypes.c_int, _DP]),
         "kapsel_gpu_save_restart": (ctypes.c_int, [_VP, ctypes.c_char_p]),
         "kapsel_gpu_write_avs": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
         "kapsel_gpu_load_restart": (ctypes.c_int, [_VP, ctypes.c_char_p]),
@@ -299,6 +300,13 @@ class Simulation:
         f = self.L.kapsel_gpu_step_graph if graph else self.L.kapsel_gpu_step
         self._check(f(self.h, int(n)))
 
+    def step_particles(self, n: int = 1) -> dict:
+        """n graph-replayed steps, then the particle records, with one host
+        synchronisation (kapsel_gpu_step_graph_particles)."""
+        a = np.zeros((max(self.Np, 1), P_STRIDE))
+        self._check(self.L.kapsel_gpu_step_graph_particles(self.h, int(n), _ptr(a)))
+        return self._records(a)
+
     def step_kernel_names(self) -> list:
         """The kernel of each profiling slot (kapsel_gpu_profile_step) for
         this context's pass variants; "" for a slot with no launch."""
@@ -336,6 +344,9 @@ class Simulation:
     def particles(self) -> dict:
         a = np.zeros((max(self.Np, 1), P_STRIDE))
         self._check(self.L.kapsel_gpu_get_particles(self.h, _ptr(a)))
+        return self._records(a)
+
+    def _records(self, a: np.ndarray) -> dict:
         a = a[: self.Np]
         names = ["x", "v", "omega", "f_hydro", "torque_hydro", "fr", "x_nopbc", "v_old", "omega_old"]
         out = {n: a[:, 3 * i: 3 * i + 3].copy() for i, n in enumerate(names)}

@@ -352,6 +352,7 @@ struct BoxBase {
   }
   void drop_prefill() { noise_pre_ts[0] = noise_pre_ts[1] = -1; }
   DPart *parts_host = nullptr;  // pinned staging of the particle readout
+  int *status_host = nullptr;   // pinned copy of the status word
 };
 
 // threads per block of the x passes of the Navier-Stokes step (multiples of
@@ -1941,6 +1942,7 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   const int np1 = b->Np > 0 ? b->Np : 1;
   if (cudaMalloc(&b->parts, sizeof(DPart) * np1) != cudaSuccess) return KAPSEL_ENOMEM;
   if (cudaMallocHost(&b->parts_host, sizeof(DPart) * np1) != cudaSuccess) return KAPSEL_ENOMEM;
+  if (cudaMallocHost(&b->status_host, sizeof(int)) != cudaSuccess) return KAPSEL_ENOMEM;
   if (cudaMemset(b->parts, 0, sizeof(DPart) * np1) != cudaSuccess) return KAPSEL_ECUDA;
   if (cudaMalloc(&b->cells, sizeof(int) * cells.size()) != cudaSuccess) return KAPSEL_ENOMEM;
   if (cudaMemcpy(b->cells, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -1993,6 +1995,7 @@ int kapsel_gpu_destroy(kapsel_ctx *ctx) {
     b->free_cells();
     cudaFree(b->parts);
     cudaFreeHost(b->parts_host);
+    cudaFreeHost(b->status_host);
     cudaFree(b->cells);
     cudaFree(b->uk_dc);
     cudaFree(b->status);
@@ -2082,7 +2085,8 @@ static int check_status(BoxBase *b) {
   return st;
 }
 
-static int step_impl(kapsel_ctx *ctx, int n, bool use_graph) {
+// n steps enqueued on the context's stream (no synchronisation)
+static int step_loop(kapsel_ctx *ctx, int n, bool use_graph) {
   if (!ctx || n < 0) return KAPSEL_EINVAL;
   BoxBase *b = ctx->box.get();
   if (!b->initialised) return KAPSEL_ESTATE;
@@ -2110,7 +2114,36 @@ static int step_impl(kapsel_ctx *ctx, int n, bool use_graph) {
     b->time += b->prm.dt;
     if ((rc = b->prefill_noise())) return rc;
   }
-  return check_status(b);
+  return 0;
+}
+
+static int step_impl(kapsel_ctx *ctx, int n, bool use_graph) {
+  const int rc = step_loop(ctx, n, use_graph);
+  return rc ? rc : check_status(ctx->box.get());
+}
+
+// The particle records (KAPSEL_P_STRIDE doubles each) of the pinned copy.
+static void particle_records(const BoxBase *b, double *out) {
+  const DPart *h = b->parts_host;
+  for (int n = 0; n < b->Np; ++n) {
+    double *o = out + (size_t)KAPSEL_P_STRIDE * n;
+    const DPart &a = h[n];
+    for (int d = 0; d < 3; ++d) {
+      o[KAPSEL_P_X + d] = a.x[d];
+      o[KAPSEL_P_V + d] = a.v[d];
+      o[KAPSEL_P_OMEGA + d] = a.omega[d];
+      o[KAPSEL_P_FHYDRO + d] = a.f_hydro_prev[d];
+      o[KAPSEL_P_THYDRO + d] = a.t_hydro_prev[d];
+      o[KAPSEL_P_FR + d] = a.fr_prev[d];
+      o[KAPSEL_P_XNOPBC + d] = a.x_nopbc[d];
+      o[KAPSEL_P_VOLD + d] = a.v_old[d];
+      o[KAPSEL_P_OMEGAOLD + d] = a.omega_old[d];
+    }
+    for (int i = 0; i < 4; ++i) {
+      o[KAPSEL_P_Q + i] = a.q[i];
+      o[KAPSEL_P_QOLD + i] = a.q_old[i];
+    }
+  }
 }
 
 int kapsel_gpu_step(kapsel_ctx *ctx, int n) { return step_impl(ctx, n, false); }
@@ -2149,31 +2182,28 @@ int kapsel_gpu_get_velocity(kapsel_ctx *ctx, double *u) {
 int kapsel_gpu_get_particles(kapsel_ctx *ctx, double *out) {
   if (!ctx || (!out && ctx->box->Np > 0)) return KAPSEL_EINVAL;
   BoxBase *b = ctx->box.get();
-  const DPart *h = b->parts_host;  // pinned: a direct DMA, no staging copy
   if (cudaMemcpyAsync(b->parts_host, b->parts, sizeof(DPart) * std::max(b->Np, 1), cudaMemcpyDeviceToHost,
                       b->stream) != cudaSuccess)
     return KAPSEL_ECUDA;
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return KAPSEL_ECUDA;
-  for (int n = 0; n < b->Np; ++n) {
-    double *o = out + (size_t)KAPSEL_P_STRIDE * n;
-    const DPart &a = h[n];
-    for (int d = 0; d < 3; ++d) {
-      o[KAPSEL_P_X + d] = a.x[d];
-      o[KAPSEL_P_V + d] = a.v[d];
-      o[KAPSEL_P_OMEGA + d] = a.omega[d];
-      o[KAPSEL_P_FHYDRO + d] = a.f_hydro_prev[d];
-      o[KAPSEL_P_THYDRO + d] = a.t_hydro_prev[d];
-      o[KAPSEL_P_FR + d] = a.fr_prev[d];
-      o[KAPSEL_P_XNOPBC + d] = a.x_nopbc[d];
-      o[KAPSEL_P_VOLD + d] = a.v_old[d];
-      o[KAPSEL_P_OMEGAOLD + d] = a.omega_old[d];
-    }
-    for (int i = 0; i < 4; ++i) {
-      o[KAPSEL_P_Q + i] = a.q[i];
-      o[KAPSEL_P_QOLD + i] = a.q_old[i];
-    }
-  }
+  particle_records(b, out);
   return 0;
+}
+
+int kapsel_gpu_step_graph_particles(kapsel_ctx *ctx, int n, double *out) {
+  // the copies of the particles and of the status word follow the steps on
+  // the stream, so one synchronisation covers steps, status and readout
+  if (!ctx || (!out && ctx->box->Np > 0)) return KAPSEL_EINVAL;
+  int rc = step_loop(ctx, n, true);
+  if (rc) return rc;
+  BoxBase *b = ctx->box.get();
+  if (cudaMemcpyAsync(b->parts_host, b->parts, sizeof(DPart) * std::max(b->Np, 1), cudaMemcpyDeviceToHost,
+                      b->stream) != cudaSuccess ||
+      cudaMemcpyAsync(b->status_host, b->status, sizeof(int), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess)
+    return KAPSEL_ECUDA;
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) return KAPSEL_ECUDA;
+  particle_records(b, out);
+  return *b->status_host;
 }
 
 int kapsel_gpu_set_particle_state(kapsel_ctx *ctx, const double *in) {

@@ -234,6 +234,24 @@ def test_step_mixed_deterministic_graph_equals_eager():
             assert np.array_equal(a.particles()[k], s.particles()[k]), k
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_step_graph_particles_equals_step_then_readout(precision):
+    """kapsel_gpu_step_graph_particles (steps and particle readout with one
+    host synchronisation) gives the state and records of
+    kapsel_gpu_step_graph followed by kapsel_gpu_get_particles."""
+    cfg = _cfg((6, 6, 6), 12, seed=4, kbt=1e-3, min_gap=0.5)
+    a = _sim(cfg, precision)
+    b = _sim(cfg, precision)
+    for n in (1, 1, 3, 1):
+        a.step(n, graph=True)
+        pa = a.particles()
+        pb = b.step_particles(n)
+        for k in pa:
+            assert np.array_equal(pa[k], pb[k]), k
+    assert np.array_equal(a.zeta(), b.zeta())
+    assert a.time() == b.time()
+
+
 def test_step_fp64_neighbor_lists_match_oracle():
     """The per-step cell and neighbour lists (used above 1024 particles)
     forced on at 32^3, where the reference's LJ cell list has 2 cells per
