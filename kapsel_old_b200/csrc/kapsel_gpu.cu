@@ -649,9 +649,11 @@ struct Box : BoxBase {
       zw_avail = zw;
       if (!zw_ok) zw = 0;
       // FP32: the fused y/z plane kernels wherever the warp-level z kernels
-      // run (128^3 mixed step 0.200 -> 0.189 ms); FP64 planes (90 KB at
-      // 128^3) leave one block per SM and run slower than the separate passes
-      if (sizeof(R) == 4 && zw && yz_ly) ymode = 3;
+      // run and three plane blocks fit on an SM (128^3 mixed step 0.200 ->
+      // 0.189 ms; 256x128x128 0.335 -> 0.316; at 128x128x256, one block per
+      // SM, 0.377 -> 0.395, so not there); FP64 planes (90 KB at 128^3)
+      // leave one block per SM and run slower than the separate passes
+      if (sizeof(R) == 4 && zw && yz_ly && 3 * yz_sm <= 227 * 1024) ymode = 3;
     }
     KCHECK(allow_smem(k_x_zeta_to_u<R, KCX>, smem_xu));
     KCHECK(allow_smem(k_x_advect_update<R, KCX>, smem_xadv));
