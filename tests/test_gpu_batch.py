@@ -109,7 +109,8 @@ def _set_variant(sim, zmode, ymode):
     assert fn(sim.h, zmode, ymode) == 0
 
 
-@pytest.mark.parametrize("shape,n", [((7, 7, 7), 256), ((6, 6, 7), 12), ((6, 6, 6), 6)])
+@pytest.mark.parametrize("shape,n", [((7, 7, 7), 256), ((6, 6, 7), 12), ((6, 6, 6), 6), ((5, 5, 6), 3),
+                                     ((6, 7, 6), 10)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_fused_yz_planes_bitwise(shape, n, precision):
     """Pass variant 3 runs the inverse y + z c2r and the force's z + y passes
