@@ -259,6 +259,36 @@ int kapsel_gpu_make_phi(kapsel_ctx *ctx, double *phi);
    context's own fluid state is replaced by the result. */
 int kapsel_gpu_ns_slaved_euler(kapsel_ctx *ctx, double *zeta, const double *uk_dc);
 
+/* The Electrolyte routines, on an Electrolyte context whose particle state
+   (kapsel_gpu_set_particle_state) gives the positions; concentrations are
+   conc_k[2] in the Ooura layout (2*NX*NY*NZ_ doubles, species 0 then 1), as
+   the reference's Concentration.  KAPSEL_ESTATE on another kind of context.
+
+   NSsolute_solver_Euler (fluid_solver.cxx:306-326, replaces the call of
+   fluid_solver.h:116): Rhs_NS_Nernst_Planck (the potential gradient of the
+   charge, the advection term, and per species Diffusion_flux_single,
+   Solute_solver_rhs_nonlinear_x_single, Solute_impermeability,
+   Add_advection_flux and the flux divergence, solute_rhs.cxx:42-234) and the
+   explicit Euler update of zeta and of both concentrations, in place.  As in
+   the reference, which truncates zeta and conc_k to the 2/3 box before using
+   them, the modes outside the box come back zero; uk_dc is not changed (its
+   right-hand side is zero).  The context's own fluid state is replaced. */
+int kapsel_gpu_ns_solute_euler(kapsel_ctx *ctx, double *zeta, const double *uk_dc, double *conc_k);
+
+/* Rescale_solute (solute_rhs.cxx:99-128, replaces solute_rhs.h:107): the
+   factors total_solute[n] / (DX3 sum (1 - phi) c_n) at the current positions
+   into rescale_factor[2], and conc_k scaled by them in place (2/3-truncated
+   input, as NSsolute_solver_Euler leaves it; modes outside the box come back
+   zero).  The context's own target totals are not changed. */
+int kapsel_gpu_rescale_solute(kapsel_ctx *ctx, const double *total_solute, double *conc_k, double *rescale_factor);
+
+/* Make_Coulomb_force_x_on_fluid (operate_electrolyte.cxx:90-177, replaces
+   the call of operate_electrolyte.h:78) at the current positions: the force
+   density rho_e (-grad psi + E_ext) of the charge field of Conc_k2charge_field
+   (operate_electrolyte.cxx:45-74) and conc_k, with the potential of the full
+   (untruncated) spectrum, as three NX*NY*NZ_ fields (row padding zero). */
+int kapsel_gpu_coulomb_force(kapsel_ctx *ctx, const double *conc_k, double *f0, double *f1, double *f2);
+
 /* MD_solver_position_Euler (euler != 0) / MD_solver_position_AB2
    (particle_solver.cxx:36-88) on the context's particle state (set it with
    kapsel_gpu_set_particle_state, read it with kapsel_gpu_get_particles). */

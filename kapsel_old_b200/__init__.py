@@ -116,6 +116,9 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_calc_lj": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_make_phi": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_ns_slaved_euler": (ctypes.c_int, [_VP, _DP, _DP]),
+        "kapsel_gpu_ns_solute_euler": (ctypes.c_int, [_VP, _DP, _DP, _DP]),
+        "kapsel_gpu_rescale_solute": (ctypes.c_int, [_VP, _DP, _DP, _DP]),
+        "kapsel_gpu_coulomb_force": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP]),
         "kapsel_gpu_md_position": (ctypes.c_int, [_VP, ctypes.c_int]),
         "kapsel_gpu_md_velocity": (ctypes.c_int, [_VP, _DP, _DP, ctypes.c_int]),
         "kapsel_gpu_set_time": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_double]),

@@ -315,6 +315,11 @@ struct BoxBase {
   virtual int fhydro_host(const double *u0, const double *u1, const double *u2, double *f, double *t) = 0;
   // NS_solver_slavedEuler on a host zeta (Ooura layout): retained modes updated in place
   virtual int slaved_euler_host(double *z, const double *ukdc) = 0;
+  // the Electrolyte routines NSsolute_solver_Euler, Rescale_solute and
+  // Make_Coulomb_force_x_on_fluid on host arrays (Ooura layout)
+  virtual int ns_solute_host(double *z, const double *ukdc, double *c) = 0;
+  virtual int rescale_solute_host(const double *total, double *c, double *factors) = 0;
+  virtual int coulomb_force_host(const double *c, double *f0, double *f1, double *f2) = 0;
   virtual void free_all() = 0;
 
   int fill_noise(int slot) {
@@ -1096,9 +1101,12 @@ struct Box : BoxBase {
     k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(g, tw, bufB, out, npts(), g.NZ, PPar{}, nullptr, 0, nullptr);
   }
 
-  void launch_step_el(int euler) {
+  // NSsolute_solver_Euler (fluid_solver.cxx:306-326): Rhs_NS_Nernst_Planck
+  // at the current positions, then the explicit Euler update of zeta and of
+  // both ion concentrations (uk_dc is unchanged: its rhs is zero,
+  // fluid_solver.cxx:176-178)
+  void launch_el_fluid() {
     const size_t N = npts(), nz = (size_t)g.KXc * g.KYc * g.TS;
-    const double dx3 = prm.dx * prm.dx * prm.dx;
     const double ve[2] = {prm.valency_p, prm.valency_n}, L[2] = {prm.onsager_p, prm.onsager_n};
     const double ieps = 1.0 / prm.dielectric;
     const int pb = 592;
@@ -1129,17 +1137,29 @@ struct Box : BoxBase {
       k_x_fwd_op<R, KCX, XF_CONCUPD, 3><<<gx(), 256, sm_el, stream>>>(g, tw, bufA, conc_k + n * nz, 0,
                                                                          KOp{prm.dt, {0, 0, 0}});
     }
-    if (Np > 0) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
-    launch_cells();
-    // Rescale_solute at the new positions, then the Coulomb force
+  }
+  // Rescale_solute (solute_rhs.cxx:99-128) at the current positions: the
+  // factors total[n] / (sum (1 - phi) c_n DX3) into scal[1..2], conc_k scaled.
+  // phiq then holds phi and the surface charge of these positions and creal
+  // the concentrations before the scaling.
+  void launch_el_rescale() {
+    const size_t N = npts(), nz = (size_t)g.KXc * g.KYc * g.TS;
+    const double dx3 = prm.dx * prm.dx * prm.dx;
     el_scatter(0);
     el_surface_scale();
     el_conc_real();
     k_reduce_partial<R, RED_PHI_C><<<RED_BLOCKS, 256, 0, stream>>>(N, phiq, creal, N, 2, partial);
     k_reduce_final<<<1, 256, 0, stream>>>(partial, RED_BLOCKS, 2, 1, 0.0, total_solute, dx3, scal);
-    k_scale_conc<R><<<pb, 256, 0, stream>>>(nz, conc_k, scal);
-    k_el_charge<R><<<pb, 256, 0, stream>>>(N, phiq, creal, scal, 1, ve[0], ve[1], charge);
-    // full (untruncated) potential gradient with the Ooura inverse semantics
+    k_scale_conc<R><<<592, 256, 0, stream>>>(nz, conc_k, scal);
+  }
+  // Make_Coulomb_force_x_on_fluid (operate_electrolyte.cxx:90-177) from the
+  // charge field: the full (untruncated) potential gradient with the Ooura
+  // inverse semantics, then f = charge (-grad psi + E_ext), times `scale`,
+  // into fluxr
+  void launch_el_coulomb(double scale) {
+    const size_t N = npts();
+    const double ieps = 1.0 / prm.dielectric;
+    const int pb = 592;
     const size_t nfull = (size_t)g.NX * g.NY * gF.TS;
     k_z_r2c<R><<<dim3(gz(), 1), 256, sm_el, stream>>>(gF, tw, charge, g.NZ, N, F2, gF.TZ, gF.TS);
     launch_y<false>(gF, 1, F2, F1);
@@ -1151,7 +1171,20 @@ struct Box : BoxBase {
     k_z_c2r<R><<<dim3(gz(), 3), 256, sm_el, stream>>>(gF, tw, F2, gradr, N, g.NZ, PPar{}, nullptr, 0, nullptr);
     const bool ext = ext_on();
     k_el_coulomb<R><<<pb, 256, 0, stream>>>(N, charge, gradr, ext ? prm.e_ext[0] : 0.0, ext ? prm.e_ext[1] : 0.0,
-                                            ext ? prm.e_ext[2] : 0.0, prm.dt / prm.rho, fluxr);
+                                            ext ? prm.e_ext[2] : 0.0, scale, fluxr);
+  }
+
+  void launch_step_el(int euler) {
+    const size_t N = npts();
+    const double ve[2] = {prm.valency_p, prm.valency_n};
+    launch_el_fluid();
+    if (Np > 0) k_particles_position<<<(Np + 127) / 128, 128, 0, stream>>>(pp, parts, euler, status);
+    launch_cells();
+    // Rescale_solute at the new positions, then the Coulomb force (the
+    // charge from the concentrations before the scaling times the factors)
+    launch_el_rescale();
+    k_el_charge<R><<<592, 256, 0, stream>>>(N, phiq, creal, scal, 1, ve[0], ve[1], charge);
+    launch_el_coulomb(prm.dt / prm.rho);
     // u += f dt/rho; Solenoidal_u: in k-space zeta += zeta(sol f), uk_dc += f(0)
     el_forward_trunc(fluxr, 3);
     x_force(false, bufA);
@@ -1347,6 +1380,88 @@ struct Box : BoxBase {
           const size_t o = c * plane + ((size_t)i * g.NY + j) * NZ_;
           memcpy(z + o, full.data() + o, sizeof(double) * 2 * g.TZ);
         }
+      }
+    return 0;
+  }
+
+  // NSsolute_solver_Euler (fluid_solver.cxx:306-326) on host arrays: zeta
+  // and both concentrations updated in place.  The reference truncates both
+  // to the 2/3 box before it uses them (Rhs_NS_solute, fluid_solver.cxx:
+  // 200-210) and updates only that box, so the modes outside it come back
+  // zero.  uk_dc is not changed (its right-hand side is zero).
+  int ns_solute_host(double *z, const double *ukdc, double *c) override {
+    if (prm.eq != KAPSEL_EQ_ELECTROLYTE || !conc_k) return KAPSEL_EINVAL;
+    int rc = zeta_from_host(z);
+    if (!rc) rc = conc_from_host(c);
+    if (rc) return rc;
+    KCHECK(cudaMemcpyAsync(uk_dc, ukdc, sizeof(double) * 3, cudaMemcpyHostToDevice, stream));
+    launch_cells();
+    launch_el_fluid();
+    KCHECK(cudaGetLastError());
+    // the update applied FIX_CELL to the device uk_dc and overwrote bufA
+    KCHECK(cudaMemcpyAsync(uk_dc, ukdc, sizeof(double) * 3, cudaMemcpyHostToDevice, stream));
+    u_spec_ready = false;
+    if ((rc = zeta_to_host(z))) return rc;
+    return conc_to_host(c);
+  }
+
+  // Rescale_solute (solute_rhs.cxx:99-128) on host concentrations at the
+  // current positions with the caller's target totals; the factors are
+  // returned.  The concentrations are the 2/3-truncated ones that
+  // NSsolute_solver_Euler leaves (the modes outside the box come back zero).
+  // The context's own targets are not changed.
+  int rescale_solute_host(const double *total, double *c, double *factors) override {
+    if (prm.eq != KAPSEL_EQ_ELECTROLYTE || !conc_k) return KAPSEL_EINVAL;
+    int rc = conc_from_host(c);
+    if (rc) return rc;
+    double *own = total_solute, *tmp = nullptr;
+    if (cudaMalloc(&tmp, sizeof(double) * 2) != cudaSuccess) return KAPSEL_ENOMEM;
+    if (cudaMemcpyAsync(tmp, total, sizeof(double) * 2, cudaMemcpyHostToDevice, stream) != cudaSuccess) rc = KAPSEL_ECUDA;
+    if (!rc) {
+      total_solute = tmp;
+      launch_cells();
+      launch_el_rescale();
+      total_solute = own;
+      if (cudaGetLastError() != cudaSuccess) rc = KAPSEL_ECUDA;
+    }
+    double h[3] = {0.0, 0.0, 0.0};
+    if (!rc && cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess) rc = KAPSEL_ECUDA;
+    if (!rc) rc = conc_to_host(c);  // synchronises the stream
+    cudaFree(tmp);
+    if (rc) return rc;
+    factors[0] = h[1];
+    factors[1] = h[2];
+    return 0;
+  }
+
+  // Make_Coulomb_force_x_on_fluid (operate_electrolyte.cxx:90-177) from host
+  // concentrations at the current positions: the force density
+  // charge * (-grad psi + E_ext) as three real fields in the reference layout
+  // (NX*NY*NZ_ doubles each, the two padding entries of a row zero).
+  int coulomb_force_host(const double *c, double *f0, double *f1, double *f2) override {
+    if (prm.eq != KAPSEL_EQ_ELECTROLYTE || !conc_k) return KAPSEL_EINVAL;
+    int rc = conc_from_host(c);
+    if (rc) return rc;
+    const size_t N = npts();
+    launch_cells();
+    el_scatter(0);
+    el_surface_scale();
+    el_conc_real();
+    k_el_charge<R><<<592, 256, 0, stream>>>(N, phiq, creal, scal, 0, prm.valency_p, prm.valency_n, charge);
+    launch_el_coulomb(1.0);
+    KCHECK(cudaGetLastError());
+    std::vector<R> h(3 * N);
+    KCHECK(cudaMemcpyAsync(h.data(), fluxr, sizeof(R) * h.size(), cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    double *f[3] = {f0, f1, f2};
+    const int NZ_ = g.NZ + 2;
+    const size_t rows = (size_t)g.NX * g.NY;
+    for (int d = 0; d < 3; ++d)
+      for (size_t r = 0; r < rows; ++r) {
+        double *o = f[d] + r * NZ_;
+        const R *in = h.data() + d * N + r * g.NZ;
+        for (int k = 0; k < g.NZ; ++k) o[k] = (double)in[k];
+        o[g.NZ] = o[g.NZ + 1] = 0.0;
       }
     return 0;
   }
@@ -2354,6 +2469,42 @@ int kapsel_gpu_ns_slaved_euler(kapsel_ctx *ctx, double *zeta, const double *uk_d
   if (rc) return rc;
   b->initialised = true;
   return check_status(b);
+}
+
+// The Electrolyte routines behind their reference names: the context must
+// be an Electrolyte one; its particle state (kapsel_gpu_set_particle_state)
+// gives the positions.
+static int el_routine_ready(kapsel_ctx *ctx) {
+  BoxBase *b = ctx->box.get();
+  if (b->prm.eq != KAPSEL_EQ_ELECTROLYTE) return KAPSEL_ESTATE;
+  if (b->Np > 0 && !b->particles_set) return KAPSEL_ESTATE;
+  return 0;
+}
+
+int kapsel_gpu_ns_solute_euler(kapsel_ctx *ctx, double *zeta, const double *uk_dc, double *conc_k) {
+  if (!ctx || !zeta || !uk_dc || !conc_k) return KAPSEL_EINVAL;
+  int rc = el_routine_ready(ctx);
+  if (rc) return rc;
+  BoxBase *b = ctx->box.get();
+  if ((rc = b->ns_solute_host(zeta, uk_dc, conc_k))) return rc;
+  b->initialised = true;
+  return check_status(b);
+}
+
+int kapsel_gpu_rescale_solute(kapsel_ctx *ctx, const double *total_solute, double *conc_k, double *rescale_factor) {
+  if (!ctx || !total_solute || !conc_k || !rescale_factor) return KAPSEL_EINVAL;
+  int rc = el_routine_ready(ctx);
+  if (rc) return rc;
+  if ((rc = ctx->box->rescale_solute_host(total_solute, conc_k, rescale_factor))) return rc;
+  return check_status(ctx->box.get());
+}
+
+int kapsel_gpu_coulomb_force(kapsel_ctx *ctx, const double *conc_k, double *f0, double *f1, double *f2) {
+  if (!ctx || !conc_k || !f0 || !f1 || !f2) return KAPSEL_EINVAL;
+  int rc = el_routine_ready(ctx);
+  if (rc) return rc;
+  if ((rc = ctx->box->coulomb_force_host(conc_k, f0, f1, f2))) return rc;
+  return check_status(ctx->box.get());
 }
 
 int kapsel_gpu_md_position(kapsel_ctx *ctx, int euler) {

@@ -17,6 +17,11 @@
  *                                                   md_force.h:75, calls)
  *     MD_solver_position_Euler / _AB2              particle_solver.h:38,55
  *     MD_solver_velocity_Euler / _AB2_hydro        particle_solver.h:62,71
+ *     NSsolute_solver_Euler                        fluid_solver.h:116 (with
+ *                                                   the solute_rhs.cxx routines
+ *                                                   it calls)
+ *     Rescale_solute                               solute_rhs.h:107
+ *     Make_Coulomb_force_x_on_fluid                operate_electrolyte.h:78
  *
  * so that the reference's main loop (sp_3d_ns.cxx:442-657) runs unchanged on
  * the GPU once the reference's own definitions of these names are removed
@@ -30,9 +35,11 @@
  *   - the whole-step shims: one context per zeta[0] (the run's state lives
  *     on the device between steps; the first call uploads zeta, uk_dc, the
  *     particles (and the ion concentrations) and the step counter);
- *   - the routine shims: one work context per process, whose particle and
- *     field state every call uploads from the arguments and whose results
- *     every call writes back (the routines have no state of their own).
+ *   - the routine shims: one work context per process (and a second one,
+ *     of the Electrolyte kind, for the Electrolyte routines), whose particle
+ *     and field state every call uploads from the arguments and whose
+ *     results every call writes back (the routines have no state of their
+ *     own).
  * Host mirrors of the whole-step state: the particles after every step; zeta,
  * uk_dc (and the concentrations) after the steps whose state the main loop
  * reads -- ts+1 a multiple of GTS (Output_udf / Output_avs at the top of the
@@ -107,6 +114,10 @@ void check_supported() {
     if (PINNING) shim_fail("pinned particles", 0);
   }
   if (DBG_MASS_GRID) shim_fail("DBG_MASS_GRID", 0);
+  if (SW_EQ == Electrolyte) {
+    if (N_spec != 2) shim_fail("an ion model other than two species (salt)", 0);
+    if (External_field && AC) shim_fail("an AC external electric field", 0);
+  }
 }
 
 // kapsel_params from the reference's globals (set by Gourmet_file_io and
@@ -363,6 +374,35 @@ kapsel_ctx *work_ctx() {
   return g_work;
 }
 
+kapsel_ctx *g_work_el = nullptr;
+
+// true when every mode of the two k-space fields outside the 2/3 box
+// (Truncate_two_third_rule_ooura, fft_wrapper.h:723-766) is zero: the
+// library keeps only the box, so a field with modes outside it (an initial
+// profile other than Uniform, operate_electrolyte.cxx:490-515) is refused
+bool truncated2(double *const *a) {
+  for (int f = 0; f < 2; f++)
+    for (int i = 0; i < NX; i++)
+      for (int j = 0; j < NY; j++) {
+        const bool row_in = (i < TRN_X || i > NX - TRN_X) && (j < TRN_Y || j > NY - TRN_Y);
+        const double *r = a[f] + ((size_t)i * NY + j) * NZ_;
+        for (int k = row_in ? 2 * TRN_Z : 0; k < NZ_; k++)
+          if (r[k] != 0.0) return false;
+      }
+  return true;
+}
+
+kapsel_ctx *work_ctx_el() {
+  if (SW_EQ != Electrolyte) shim_fail("an Electrolyte routine outside the Electrolyte branch", 0);
+  if (!g_work_el) {
+    kapsel_params prm = params_from_globals();
+    check(kapsel_gpu_create(&prm, &g_work_el), "kapsel_gpu_create");
+    fprintf(stderr, "kapsel shim: Electrolyte routines on the GPU (%dx%dx%d, %d particles)\n", NX, NY, NZ,
+            Particle_Number);
+  }
+  return g_work_el;
+}
+
 void upload_particles(kapsel_ctx *c, const Particle *p) {
   if (Particle_Number == 0) return;
   std::vector<double> rec;
@@ -520,4 +560,52 @@ void MD_solver_position_Euler(Particle *p, const CTime &jikan) { position_update
 void MD_solver_position_AB2(Particle *p, const CTime &jikan) { position_update(p, jikan, 0); }
 void MD_solver_velocity_Euler(Particle *p, const CTime &jikan) { velocity_update(p, jikan, 1); }
 void MD_solver_velocity_AB2_hydro(Particle *p, const CTime &jikan) { velocity_update(p, jikan, 0); }
+
+void NSsolute_solver_Euler(double **zeta, const CTime &jikan, double uk_dc[DIM], double **concentration_k,
+                           Particle *p, const Index_range *ijk_range, const int &n_ijk_range) {
+  // the ranges are the 2/3 box (sp_3d_ns.cxx:46-58), the only ones the
+  // reference passes; zeta and the concentrations come back truncated to it,
+  // as the reference leaves them (Rhs_NS_solute truncates both first)
+  (void)ijk_range;
+  (void)n_ijk_range;
+  if (jikan.dt_fluid != DT) shim_fail("a fluid time step other than DT", 0);
+  kapsel_ctx *c = work_ctx_el();
+  upload_particles(c, p);
+  std::vector<double> z, conc;
+  pack2(zeta, z);
+  pack2(concentration_k, conc);
+  check(kapsel_gpu_ns_solute_euler(c, z.data(), uk_dc, conc.data()), "kapsel_gpu_ns_solute_euler");
+  unpack2(z, zeta);
+  unpack2(conc, concentration_k);
+}
+
+void Rescale_solute(double *rescale_factor, double *total_solute, double **conc_k, Particle *p, double *phi,
+                    double *conc_x) {
+  // phi and conc_x are the reference's working memory; no caller reads them
+  // afterwards (sp_3d_ns.cxx:89-95 resets phi next; fluid_solver.cxx:296-301)
+  (void)phi;
+  (void)conc_x;
+  kapsel_ctx *c = work_ctx_el();
+  if (!truncated2(conc_k)) shim_fail("Rescale_solute on concentrations with modes outside the 2/3 box", 0);
+  upload_particles(c, p);
+  std::vector<double> conc;
+  pack2(conc_k, conc);
+  check(kapsel_gpu_rescale_solute(c, total_solute, conc.data(), rescale_factor), "kapsel_gpu_rescale_solute");
+  unpack2(conc, conc_k);
+}
+
+void Make_Coulomb_force_x_on_fluid(double **force, Particle *p, double **conc_k, double *charge_density,
+                                   double *potential, const CTime &jikan) {
+  // charge_density and potential are working memory (up[0], up[1] in
+  // Time_evolution_hydro, reset before their next use); the DC field only
+  (void)charge_density;
+  (void)potential;
+  (void)jikan;
+  kapsel_ctx *c = work_ctx_el();
+  if (!truncated2(conc_k)) shim_fail("the Coulomb force of concentrations with modes outside the 2/3 box", 0);
+  upload_particles(c, p);
+  std::vector<double> conc;
+  pack2(conc_k, conc);
+  check(kapsel_gpu_coulomb_force(c, conc.data(), force[0], force[1], force[2]), "kapsel_gpu_coulomb_force");
+}
 #endif  // KAPSEL_SHIM_ROUTINES

@@ -8,10 +8,14 @@ reference objects read the same input file and run the same steps:
                             whole-step shim (state on the GPU between steps);
   kapsel_ref_main_routines  NS_solver_slavedEuler, Make_phi_u_particle,
                             Calc_f_hydro_correct_precision, the LJ cell-list
-                            force and MD_solver_position/velocity_* replaced
-                            by the routine shims (host arrays in and out).
-Their restart records (Save_Restart_udf at MSTEP) and output records
-(Output_udf every GTS steps) are compared.  Tolerances: FP64 relative error
+                            force, MD_solver_position/velocity_* and the
+                            Electrolyte routines (NSsolute_solver_Euler,
+                            Rescale_solute, Make_Coulomb_force_x_on_fluid)
+                            replaced by the routine shims (host arrays in
+                            and out).
+Their restart records (Save_Restart_udf at MSTEP; with the ion
+concentrations in the Electrolyte branch) and output records (Output_udf
+every GTS steps) are compared.  Tolerances: FP64 relative error
 <= 1e-10 per quantity (zeta compared on the 2/3-truncated modes that every
 step reads; the whole-step shim's host zeta holds only those); with
 KAPSEL_SHIM_PRECISION=mixed the velocity-field bound of the mixed path,
@@ -94,6 +98,24 @@ def _restart_state(rec, cfg):
     return {"zeta": z, "uk_dc": ukdc, "ts": rec[base + "jikan.ts"], **parts}
 
 
+_CK = re.compile(r"resume\.CONTINUE\.Saved_Data\.Concentration\[(\d+)\]\[(\d+)\]\[(\d+)\]\[(\d+)\]\.ck")
+
+
+def _restart_conc(rec, cfg):
+    """Concentration[n] of an Electrolyte restart record, Ooura layout."""
+    N = [1 << p for p in cfg["np_xyz"]]
+    c = np.zeros((2, N[0], N[1], N[2] + 2))
+    seen = 0
+    for k, v in rec.items():
+        m = _CK.fullmatch(k)
+        if m:
+            n, i, j, kk = (int(g) for g in m.groups())
+            c[n, i, j, kk] = v
+            seen += 1
+    assert seen == c.size, seen
+    return c
+
+
 def _out_particles(recs, n):
     """Per output record: R, v, omega of every particle (Output_udf)."""
     out = []
@@ -123,6 +145,8 @@ def _compare(a, b, cfg, tol, what):
         assert len(oa) == len(ob) > 0
         errs["records_R"] = max(np.abs(y["R"] - x["R"]).max() for x, y in zip(oa, ob))
         errs["records_v"] = max(rel(y["v"], x["v"]) for x, y in zip(oa, ob))
+    if cfg.get("eq") == "Electrolyte":
+        errs["conc"] = rel(_restart_conc(b[0], cfg), _restart_conc(a[0], cfg))
     for k, v in errs.items():
         assert v < tol.get(k, tol["default"]), (what, k, v, errs)
     return errs
@@ -171,6 +195,20 @@ def test_main_loop_whole_step_shim_electrolyte(tmp_path):
     b = _run("step", cfg, str(tmp_path))
     assert "kapsel shim: Time_evolution on the GPU" in b[2]
     _compare(a, b, cfg, {"default": FP64_TOL}, "step electrolyte")
+
+
+def test_main_loop_routine_shims_electrolyte(tmp_path):
+    """NSsolute_solver_Euler (with the solute_rhs routines it calls),
+    Rescale_solute and Make_Coulomb_force_x_on_fluid behind their reference
+    names, with the particle routines, in the reference's main loop; the
+    concentrations are compared as well."""
+    _need("ref", "routines")
+    cfg = udf.electrolyte_config((5, 5, 5), 2, seed=6, efield=(0.05, 0.0, 0.0))
+    cfg["gts"], cfg["num_snap"] = 3, 2
+    a = _run("ref", cfg, str(tmp_path))
+    b = _run("routines", cfg, str(tmp_path))
+    assert "kapsel shim: Electrolyte routines on the GPU" in b[2]
+    _compare(a, b, cfg, {"default": FP64_TOL}, "routines electrolyte")
 
 
 def test_main_loop_whole_step_shim_mixed(tmp_path):
