@@ -188,6 +188,12 @@ int kapsel_gpu_set_oblique(kapsel_ctx *ctx, double degree_oblique, double shear_
 /* Ion concentrations conc_k[2] in the Ooura layout (2*NX*NY*NZ_ doubles;
    the Concentration array of solute_rhs.cxx:16), Electrolyte only. */
 int kapsel_gpu_get_concentration(kapsel_ctx *ctx, double *conc);
+/* Sets them (the retained 2/3 box is kept; a restored or host-modified
+   state, as Force_restore_parameters leaves it, resume.cxx:274-365) and,
+   when total_solute is not NULL, the target totals of Rescale_solute
+   (Total_solute[2], solute_rhs.cxx:20), which Init_rho_ion computed at the
+   start of the run. */
+int kapsel_gpu_set_concentration(kapsel_ctx *ctx, const double *conc, const double *total_solute);
 
 /* ---- Batched ensemble of independent boxes. ---- */
 

@@ -107,6 +107,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_get_oblique": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_set_oblique": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double]),
         "kapsel_gpu_get_concentration": (ctypes.c_int, [_VP, _DP]),
+        "kapsel_gpu_set_concentration": (ctypes.c_int, [_VP, _DP, _DP]),
         "kapsel_gpu_A2a_k": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_A_k2a": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_solenoidal_u": (ctypes.c_int, [_VP, _DP, _DP, _DP]),

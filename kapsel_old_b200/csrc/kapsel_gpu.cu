@@ -298,6 +298,7 @@ struct BoxBase {
   virtual int init_el() = 0;
   virtual int conc_to_host(double *c) = 0;
   virtual int conc_from_host(const double *c) = 0;
+  virtual int total_solute_from_host(const double *t) = 0;  // Total_solute[2]
   virtual void launch_step(const double *noise, int euler, cudaEvent_t *ev = nullptr) = 0;
   virtual void launch_init() = 0;
   // launch the first x pass if bufA does not hold u_k (before a step or a
@@ -1248,6 +1249,13 @@ struct Box : BoxBase {
         }
       }
     KCHECK(cudaMemcpyAsync(conc_k, h.data(), sizeof(Cx<R>) * h.size(), cudaMemcpyHostToDevice, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    return 0;
+  }
+
+  int total_solute_from_host(const double *t) override {
+    if (!total_solute) return KAPSEL_ESTATE;
+    KCHECK(cudaMemcpyAsync(total_solute, t, sizeof(double) * 2, cudaMemcpyHostToDevice, stream));
     KCHECK(cudaStreamSynchronize(stream));
     return 0;
   }
@@ -2394,6 +2402,15 @@ int kapsel_gpu_get_concentration(kapsel_ctx *ctx, double *c) {
   if (!ctx || !c) return KAPSEL_EINVAL;
   if (ctx->box->prm.eq != KAPSEL_EQ_ELECTROLYTE) return KAPSEL_ESTATE;
   return ctx->box->conc_to_host(c);
+}
+
+int kapsel_gpu_set_concentration(kapsel_ctx *ctx, const double *c, const double *total_solute) {
+  if (!ctx || !c) return KAPSEL_EINVAL;
+  BoxBase *b = ctx->box.get();
+  if (b->prm.eq != KAPSEL_EQ_ELECTROLYTE) return KAPSEL_ESTATE;
+  int rc = b->conc_from_host(c);
+  if (rc || !total_solute) return rc;
+  return b->total_solute_from_host(total_solute);
 }
 
 int kapsel_gpu_A2a_k(kapsel_ctx *ctx, double *a) {

@@ -257,6 +257,15 @@ bool host_changed(const StepCtx &s, const Particle *p) {
   return false;
 }
 
+// the ion concentrations and the Rescale_solute targets of the host run
+// (Electrolyte branch)
+void upload_concentrations(kapsel_ctx *c) {
+  if (SW_EQ != Electrolyte) return;
+  std::vector<double> buf;
+  pack2(Concentration, buf);
+  check(kapsel_gpu_set_concentration(c, buf.data(), Total_solute), "kapsel_gpu_set_concentration");
+}
+
 void upload(StepCtx &s, double **zeta, const double *uk_dc, Particle *p, const CTime &jikan) {
   std::vector<double> buf, rec;
   if (Particle_Number > 0) {
@@ -265,7 +274,7 @@ void upload(StepCtx &s, double **zeta, const double *uk_dc, Particle *p, const C
   }
   pack2(zeta, buf);
   check(kapsel_gpu_set_zeta(s.ctx, buf.data(), uk_dc), "kapsel_gpu_set_zeta");
-  if (SW_EQ == Electrolyte) shim_fail("resuming an Electrolyte run on the GPU (host concentrations)", 0);
+  upload_concentrations(s.ctx);
   if (SW_EQ == Shear_Navier_Stokes_Lees_Edwards)
     check(kapsel_gpu_set_oblique(s.ctx, degree_oblique, Shear_rate_eff), "kapsel_gpu_set_oblique");
   check(kapsel_gpu_set_time(s.ctx, jikan.ts, jikan.time), "kapsel_gpu_set_time");
@@ -293,9 +302,8 @@ StepCtx &attach(double **zeta, double *uk_dc, Particle *p, const CTime &jikan) {
       }
       check(kapsel_gpu_set_particles(s.ctx, x.data(), q.data()), "kapsel_gpu_set_particles");
     }
-    // the device's own initialisation; in the Electrolyte branch it includes
-    // Init_rho_ion (operate_electrolyte.cxx), which the reference's main ran
-    // on the same particles, so the device concentrations are the host's
+    // the device's own initialisation (its fields are replaced by the host's
+    // below)
     check(kapsel_gpu_init_state(s.ctx), "kapsel_gpu_init_state");
     fprintf(stderr, "kapsel shim: Time_evolution on the GPU (%dx%dx%d, %d particles, %s)\n", NX, NY, NZ,
             Particle_Number, prm.precision == KAPSEL_FP64 ? "FP64" : "mixed");
@@ -309,6 +317,7 @@ StepCtx &attach(double **zeta, double *uk_dc, Particle *p, const CTime &jikan) {
     }
     pack2(zeta, buf);
     check(kapsel_gpu_set_zeta(a.ctx, buf.data(), uk_dc), "kapsel_gpu_set_zeta");
+    upload_concentrations(a.ctx);
     if (SW_EQ == Shear_Navier_Stokes_Lees_Edwards)
       check(kapsel_gpu_set_oblique(a.ctx, degree_oblique, Shear_rate_eff), "kapsel_gpu_set_oblique");
     check(kapsel_gpu_set_time(a.ctx, jikan.ts, jikan.time), "kapsel_gpu_set_time");

@@ -62,10 +62,11 @@ def _records(path):
     return out
 
 
-def _run(which, cfg, tmp, env=None):
+def _run(which, cfg, tmp, env=None, extra=()):
     d = os.path.join(tmp, which)
     os.makedirs(d, exist_ok=True)
     lines = [("output.UDF = ON" if s.startswith("output.UDF") else s) for s in udf.spm_udf_lines(cfg)]
+    lines += list(extra)  # later lines win (the stand-in UDF reader)
     kv = os.path.join(d, "in.kv")
     with open(kv, "w") as f:
         f.write("\n".join(lines) + "\n")
@@ -195,6 +196,26 @@ def test_main_loop_whole_step_shim_electrolyte(tmp_path):
     b = _run("step", cfg, str(tmp_path))
     assert "kapsel shim: Time_evolution on the GPU" in b[2]
     _compare(a, b, cfg, {"default": FP64_TOL}, "step electrolyte")
+
+
+def test_main_loop_whole_step_shim_electrolyte_resumed(tmp_path):
+    """A resumed Electrolyte run (resume.Calculation = CONTINUE with the
+    reference's own restart record of step 6): the whole-step shim uploads
+    the restored zeta, particles, ion concentrations and Rescale_solute
+    targets and continues to step 12 as the reference does."""
+    _need("ref", "step")
+    cfg = udf.electrolyte_config((5, 5, 5), 2, seed=6, efield=(0.05, 0.0, 0.0))
+    cfg["gts"], cfg["num_snap"] = 3, 2
+    _run("ref", cfg, str(tmp_path / "first"))
+    with open(os.path.join(str(tmp_path / "first"), "ref", "res.kv")) as f:
+        saved = [ln for ln in f.read().splitlines() if "resume.CONTINUE.Saved_Data." in ln]
+    extra = ["resume.Calculation = CONTINUE"] + saved
+    cont = dict(cfg, num_snap=4)
+    a = _run("ref", cont, str(tmp_path / "cont"), extra=extra)
+    b = _run("step", cont, str(tmp_path / "cont"), extra=extra)
+    assert "kapsel shim: Time_evolution on the GPU" in b[2]
+    assert _restart_state(a[0], cont)["ts"] == 12
+    _compare(a, b, cont, {"default": FP64_TOL}, "step electrolyte resumed")
 
 
 def test_main_loop_routine_shims_electrolyte(tmp_path):
