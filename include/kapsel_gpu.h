@@ -163,7 +163,14 @@ int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path);
    pressure tau_xy tau_yz tau_zx tau_xx tau_yy, x fastest.  phi is the
    unclamped profile sum of Make_phi_particle; tau is ETA times the
    symmetric strain rate of the velocity by the spectral formula of
-   Zeta_k2Strain_k; the pressure column is zero (the step computes none). */
+   Zeta_k2Strain_k; the pressure column is zero (the step computes none).
+   On an Electrolyte context the snapshot is Output_avs_charge's
+   (avs_output.cxx:451-549): columns ux uy uz phi surface_charge rho
+   e_potential -- phi and the normalised surface charge density (times
+   4 pi a^2) of Make_phi_qq_particle, the ionic charge density (1 - phi)
+   sum_n z_n c_n, and the Coulomb potential of the total charge over the
+   full spectrum.  Unlike the reference, which transforms its concentrations
+   to real space and back in place, the state is not changed. */
 int kapsel_gpu_write_avs(kapsel_ctx *ctx, const char *out_dir, const char *out_name, int nstep, int init);
 
 /* Time step counter jikan.ts and time jikan.time. */

@@ -19,7 +19,7 @@ struct KOp {
 };
 
 enum { XI_IDENT = 0, XI_GRADPSI = 1, XI_GRADDIFF = 2 };
-enum { XF_STORE = 0, XF_CONCUPD = 1, XF_GRADPSI_FULL = 2 };
+enum { XF_STORE = 0, XF_CONCUPD = 1, XF_GRADPSI_FULL = 2, XF_PSI_FULL = 3 };
 
 // x pass, inverse, with a k-space operator on the (compact) input spectra:
 //   XI_IDENT     out_c = in_c                        (NOUT == NIN)
@@ -98,6 +98,8 @@ __global__ void __launch_bounds__(256) k_x_inv_op(Geo g, Twiddles<R> tw, const C
 //                    concentration part of Field_solver_Euler, fluid_solver.cxx:122-135)
 //   XF_GRADPSI_FULL  out[d][o] = -i k_d X_0 IK2 a       (full spectrum, no truncation:
 //                    Make_Coulomb_force_x_on_fluid, operate_electrolyte.cxx:97-101)
+//   XF_PSI_FULL      out[o] = X_0 IK2 a                 (full spectrum: the Coulomb
+//                    potential of Output_avs_charge, avs_output.cxx:464-466)
 // out planes are out_cstride apart.
 template <typename R, int KC, int OP, int NIN>
 __global__ void __launch_bounds__(256) k_x_fwd_op(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ in,
@@ -141,6 +143,10 @@ __global__ void __launch_bounds__(256) k_x_fwd_op(Geo g, Twiddles<R> tw, const C
       const Cx<R> dv = {kx * f0.y + ky * f1.y + kzr * f2.y, -(kx * f0.x + ky * f1.x + kzr * f2.x)};
       const R dt = R(op.a);
       out[o] = {out[o].x + dt * dv.x, out[o].y + dt * dv.y};
+    } else if (OP == XF_PSI_FULL) {
+      const R k2 = kx * kx + ky * ky + kzr * kzr;
+      const R s = k2 > R(0) ? R(op.a) / k2 : R(0);
+      out[o] = {p[0].x * s, p[0].y * s};
     } else {
       const R k2 = kx * kx + ky * ky + kzr * kzr;
       const R s = k2 > R(0) ? R(op.a) / k2 : R(0);

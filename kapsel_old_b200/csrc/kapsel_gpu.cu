@@ -321,6 +321,7 @@ struct BoxBase {
   virtual int ns_solute_host(double *z, const double *ukdc, double *c) = 0;
   virtual int rescale_solute_host(const double *total, double *c, double *factors) = 0;
   virtual int coulomb_force_host(const double *c, double *f0, double *f1, double *f2) = 0;
+  virtual int el_snapshot_host(double *phi, double *surf, double *conc, double *pot) = 0;
   virtual void free_all() = 0;
 
   int fill_noise(int slot) {
@@ -1059,6 +1060,8 @@ struct Box : BoxBase {
     KCHECK(allow_smem(k_x_fwd_op<R, KCX, XF_STORE, 1>, sm));
     KCHECK(allow_smem(k_x_fwd_op<R, KCX, XF_CONCUPD, 3>, sm));
     KCHECK(allow_smem(k_x_fwd_op<R, KCX, XF_GRADPSI_FULL, 1>, sm));
+    KCHECK(allow_smem(k_x_fwd_op<R, KCX, XF_PSI_FULL, 1>, sm));
+    KCHECK(allow_smem(k_x_inv_op<R, KCX, XI_IDENT, 1, 1>, sm));
     KCHECK(allow_smem(k_z_r2c<R>, sm));
     KCHECK(allow_smem(k_z_c2r<R>, sm));
     KCHECK(allow_smem(k_y_pass<R, true, KCY>, sm));
@@ -1173,6 +1176,58 @@ struct Box : BoxBase {
     const bool ext = ext_on();
     k_el_coulomb<R><<<pb, 256, 0, stream>>>(N, charge, gradr, ext ? prm.e_ext[0] : 0.0, ext ? prm.e_ext[1] : 0.0,
                                             ext ? prm.e_ext[2] : 0.0, scale, fluxr);
+  }
+
+  // the Coulomb potential of the charge field (Conc_k2charge_field, A2a_k,
+  // Charge_field_k2Coulomb_potential_k_PBC, A_k2a over the full spectrum;
+  // avs_output.cxx:463-466) into out[N]
+  void launch_el_potential(R *out) {
+    const size_t N = npts();
+    const size_t nfull = (size_t)g.NX * g.NY * gF.TS;
+    k_z_r2c<R><<<dim3(gz(), 1), 256, sm_el, stream>>>(gF, tw, charge, g.NZ, N, F2, gF.TZ, gF.TS);
+    launch_y<false>(gF, 1, F2, F1);
+    k_x_fwd_op<R, KCX, XF_PSI_FULL, 1><<<gxF(), 256, sm_el, stream>>>(gF, tw, F1, F2, nfull,
+                                                                         KOp{1.0 / prm.dielectric, {0, 0, 0}});
+    k_hermitian_planes<R><<<592, 256, 0, stream>>>(gF, F2, 1);
+    k_x_inv_op<R, KCX, XI_IDENT, 1, 1><<<gxF(), 256, sm_el, stream>>>(gF, tw, F2, nfull, F1, KOp{});
+    launch_y<true>(gF, 1, F1, F2);
+    k_z_c2r<R><<<dim3(gz(), 1), 256, sm_el, stream>>>(gF, tw, F2, out, N, g.NZ, PPar{}, nullptr, 0, nullptr);
+  }
+
+  // The fields of Output_avs_charge (avs_output.cxx:451-549) at the current
+  // state, as NX*NY*NZ_ doubles: phi and the normalised surface charge
+  // density of Make_phi_qq_particle (operate_electrolyte.cxx:179-242), the
+  // real concentrations of both species (A_k2a of conc_k) and the Coulomb
+  // potential.  Scratch fields only: the state is not changed.
+  int el_snapshot_host(double *phi, double *surf, double *conc, double *pot) override {
+    if (prm.eq != KAPSEL_EQ_ELECTROLYTE || !conc_k) return KAPSEL_EINVAL;
+    const size_t N = npts();
+    launch_cells();
+    el_scatter(0);
+    el_surface_scale();
+    el_conc_real();
+    k_el_charge<R><<<592, 256, 0, stream>>>(N, phiq, creal, scal, 0, prm.valency_p, prm.valency_n, charge);
+    launch_el_potential(gradr);
+    KCHECK(cudaGetLastError());
+    std::vector<R> h(5 * N);  // phi, surface, c0, c1, potential
+    double s0 = 0.0;
+    KCHECK(cudaMemcpyAsync(h.data(), phiq, sizeof(R) * 2 * N, cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaMemcpyAsync(h.data() + 2 * N, creal, sizeof(R) * 2 * N, cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaMemcpyAsync(h.data() + 4 * N, gradr, sizeof(R) * N, cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaMemcpyAsync(&s0, scal, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    KCHECK(cudaStreamSynchronize(stream));
+    const int NZ_ = g.NZ + 2;
+    const size_t rows = (size_t)g.NX * g.NY, plane = rows * NZ_;
+    for (size_t r = 0; r < rows; ++r)
+      for (int k = 0; k < g.NZ; ++k) {
+        const size_t i = r * g.NZ + k, o = r * NZ_ + k;
+        phi[o] = (double)h[i];
+        surf[o] = (double)h[N + i] * s0;
+        conc[o] = (double)h[2 * N + i];
+        conc[plane + o] = (double)h[3 * N + i];
+        pot[o] = (double)h[4 * N + i];
+      }
+    return 0;
   }
 
   void launch_step_el(int euler) {
@@ -3563,8 +3618,10 @@ int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path) {
 
 // ---------------------------------------------------------------------------
 // AVS/Express field snapshots: Init_avs, Add_field_description and the
-// binary branch of Output_avs (avs_output.cxx:20-109, 162-342), Navier_Stokes
-// columns "ux uy uz phi pressure tau_xy tau_yz tau_zx tau_xx tau_yy".
+// binary branches of Output_avs (avs_output.cxx:20-109, 162-342; Navier_Stokes
+// columns "ux uy uz phi pressure tau_xy tau_yz tau_zx tau_xx tau_yy") and
+// Output_avs_charge (avs_output.cxx:451-549; Electrolyte columns "ux uy uz
+// phi surface_charge rho e_potential").
 namespace {
 
 void avs_binary_write(FILE *f, const double *a, int NX, int NY, int NZ) {
@@ -3586,13 +3643,17 @@ int kapsel_gpu_write_avs(kapsel_ctx *ctx, const char *out_dir, const char *out_n
   if (!ctx || !out_dir || !out_name || nstep < 1) return KAPSEL_EINVAL;
   BoxBase *b = ctx->box.get();
   if (!b->initialised) return KAPSEL_ESTATE;
-  if (b->prm.eq != KAPSEL_EQ_NAVIER_STOKES) return KAPSEL_EINVAL;
+  const bool el = b->prm.eq == KAPSEL_EQ_ELECTROLYTE;
+  if (b->prm.eq != KAPSEL_EQ_NAVIER_STOKES && !el) return KAPSEL_EINVAL;
   const int NX = b->g.NX, NY = b->g.NY, NZ = b->g.NZ, NZ_ = NZ + 2;
   const double DX = b->prm.dx, ETA = b->prm.eta;
   const size_t plane = (size_t)NX * NY * NZ_;
   const std::string dir(out_dir), name(out_name);
   const std::string fld = dir + "/" + name + ".fld", cod = name + ".cod";
-  const int veclen = 10;
+  // Veclen / Label, Veclen_charge / Label_charge (avs_output.cxx:14-19)
+  const int veclen = el ? 7 : 10;
+  const char *label = el ? "ux uy uz phi surface_charge rho e_potential"
+                         : "ux uy uz phi pressure tau_xy tau_yz tau_zx tau_xx tau_yy";
   if (init) {
     mkdir((dir + "/avs").c_str(), 0755);
     FILE *f = fopen(fld.c_str(), "w");
@@ -3600,7 +3661,7 @@ int kapsel_gpu_write_avs(kapsel_ctx *ctx, const char *out_dir, const char *out_n
     fprintf(f, "# AVS field file\nndim=%d\ndim1=%d\ndim2=%d\ndim3=%d\nnspace=%d\nveclen=%d\n", 3, NX, NY, NZ, 3,
             veclen);
     fprintf(f, "data=float\nfield=uniform\nnstep=%d\n", nstep);
-    fprintf(f, "label = %s\n", "ux uy uz phi pressure tau_xy tau_yz tau_zx tau_xx tau_yy");
+    fprintf(f, "label = %s\n", label);
     fclose(f);
     f = fopen((dir + "/" + cod).c_str(), "wb");
     if (!f) return KAPSEL_EINVAL;
@@ -3609,40 +3670,47 @@ int kapsel_gpu_write_avs(kapsel_ctx *ctx, const char *out_dir, const char *out_n
     fclose(f);
   }
   // fields in the Ooura real layout [NX][NY][NZ_]
-  std::vector<double> u(3 * plane), phi(plane), strain(5 * plane, 0.0);
+  std::vector<double> u(3 * plane), phi(plane), strain(el ? 0 : 5 * plane, 0.0);
+  std::vector<double> surf(el ? plane : 0), conc(el ? 2 * plane : 0), pot(el ? plane : 0);
   int rc = b->velocity_to_host(u.data());
   if (rc) return rc;
-  if ((rc = b->phi_only_host(phi.data()))) return rc;
-  // viscous strain tensor eta*(d_i u_j + d_j u_i)/2 of the velocity, by the
-  // spectral formula of Zeta_k2Strain_k (fft_wrapper.cxx:201-257)
-  std::vector<double> uk(u);
-  for (int c = 0; c < 3; ++c)
-    if ((rc = b->fft_fwd_host(uk.data() + c * plane))) return rc;
-  const double wx = 2.0 * M_PI / (NX * DX), wy = 2.0 * M_PI / (NY * DX), wz = 2.0 * M_PI / (NZ * DX);
-  for (int i = 0; i < NX; ++i)
-    for (int j = 0; j < NY; ++j)
-      for (int k = 0; k < NZ_ / 2; ++k) {
-        const size_t im0 = ((size_t)i * NY + j) * NZ_ + 2 * k, im1 = im0 + 1;
-        const double ks[3] = {(i > NX / 2 ? i - NX : i) * wx * .5, (j > NY / 2 ? j - NY : j) * wy * .5, k * wz * .5};
-        double ud[3][2];
-        for (int d = 0; d < 3; ++d) {
-          ud[d][0] = ETA * uk[d * plane + im0];
-          ud[d][1] = ETA * uk[d * plane + im1];
+  if (el) {
+    // Output_avs_charge (avs_output.cxx:451-549)
+    if ((rc = b->el_snapshot_host(phi.data(), surf.data(), conc.data(), pot.data()))) return rc;
+  } else {
+    if ((rc = b->phi_only_host(phi.data()))) return rc;
+    // viscous strain tensor eta*(d_i u_j + d_j u_i)/2 of the velocity, by the
+    // spectral formula of Zeta_k2Strain_k (fft_wrapper.cxx:201-257)
+    std::vector<double> uk(u);
+    for (int c = 0; c < 3; ++c)
+      if ((rc = b->fft_fwd_host(uk.data() + c * plane))) return rc;
+    const double wx = 2.0 * M_PI / (NX * DX), wy = 2.0 * M_PI / (NY * DX), wz = 2.0 * M_PI / (NZ * DX);
+    for (int i = 0; i < NX; ++i)
+      for (int j = 0; j < NY; ++j)
+        for (int k = 0; k < NZ_ / 2; ++k) {
+          const size_t im0 = ((size_t)i * NY + j) * NZ_ + 2 * k, im1 = im0 + 1;
+          const double ks[3] = {(i > NX / 2 ? i - NX : i) * wx * .5, (j > NY / 2 ? j - NY : j) * wy * .5,
+                                k * wz * .5};
+          double ud[3][2];
+          for (int d = 0; d < 3; ++d) {
+            ud[d][0] = ETA * uk[d * plane + im0];
+            ud[d][1] = ETA * uk[d * plane + im1];
+          }
+          double *s0 = strain.data();
+          s0[0 * plane + im0] = ks[0] * ud[0][1] * 2.;
+          s0[0 * plane + im1] = -ks[0] * ud[0][0] * 2.;
+          s0[1 * plane + im0] = ks[0] * ud[1][1] + ks[1] * ud[0][1];
+          s0[1 * plane + im1] = -ks[0] * ud[1][0] - ks[1] * ud[0][0];
+          s0[2 * plane + im0] = ks[0] * ud[2][1] + ks[2] * ud[0][1];
+          s0[2 * plane + im1] = -ks[0] * ud[2][0] - ks[2] * ud[0][0];
+          s0[3 * plane + im0] = ks[1] * ud[1][1] * 2.;
+          s0[3 * plane + im1] = -ks[1] * ud[1][0] * 2.;
+          s0[4 * plane + im0] = ks[1] * ud[2][1] + ks[2] * ud[1][1];
+          s0[4 * plane + im1] = -ks[1] * ud[2][0] - ks[2] * ud[1][0];
         }
-        double *s0 = strain.data();
-        s0[0 * plane + im0] = ks[0] * ud[0][1] * 2.;
-        s0[0 * plane + im1] = -ks[0] * ud[0][0] * 2.;
-        s0[1 * plane + im0] = ks[0] * ud[1][1] + ks[1] * ud[0][1];
-        s0[1 * plane + im1] = -ks[0] * ud[1][0] - ks[1] * ud[0][0];
-        s0[2 * plane + im0] = ks[0] * ud[2][1] + ks[2] * ud[0][1];
-        s0[2 * plane + im1] = -ks[0] * ud[2][0] - ks[2] * ud[0][0];
-        s0[3 * plane + im0] = ks[1] * ud[1][1] * 2.;
-        s0[3 * plane + im1] = -ks[1] * ud[1][0] * 2.;
-        s0[4 * plane + im0] = ks[1] * ud[2][1] + ks[2] * ud[1][1];
-        s0[4 * plane + im1] = -ks[1] * ud[2][0] - ks[2] * ud[1][0];
-      }
-  for (int c = 0; c < 5; ++c)
-    if ((rc = b->fft_inv_host(strain.data() + c * plane))) return rc;
+    for (int c = 0; c < 5; ++c)
+      if ((rc = b->fft_inv_host(strain.data() + c * plane))) return rc;
+  }
   // Add_field_description (BINARY, uniform field)
   const size_t data_size = sizeof(float) * (size_t)NX * NY * NZ;
   const std::string pfx = "avs/" + name + "_";
@@ -3660,13 +3728,36 @@ int kapsel_gpu_write_avs(kapsel_ctx *ctx, const char *out_dir, const char *out_n
   if (!f) return KAPSEL_EINVAL;
   for (int c = 0; c < 3; ++c) avs_binary_write(f, u.data() + c * plane, NX, NY, NZ);
   avs_binary_write(f, phi.data(), NX, NY, NZ);
-  {
+  if (el) {
+    // surface charge * 4 pi a^2, rho = (1 - phi) sum_n e z_n c_n summed in
+    // float as the reference does, then the potential (avs_output.cxx:490-513)
+    const double area = 4.0 * M_PI * (b->prm.a * DX) * (b->prm.a * DX);
+    const double val[2] = {b->prm.valency_p, b->prm.valency_n};
+    std::vector<float> row((size_t)NX);
+    for (int k = 0; k < NZ; ++k)
+      for (int j = 0; j < NY; ++j) {
+        for (int i = 0; i < NX; ++i) row[i] = (float)(surf[((size_t)i * NY + j) * NZ_ + k] * area);
+        fwrite(row.data(), sizeof(float), row.size(), f);
+      }
+    for (int k = 0; k < NZ; ++k)
+      for (int j = 0; j < NY; ++j) {
+        for (int i = 0; i < NX; ++i) {
+          const size_t im = ((size_t)i * NY + j) * NZ_ + k;
+          float q = 0.f;
+          for (int n = 0; n < 2; ++n) q += (float)(1.0 * val[n] * conc[n * plane + im]);  // Elementary_charge = 1
+          q = (float)((double)q * (1. - phi[im]));
+          row[i] = q;
+        }
+        fwrite(row.data(), sizeof(float), row.size(), f);
+      }
+    avs_binary_write(f, pot.data(), NX, NY, NZ);
+  } else {
     // the Navier_Stokes step computes no pressure field
     std::vector<double> zero(plane, 0.0);
     avs_binary_write(f, zero.data(), NX, NY, NZ);
+    const int order[5] = {1, 4, 2, 0, 3};  // xy, yz, zx, xx, yy
+    for (int c = 0; c < 5; ++c) avs_binary_write(f, strain.data() + order[c] * plane, NX, NY, NZ);
   }
-  const int order[5] = {1, 4, 2, 0, 3};  // xy, yz, zx, xx, yy
-  for (int c = 0; c < 5; ++c) avs_binary_write(f, strain.data() + order[c] * plane, NX, NY, NZ);
   const bool ok = !ferror(f);
   fclose(f);
   return ok ? 0 : KAPSEL_EINVAL;

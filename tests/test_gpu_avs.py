@@ -1,4 +1,5 @@
-"""AVS snapshots written from device state against Output_avs of the
+"""AVS snapshots written from device state against Output_avs (and
+Output_avs_charge in the Electrolyte branch) of the
 compiled reference (oracle/_ref) on the same state: identical .fld/.cod
 text, and the velocity and phi columns of the binary .dat equal to float32
 rounding.  The reference's pressure column is never assigned in the
@@ -63,3 +64,38 @@ def test_avs_snapshot_matches_reference(tmp_path):
     for c, key in zip(range(5, 10), ("xy", "yz", "zx", "xx", "yy")):
         scale = max(np.abs(tau[key]).max(), 1e-30)
         assert np.abs(B[c] - tau[key]).max() <= 1e-4 * scale, key
+
+
+def test_avs_electrolyte_snapshot_matches_reference(tmp_path):
+    """Output_avs_charge: the same .fld/.cod text and all seven columns (u,
+    phi, surface charge, ionic charge density, Coulomb potential) equal to
+    float32 rounding of the reference's snapshot of the same state."""
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+    import kapsel_old_b200 as kg
+
+    def cfg(d):
+        c = udf.electrolyte_config((5, 5, 5), 2, seed=6, efield=(0.05, 0.0, 0.0))
+        c["avs"] = {"dir": d, "name": "snap"}
+        return c
+
+    dr, dg = os.path.join(tmp_path, "ref"), os.path.join(tmp_path, "gpu")
+    os.makedirs(os.path.join(dr, "avs"))
+    os.makedirs(dg)
+    r = ref.RefSim(cfg(dr))
+    r.step(3)
+    r.output_avs(init=True)
+    g = kg.Simulation(cfg(dg), precision=kg.FP64)
+    g.step(3)
+    z_before = g.zeta()
+    g.write_avs(dg, "snap", nstep=2, init=True)
+    assert np.array_equal(g.zeta(), z_before)  # the snapshot leaves the state alone
+    for f in ("snap.fld", "snap.cod"):
+        assert open(os.path.join(dr, f)).read() == open(os.path.join(dg, f)).read(), f
+    A = np.fromfile(os.path.join(dr, "avs", "snap_3.dat"), dtype=np.float32).reshape(7, 32, 32, 32)
+    B = np.fromfile(os.path.join(dg, "avs", "snap_3.dat"), dtype=np.float32).reshape(7, 32, 32, 32)
+    for c in range(7):
+        scale = max(np.abs(A[c]).max(), 1e-30)
+        assert np.abs(A[c] - B[c]).max() <= 4e-7 * scale, (c, np.abs(A[c] - B[c]).max() / scale)
+    # every column carries signal: velocity, phi, surface charge, charge, potential
+    assert all(np.abs(A[c]).max() > 0 for c in range(7))
