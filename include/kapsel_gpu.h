@@ -170,7 +170,11 @@ int kapsel_gpu_load_restart(kapsel_ctx *ctx, const char *path);
    4 pi a^2) of Make_phi_qq_particle, the ionic charge density (1 - phi)
    sum_n z_n c_n, and the Coulomb potential of the total charge over the
    full spectrum.  Unlike the reference, which transforms its concentrations
-   to real space and back in place, the state is not changed. */
+   to real space and back in place, the state is not changed.  With
+   particles, every call also writes the particle snapshot of Output_avs_p
+   (avs_output_p.cxx:13-142), as the main loop does beside it:
+   <out_dir>/<out_name>p.fld (header with init) and avs/<out_name>p_<ts>.cod
+   / .dat (float32 positions; radius and body axes). */
 int kapsel_gpu_write_avs(kapsel_ctx *ctx, const char *out_dir, const char *out_name, int nstep, int init);
 
 /* Time step counter jikan.ts and time jikan.time. */

@@ -3635,6 +3635,71 @@ void avs_binary_write(FILE *f, const double *a, int NX, int NY, int NZ) {
     }
 }
 
+// Output_avs_p (avs_output_p.cxx:13-142, BINARY): per snapshot the particle
+// positions (<pfx><ts>.cod: z, y, x blocks) and the radius and body axes
+// (<pfx><ts>.dat: radius block, then the columns of the rotation matrix of
+// each orientation quaternion) as float32, and their description in the
+// particle .fld file.  The rotation matrix of a unit quaternion (s, v) is
+// (s^2 - v.v) I + 2 v v^T + 2 s [v]x, the matrix rqtn_rm builds
+// (quaternion.h:432-449).
+int avs_write_particles(const std::string &dir, const std::string &name, const double *rec, int np, double radius,
+                        int ts, double time, int nstep, bool init) {
+  const std::string pfld = dir + "/" + name + "p.fld", ppfx = "avs/" + name + "p_";
+  const int veclen = 10;
+  if (init) {
+    FILE *f = fopen(pfld.c_str(), "w");
+    if (!f) return KAPSEL_EINVAL;
+    fprintf(f, "# AVS field file\nndim=%d\ndim1=%d\nnspace=%d\nveclen=%d\ndata=float\nfield=irregular\n", 1, np, 3,
+            veclen);
+    fprintf(f, "nstep=%d\nlabel = %s\n", nstep, "Radius x1 x2 x3 y1 y2 y3 z1 z2 z3");
+    fclose(f);
+  }
+  FILE *f = fopen(pfld.c_str(), "a");
+  if (!f) return KAPSEL_EINVAL;
+  const int data_size = (int)sizeof(float) * np;
+  fprintf(f, "time value = \"step%dtime%g\"\n", ts, time);
+  for (int n = 0; n < 3; ++n)
+    fprintf(f, "coord %d file = %s%d.cod filetype = binary skip = %d\n", 3 - n, ppfx.c_str(), ts, n * data_size);
+  for (int n = 0; n < veclen; ++n)
+    fprintf(f, "variable %d file = %s%d.dat filetype = binary skip = %d\n", n + 1, ppfx.c_str(), ts, n * data_size);
+  fprintf(f, "EOT\n");
+  fclose(f);
+  std::vector<float> col((size_t)np);
+  f = fopen((dir + "/" + ppfx + std::to_string(ts) + ".cod").c_str(), "wb");
+  if (!f) return KAPSEL_EINVAL;
+  for (int d = 0; d < 3; ++d) {
+    for (int n = 0; n < np; ++n) col[n] = (float)rec[(size_t)KAPSEL_P_STRIDE * n + KAPSEL_P_X + 2 - d];
+    fwrite(col.data(), sizeof(float), col.size(), f);
+  }
+  bool ok = !ferror(f);
+  fclose(f);
+  f = fopen((dir + "/" + ppfx + std::to_string(ts) + ".dat").c_str(), "wb");
+  if (!f) return KAPSEL_EINVAL;
+  for (int n = 0; n < np; ++n) col[n] = (float)radius;
+  fwrite(col.data(), sizeof(float), col.size(), f);
+  // R[a][b] for each particle, written column by column (b outer, a inner)
+  for (int b = 0; b < 3; ++b)
+    for (int a = 0; a < 3; ++a) {
+      for (int n = 0; n < np; ++n) {
+        const double *q = rec + (size_t)KAPSEL_P_STRIDE * n + KAPSEL_P_Q;  // s, v0, v1, v2
+        const double qs = q[0], v[3] = {q[1], q[2], q[3]};
+        double r = 2.0 * v[a] * v[b];
+        if (a == b) r += qs * qs - (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        // 2 s [v]x: [v]x[a][b] = -eps_abc v_c
+        if (a != b) {
+          const int c = 3 - a - b;
+          const double sgn = ((b - a + 3) % 3 == 1) ? -1.0 : 1.0;
+          r += 2.0 * qs * sgn * v[c];
+        }
+        col[n] = (float)r;
+      }
+      fwrite(col.data(), sizeof(float), col.size(), f);
+    }
+  ok = ok && !ferror(f);
+  fclose(f);
+  return ok ? 0 : KAPSEL_EINVAL;
+}
+
 }  // namespace
 
 extern "C" {
@@ -3760,7 +3825,12 @@ int kapsel_gpu_write_avs(kapsel_ctx *ctx, const char *out_dir, const char *out_n
   }
   const bool ok = !ferror(f);
   fclose(f);
-  return ok ? 0 : KAPSEL_EINVAL;
+  if (!ok) return KAPSEL_EINVAL;
+  if (b->Np == 0) return 0;
+  // the particle snapshot the main loop writes beside it (sp_3d_ns.cxx:557-559)
+  std::vector<double> rec((size_t)KAPSEL_P_STRIDE * b->Np);
+  if ((rc = kapsel_gpu_get_particles(ctx, rec.data()))) return rc;
+  return avs_write_particles(dir, name, rec.data(), b->Np, b->prm.a * DX, b->ts, b->time, nstep, init != 0);
 }
 
 }  // extern "C"

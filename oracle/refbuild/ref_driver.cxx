@@ -261,14 +261,19 @@ int kref_resume(const char *path) {
   return 0;
 }
 
-/* Output_avs (Output_avs_charge in the Electrolyte branch) of the current
-   state as the step loop calls it (sp_3d_ns.cxx:553-566, BINARY); init
-   writes the .fld header and .cod file first (Init_avs).  Needs output.AVS =
-   ON in the input. */
+/* Output_avs_p and Output_avs (Output_avs_charge in the Electrolyte branch)
+   of the current state as the step loop calls them (sp_3d_ns.cxx:553-566,
+   BINARY); init writes the .fld headers and the .cod file first (Init_avs,
+   Init_avs_p).  Needs output.AVS = ON in the input. */
 int kref_output_avs(int init) {
   if (!g_ready || !SW_AVS || (SW_EQ != Navier_Stokes && SW_EQ != Electrolyte)) return -1;
   Set_avs_parameters(Avs_parameters);
-  if (init) Init_avs(Avs_parameters);
+  if (init) {
+    Init_avs(Avs_parameters);
+    if (Particle_Number > 0) Init_avs_p(Avs_parameters);
+  }
+  // as the main loop writes them (sp_3d_ns.cxx:555-566)
+  if (Particle_Number > 0) Output_avs_p(Avs_parameters, g_particles, g_jikan);
   if (SW_EQ == Electrolyte)
     Output_avs_charge(Avs_parameters, g_zeta, g_uk_dc, Concentration, g_particles, g_jikan);
   else

@@ -1,8 +1,8 @@
 """AVS snapshots written from device state against Output_avs (and
-Output_avs_charge in the Electrolyte branch) of the
-compiled reference (oracle/_ref) on the same state: identical .fld/.cod
-text, and the velocity and phi columns of the binary .dat equal to float32
-rounding.  The reference's pressure column is never assigned in the
+Output_avs_charge in the Electrolyte branch, Output_avs_p for the particles)
+of the compiled reference (oracle/_ref) on the same state: identical
+.fld/.cod text, and the velocity and phi columns of the binary .dat (and the
+particle positions and body axes) equal to float32 rounding.  The reference's pressure column is never assigned in the
 Navier_Stokes branch (uninitialised memory) and its tau columns read its
 vorticity buffer in place of the velocity, so those columns are checked
 against the viscous strain rate of the velocity computed here with numpy."""
@@ -21,6 +21,17 @@ def _cfg(d):
     cfg["avs"] = {"dir": d, "name": "snap"}
     cfg["eta"] = 1.3
     return cfg
+
+
+def _check_particle_files(dr, dg, ts, np_):
+    """Output_avs_p: the particle .fld text and the float32 positions, radius
+    and body-axis columns (rotation matrix of each quaternion)."""
+    assert open(os.path.join(dr, "snapp.fld")).read() == open(os.path.join(dg, "snapp.fld")).read()
+    for ext, rows in ((".cod", 3), (".dat", 10)):
+        A = np.fromfile(os.path.join(dr, "avs", f"snapp_{ts}{ext}"), dtype=np.float32)
+        B = np.fromfile(os.path.join(dg, "avs", f"snapp_{ts}{ext}"), dtype=np.float32)
+        assert A.shape == B.shape == (rows * np_,), ext
+        assert np.abs(A - B).max() <= 4e-7 * max(np.abs(A).max(), 1.0), ext
 
 
 def _read(path, n=32):
@@ -44,6 +55,7 @@ def test_avs_snapshot_matches_reference(tmp_path):
     g.write_avs(dg, "snap", nstep=2, init=True)
     for f in ("snap.fld", "snap.cod"):
         assert open(os.path.join(dr, f)).read() == open(os.path.join(dg, f)).read(), f
+    _check_particle_files(dr, dg, 4, 3)
     A = _read(os.path.join(dr, "avs", "snap_4.dat"))
     B = _read(os.path.join(dg, "avs", "snap_4.dat"))
     for c in range(4):
@@ -92,6 +104,7 @@ def test_avs_electrolyte_snapshot_matches_reference(tmp_path):
     assert np.array_equal(g.zeta(), z_before)  # the snapshot leaves the state alone
     for f in ("snap.fld", "snap.cod"):
         assert open(os.path.join(dr, f)).read() == open(os.path.join(dg, f)).read(), f
+    _check_particle_files(dr, dg, 3, 2)
     A = np.fromfile(os.path.join(dr, "avs", "snap_3.dat"), dtype=np.float32).reshape(7, 32, 32, 32)
     B = np.fromfile(os.path.join(dg, "avs", "snap_3.dat"), dtype=np.float32).reshape(7, 32, 32, 32)
     for c in range(7):
