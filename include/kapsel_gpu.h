@@ -17,6 +17,15 @@
  * Every entry point returns 0 on success or a negative KAPSEL_E* status; the
  * library never exits the process (the reference calls exit_job, macro.h:194).
  * One context owns one CUDA stream; contexts are independent.
+ *
+ * Failure detection: parameters and particle records are checked on the
+ * host (a NaN or Inf, a position outside the box: KAPSEL_EINVAL /
+ * KAPSEL_ERANGE, nothing is sent to the device).  During a step the device
+ * flags a non-finite particle velocity (KAPSEL_ENONFINITE), a particle
+ * outside the box or a full neighbour list (KAPSEL_ERANGE) and a bounded
+ * wait that ran out (KAPSEL_ETIMEOUT); the step's status returns it, and it
+ * stays until the state is replaced (kapsel_gpu_set_zeta,
+ * kapsel_gpu_set_particles / _set_particle_state, kapsel_gpu_load_restart).
  */
 #ifndef KAPSEL_GPU_H
 #define KAPSEL_GPU_H
@@ -416,6 +425,14 @@ int kapsel_gpu_get_stream(kapsel_ctx *ctx, void **stream);
    stream; ms[i] receives the duration of launch i (KAPSEL_N_STEP_KERNELS
    floats).  Advances the state exactly like kapsel_gpu_step(ctx, 1). */
 int kapsel_gpu_profile_step(kapsel_ctx *ctx, float *ms);
+
+/* Checks, on the current device, that the library's bounded device waits end
+   instead of hanging: a one-block kernel waits on a barrier that nothing
+   arrives at, gives up after 0.5 s as the network kernels' waits do, and
+   records the timeout.  Returns KAPSEL_ETIMEOUT when that worked (the device
+   stays usable), KAPSEL_ECUDA or KAPSEL_ENOMEM otherwise.  No counterpart in
+   the reference (it has no device waits). */
+int kapsel_gpu_check_bounded_wait(void);
 
 /* Human-readable text of a status code. */
 const char *kapsel_gpu_strerror(int status);

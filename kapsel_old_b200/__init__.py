@@ -31,7 +31,9 @@ P_STRIDE = 35
 
 
 class KapselError(RuntimeError):
-    pass
+    """A non-zero KAPSEL_E* status; `code` holds it."""
+
+    code = 0
 
 
 class _Params(ctypes.Structure):
@@ -108,6 +110,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_set_oblique": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double]),
         "kapsel_gpu_get_concentration": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_set_concentration": (ctypes.c_int, [_VP, _DP, _DP]),
+        "kapsel_gpu_check_bounded_wait": (ctypes.c_int, []),
         "kapsel_gpu_A2a_k": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_A_k2a": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_solenoidal_u": (ctypes.c_int, [_VP, _DP, _DP, _DP]),
@@ -283,7 +286,9 @@ class Simulation:
     def _check(self, rc: int):
         if rc != 0:
             msg = load_library().kapsel_gpu_strerror(rc).decode()
-            raise KapselError(f"kapsel_gpu status {rc}: {msg}")
+            err = KapselError(f"kapsel_gpu status {rc}: {msg}")
+            err.code = rc
+            raise err
 
     def close(self):
         if getattr(self, "h", None):

@@ -2004,7 +2004,14 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
                                          !(p->valency_p > 0.0) || !(p->valency_n < 0.0)))
     return KAPSEL_EINVAL;
   if (p->precision != KAPSEL_FP64 && p->precision != KAPSEL_MIXED) return KAPSEL_EINVAL;
-  if (p->n_particles < 0 || p->dx <= 0 || p->rho <= 0 || p->eta <= 0 || p->dt <= 0 || p->a <= 0 || p->a_xi <= 0)
+  // written so that a NaN fails every test
+  if (p->n_particles < 0 || !(p->dx > 0) || !(p->rho > 0) || !(p->eta > 0) || !(p->dt > 0) || !(p->a > 0) ||
+      !(p->a_xi > 0))
+    return KAPSEL_EINVAL;
+  if (!(p->kbt >= 0) || !(p->mass_ratio > 0) || !std::isfinite(p->kbt) || !std::isfinite(p->mass_ratio) ||
+      !std::isfinite(p->gravity_g) || !std::isfinite(p->epsilon) || !std::isfinite(p->alpha_v) ||
+      !std::isfinite(p->alpha_o) || !std::isfinite(p->e_ext[0]) || !std::isfinite(p->e_ext[1]) ||
+      !std::isfinite(p->e_ext[2]))
     return KAPSEL_EINVAL;
   if (p->lj_powers < 0 || p->lj_powers > 2 || p->gravity_dir < 0 || p->gravity_dir > 2) return KAPSEL_EINVAL;
   std::unique_ptr<BoxBase> b;
@@ -2218,6 +2225,7 @@ int kapsel_gpu_set_particles(kapsel_ctx *ctx, const double *x, const double *q) 
   }
   if (cudaMemcpyAsync(b->parts, h.data(), sizeof(DPart) * h.size(), cudaMemcpyHostToDevice, b->stream) !=
           cudaSuccess ||
+      cudaMemsetAsync(b->status, 0, sizeof(int), b->stream) != cudaSuccess ||
       cudaStreamSynchronize(b->stream) != cudaSuccess)
     return KAPSEL_ECUDA;
   b->particles_set = true;
@@ -2348,6 +2356,7 @@ int kapsel_gpu_set_zeta(kapsel_ctx *ctx, const double *zeta, const double *uk_dc
   int rc = b->zeta_from_host(zeta);
   if (rc) return rc;
   if (cudaMemcpyAsync(b->uk_dc, uk_dc, sizeof(double) * 3, cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+      cudaMemsetAsync(b->status, 0, sizeof(int), b->stream) != cudaSuccess ||
       cudaStreamSynchronize(b->stream) != cudaSuccess)
     return KAPSEL_ECUDA;
   b->initialised = true;
@@ -2393,6 +2402,8 @@ int kapsel_gpu_set_particle_state(kapsel_ctx *ctx, const double *in) {
   memset(h.data(), 0, sizeof(DPart) * h.size());
   for (int n = 0; n < b->Np; ++n) {
     const double *o = in + (size_t)KAPSEL_P_STRIDE * n;
+    for (int i = 0; i < KAPSEL_P_STRIDE; ++i)
+      if (!std::isfinite(o[i])) return KAPSEL_EINVAL;  // never send a NaN/Inf to the device
     DPart &a = h[n];
     for (int d = 0; d < 3; ++d) {
       a.x[d] = o[KAPSEL_P_X + d];
@@ -2413,6 +2424,7 @@ int kapsel_gpu_set_particle_state(kapsel_ctx *ctx, const double *in) {
   }
   if (cudaMemcpyAsync(b->parts, h.data(), sizeof(DPart) * h.size(), cudaMemcpyHostToDevice, b->stream) !=
           cudaSuccess ||
+      cudaMemsetAsync(b->status, 0, sizeof(int), b->stream) != cudaSuccess ||
       cudaStreamSynchronize(b->stream) != cudaSuccess)
     return KAPSEL_ECUDA;
   b->particles_set = true;
@@ -2457,6 +2469,21 @@ int kapsel_gpu_get_concentration(kapsel_ctx *ctx, double *c) {
   if (!ctx || !c) return KAPSEL_EINVAL;
   if (ctx->box->prm.eq != KAPSEL_EQ_ELECTROLYTE) return KAPSEL_ESTATE;
   return ctx->box->conc_to_host(c);
+}
+
+int kapsel_gpu_check_bounded_wait(void) {
+  int *st = nullptr, h = 0;
+  if (cudaMalloc(&st, sizeof(int)) != cudaSuccess) return KAPSEL_ENOMEM;
+  int rc = 0;
+  if (cudaMemset(st, 0, sizeof(int)) != cudaSuccess) rc = KAPSEL_ECUDA;
+  if (!rc) {
+    nc::k_wait_selfcheck<<<1, 32>>>(st);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(&h, st, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = KAPSEL_ECUDA;
+  }
+  cudaFree(st);
+  return rc ? rc : h;
 }
 
 int kapsel_gpu_set_concentration(kapsel_ctx *ctx, const double *c, const double *total_solute) {

@@ -111,6 +111,20 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   }
 }
 
+// Self-check of the bounded wait: one thread waits on an mbarrier that
+// nothing arrives at; when the wait gives up (0.5 s) it records
+// NC_ETIMEOUT, as the network kernels do, and the kernel returns.
+__global__ void k_wait_selfcheck(int *status) {
+  __shared__ __align__(8) unsigned long long bar;
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(&bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(a, 0)) atomicExch(status, NC_ETIMEOUT);
+}
+
 // 16 consecutive FP32 columns of this thread's lane.
 __device__ __forceinline__ void tmem_ld16(uint32_t addr, float *v) {
   uint32_t r[16];

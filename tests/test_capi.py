@@ -89,3 +89,11 @@ def test_invalid_arguments_rejected_without_gpu(lib):
     p.np_xyz[0] = 3  # grids are 16..512 per axis
     h = ctypes.c_void_p()
     assert L.kapsel_gpu_create(ctypes.byref(p), ctypes.byref(h)) == -1
+    # NaN, Inf and out-of-range physical parameters are refused before any
+    # device call (the reference would run on and produce NaN fields)
+    for name, value in (("dt", float("nan")), ("dx", float("nan")), ("eta", -1.0), ("kbt", float("nan")),
+                        ("kbt", -1e-3), ("mass_ratio", 0.0), ("gravity_g", float("inf")), ("a", float("nan"))):
+        q = kg._Params()
+        L.kapsel_params_default(ctypes.byref(q))
+        setattr(q, name, value)
+        assert L.kapsel_gpu_create(ctypes.byref(q), ctypes.byref(h)) == -1, name
