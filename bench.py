@@ -433,6 +433,8 @@ def run_ours(args, rank, world, local_rank):
                  "mixed_over_fp64": round(value / fp64_value, 3)},
         "fp64_value": round(fp64_value, 3),
         "mixed_over_fp64": round(value / fp64_value, 3),
+        # the same throughput in grid points advanced per second (all ranks)
+        "grid_point_steps_per_s": round(value * (1 << sum(cfg["np_xyz"])), 1),
         "parity": parity,
         "roofline": {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 4),
