@@ -141,7 +141,59 @@ def replica_value(units_per_rank: int, world: int, max_seconds: float) -> float:
     return units_per_rank * world / max_seconds
 
 
+class NvmlClockSampler:
+    """SM clock and clock-event reasons read through NVML every 5 ms on a host
+    thread while the timed steps run (read-only queries; the timed region of
+    the headline is well under a second, shorter than nvidia-smi's sampling
+    interval)."""
+
+    early = False  # started right before the timed steps
+
+    def __init__(self, index: int):
+        import pynvml
+
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        self.sm, self.bits, self.stop_ev, self.t = [], 0, None, None
+
+    def start(self):
+        import threading
+
+        self.stop_ev = threading.Event()
+
+        def run():
+            nv = self.nv
+            while not self.stop_ev.is_set():
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                self.bits |= int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.stop_ev.wait(0.005)
+
+        self.t = threading.Thread(target=run, daemon=True)
+        self.t.start()
+
+    def stop(self):
+        self.stop_ev.set()
+        self.t.join()
+        nv = self.nv
+        names = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                 "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                 "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                 "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        reasons = sorted(k for k, b in names.items() if self.bits & b)
+        try:
+            nv.nvmlShutdown()
+        except Exception:
+            pass
+        if not self.sm:
+            return None
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.sm), "source": "nvml"}
+
+
 class ClockSampler:
+    early = True  # started before the warm-up
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -210,7 +262,7 @@ def run_ours(args, rank, world, local_rank):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     L = kg.load_library()
 
-    def timed(precision, steps, warmup, cfg=cfg, setup=None):
+    def timed(precision, steps, warmup, cfg=cfg, setup=None, sampler=None):
         sim = kg.Simulation(cfg, precision=precision)
         if setup is not None:
             setup(sim)
@@ -223,6 +275,8 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        if sampler is not None and not sampler.early:
+            sampler.start()
         for k in range(steps):
             with torch.cuda.stream(stream):
                 flush.fill_(float(k))
@@ -230,14 +284,20 @@ def run_ours(args, rank, world, local_rank):
             sim._check(L.kapsel_gpu_step_graph(sim.h, 1))
             evs[k][1].record(stream)
         torch.cuda.synchronize()
+        if sampler is not None:
+            sampler.result = sampler.stop()
         ms = reduce_max(sum(a.elapsed_time(b) for a, b in evs), dist)
         return sim, stream, ms
 
-    # ---- mixed precision (headline) with clocks sampled during the timed region
-    clk = ClockSampler(local_rank)
-    clk.start()
-    sim_m, stream_m, ms_m = timed(kg.MIXED, args.steps, args.warmup)
-    clocks = clk.stop()
+    # ---- mixed precision (headline) with clocks sampled during the timed
+    # region (NVML, else nvidia-smi)
+    try:
+        clk = NvmlClockSampler(local_rank)
+    except Exception:
+        clk = ClockSampler(local_rank)
+        clk.start()  # nvidia-smi starts slowly: it samples from the warm-up on
+    sim_m, stream_m, ms_m = timed(kg.MIXED, args.steps, args.warmup, sampler=clk)
+    clocks = clk.result
     # ---- FP64 path, same workload
     sim_d, _, ms_d = timed(kg.FP64, args.steps, args.warmup)
     sim_d.close()
