@@ -405,7 +405,7 @@ def run_ours(args, rank, world, local_rank):
             "boxes": len(boxes), "particles": sum(len(c["particles"]) for c in boxes),
             "msd_mean": float(np.mean(msd)),
             "autotune": [{"shape": list(v[:3]), "z_pass": ["warp", "block"][v[3]],
-                          "y_pass": Y_VARIANTS[v[4]]} for v in chosen],
+                          "y_pass": Y_VARIANTS[v[4]], "x_split": ["default", "other"][v[5]]} for v in chosen],
             "workload": "48 boxes from {32^3, 64^3, 64x64x128, 128^3}, 1-64 spheres a in [4,6], kBT=1e-3, mixed"}
         # learned near-contact correction: trained on the GPU from the committed
         # pair set (method runs at a=5 and a=10), then the 256^3 / 2048-sphere

@@ -67,7 +67,7 @@ extern "C" {
 /* Physical and numerical parameters: the values Gourmet_file_io reads from
    the UDF (input.cxx:438-1818) for one spherical-particle species. */
 typedef struct kapsel_params {
-  int np_xyz[3];       /* grid N = 1 << np per axis (input.cxx:1392-1397) */
+  int np_xyz[3];       /* grid N = 1 << np per axis, np 4..8 (input.cxx:1392-1397) */
   int eq;              /* KAPSEL_EQ_* */
   int precision;       /* KAPSEL_FP64 or KAPSEL_MIXED */
   int n_particles;     /* Particle_Number (one species) */
@@ -231,14 +231,22 @@ int kapsel_batch_step(kapsel_batch *b, int nsteps);
    kapsel_batch_create (the R_raw records of Output_udf, avs_output.cxx:361-363). */
 int kapsel_batch_msd(kapsel_batch *b, double *msd);
 int kapsel_batch_get_stream(kapsel_batch *b, void **stream);
-/* The autotuner's choice per box shape, 5 ints each (up to cap shapes):
+/* The autotuner's choice per box shape, 6 ints each (up to cap shapes):
    NX, NY, NZ, the z-pass variant (0 warp-level line groups, 1 block-level
    row tiles) and the y-pass variant (0 warp-level, 1 block-level wide kz
    tile, 2 block-level narrow kz tile, 3 warp-level with the inverse y + z
    c2r and the force's z + y passes fused over (component, x) planes held in
-   shared memory; 3 needs z variant 0, NY = 32..128 and particles); returns
-   the number of shapes. */
+   shared memory; 3 needs z variant 0, NY = 32..128 and particles) and the
+   radix split of the x transforms (kapsel_gpu_set_x_split); returns the
+   number of shapes. */
 int kapsel_batch_variants(kapsel_batch *b, int *out, int cap);
+/* Radix split of the block-level x transforms of one context: 0 the default
+   factorisation of NX into two radix-2 networks, 1 the other one (32 = 4 x 8
+   instead of 8 x 4, 64 = 16 x 4 instead of 8 x 8, 128 = 16 x 8 instead of
+   8 x 16; NX = 256 has only the default).  Same results to roundoff; the
+   batch autotuner times both per box shape.  KAPSEL_EINVAL where NX has no
+   other split. */
+int kapsel_gpu_set_x_split(kapsel_ctx *ctx, int split);
 /* Sets the pass variants (as above) of one Navier_Stokes context; results
    are the same to roundoff, speed differs by shape.  KAPSEL_EINVAL for a
    variant the shape does not allow. */

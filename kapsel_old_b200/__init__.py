@@ -111,6 +111,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "kapsel_gpu_get_concentration": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_set_concentration": (ctypes.c_int, [_VP, _DP, _DP]),
         "kapsel_gpu_check_bounded_wait": (ctypes.c_int, []),
+        "kapsel_gpu_set_x_split": (ctypes.c_int, [_VP, ctypes.c_int]),
         "kapsel_gpu_A2a_k": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_A_k2a": (ctypes.c_int, [_VP, _DP]),
         "kapsel_gpu_solenoidal_u": (ctypes.c_int, [_VP, _DP, _DP, _DP]),
@@ -496,13 +497,14 @@ class Batch:
 
     def variants(self) -> list:
         """The autotuner's choice per box shape: (NX, NY, NZ, z variant,
-        y variant); z 0 warp-level / 1 block-level, y 0 warp-level /
+        y variant, x split); z 0 warp-level / 1 block-level, y 0 warp-level /
         1 block-level wide tile / 2 block-level narrow tile / 3 warp-level
-        with the fused y/z plane kernels."""
+        with the fused y/z plane kernels, x split 0 default / 1 the other
+        radix factorisation of NX."""
         self.L.kapsel_batch_variants.argtypes = [_VP, _IP, ctypes.c_int]
-        buf = (ctypes.c_int * (5 * 64))()
+        buf = (ctypes.c_int * (6 * 64))()
         n = self.L.kapsel_batch_variants(self.h, buf, 64)
-        return [tuple(buf[5 * i: 5 * i + 5]) for i in range(max(n, 0))]
+        return [tuple(buf[6 * i: 6 * i + 6]) for i in range(max(n, 0))]
 
     def close(self):
         if getattr(self, "h", None):

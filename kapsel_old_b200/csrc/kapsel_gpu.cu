@@ -289,6 +289,11 @@ struct BoxBase {
   virtual float time_variant(int zmode, int ymode, int reps) = 0;
   virtual void set_variant(int zmode, int ymode) = 0;
   virtual bool variant_ok(int zmode, int ymode) const = 0;
+  // radix split of the block-level x transforms: 0 the default, 1 the other
+  // factorisation of NX (fft2_n1_sel); time_variant times the current one
+  int xsplit = 0;
+  virtual bool xsplit_ok(int xs) const = 0;
+  virtual void set_xsplit(int xs) = 0;
   // the step runs the fused y/z plane kernels (k_yzw_c2r, k_zyw_force)
   virtual bool fused_yz() const { return false; }
   virtual int alloc_el() = 0;
@@ -399,26 +404,45 @@ struct Box : BoxBase {
   size_t npts() const { return (size_t)g.NX * g.NY * g.NZ; }
 
   // x passes with compile-time NX for NX = 32..256 (the runtime-NX kernels otherwise)
-  template <int LX>
-  int x_setup() {
-    KCHECK(allow_smem(k_x_zeta_to_u<R, KCX, LX>, smem_xu));
-    KCHECK(allow_smem(k_x_advect_update<R, KCX, 0, LX>, smem_xadv));
-    KCHECK(allow_smem(k_x_advect_update<R, KCX, 1, LX>, smem_xadv));
-    KCHECK(allow_smem(k_x_force_to_zeta<R, KCX, LX>, smem_xf));
-    KCHECK(allow_smem(k_x_force_to_zeta<R, KCX, LX, 1>, smem_xf));
+  template <int LX, int XS>
+  int x_setup_s() {
+    KCHECK(allow_smem(k_x_zeta_to_u<R, KCX, LX, XS>, smem_xu));
+    KCHECK(allow_smem(k_x_advect_update<R, KCX, 0, LX, XS>, smem_xadv));
+    KCHECK(allow_smem(k_x_advect_update<R, KCX, 1, LX, XS>, smem_xadv));
+    KCHECK(allow_smem(k_x_force_to_zeta<R, KCX, LX, 0, XS>, smem_xf));
+    KCHECK(allow_smem(k_x_force_to_zeta<R, KCX, LX, 1, XS>, smem_xf));
     return 0;
   }
   template <int LX>
+  int x_setup() {
+    const int rc = x_setup_s<LX, 0>();
+    return rc ? rc : x_setup_s<LX, 1>();
+  }
+  // the x-pass launches, with the radix split of this context (xsplit)
+  template <int LX>
   void xz_l(bool pdl, const Cx<R> *z, const double *u, Cx<R> *out) {
-    launch_k(pdl, k_x_zeta_to_u<R, KCX, LX>, gx(), dim3(kXZThreads), smem_xu, stream, g, tw, z, u, out);
+    if (xsplit)
+      launch_k(pdl, k_x_zeta_to_u<R, KCX, LX, 1>, gx(), dim3(kXZThreads), smem_xu, stream, g, tw, z, u, out);
+    else
+      launch_k(pdl, k_x_zeta_to_u<R, KCX, LX, 0>, gx(), dim3(kXZThreads), smem_xu, stream, g, tw, z, u, out);
   }
   template <int EU, int LX>
   void xa_l(bool pdl) {
-    launch_k(pdl, k_x_advect_update<R, KCX, EU, LX>, gx(), dim3(kXAdvThreads), smem_xadv, stream, g, tw, bufA, zeta, uk_dc);
+    if (xsplit)
+      launch_k(pdl, k_x_advect_update<R, KCX, EU, LX, 1>, gx(), dim3(kXAdvThreads), smem_xadv, stream, g, tw, bufA,
+               zeta, uk_dc);
+    else
+      launch_k(pdl, k_x_advect_update<R, KCX, EU, LX, 0>, gx(), dim3(kXAdvThreads), smem_xadv, stream, g, tw, bufA,
+               zeta, uk_dc);
   }
   template <int LX, int NEXTU = 0>
   void xf_l(bool pdl, Cx<R> *in) {
-    launch_k(pdl, k_x_force_to_zeta<R, KCX, LX, NEXTU>, gx(), dim3(kXForceThreads), smem_xf, stream, g, tw, in, zeta, uk_dc);
+    if (xsplit)
+      launch_k(pdl, k_x_force_to_zeta<R, KCX, LX, NEXTU, 1>, gx(), dim3(kXForceThreads), smem_xf, stream, g, tw, in,
+               zeta, uk_dc);
+    else
+      launch_k(pdl, k_x_force_to_zeta<R, KCX, LX, NEXTU, 0>, gx(), dim3(kXForceThreads), smem_xf, stream, g, tw, in,
+               zeta, uk_dc);
   }
   void x_zeta(bool pdl, const Cx<R> *z, const double *u, Cx<R> *out) {
     switch (g.NX) {
@@ -662,10 +686,10 @@ struct Box : BoxBase {
       // leave one block per SM and run slower than the separate passes
       if (sizeof(R) == 4 && zw && yz_ly && 3 * yz_sm <= 227 * 1024) ymode = 3;
     }
-    KCHECK(allow_smem(k_x_zeta_to_u<R, KCX>, smem_xu));
-    KCHECK(allow_smem(k_x_advect_update<R, KCX>, smem_xadv));
-    KCHECK(allow_smem(k_x_force_to_zeta<R, KCX>, smem_xf));
-    KCHECK(allow_smem(k_x_force_to_zeta<R, KCX, 0, 1>, smem_xf));
+    {
+      const int rc = x_setup<0>();
+      if (rc) return rc;
+    }
     KCHECK(allow_smem(k_y_pass<R, true, KCY>, smem_y));
     KCHECK(allow_smem(k_y_pass<R, false, KCY>, smem_y));
     KCHECK(allow_smem(k_y_pass<R, true, KCY / 2>, smem_y));
@@ -738,6 +762,19 @@ struct Box : BoxBase {
                in, out);
   }
   size_t sm_y_any = 0;
+  bool xsplit_ok(int xs) const override { return xs == 0 || (xs == 1 && g.NX >= 8 && g.NX <= 128); }
+  void set_xsplit(int xs) override {
+    if (xs == xsplit) return;
+    xsplit = xs;
+    // bufA's u_k was formed with the other split; the captured graphs hold
+    // the other launches
+    u_spec_ready = false;
+    for (int s = 0; s < 2; ++s)
+      if (graph[s]) {
+        cudaGraphExecDestroy(graph[s]);
+        graph[s] = nullptr;
+      }
+  }
   bool variant_ok(int zmode, int ymode_) const override {
     if (prm.eq != KAPSEL_EQ_NAVIER_STOKES || zmode < 0 || zmode > 1 || ymode_ < 0 || ymode_ > 3) return false;
     if (zmode == 0 && !zw_avail) return false;
@@ -1996,7 +2033,9 @@ int kapsel_gpu_create(const kapsel_params *p, kapsel_ctx **out) {
   if (!p || !out) return KAPSEL_EINVAL;
   *out = nullptr;
   for (int d = 0; d < 3; ++d)
-    if (p->np_xyz[d] < 4 || p->np_xyz[d] > 9) return KAPSEL_EINVAL;  // 16..512 per axis
+    // 16..256 per axis: the in-kernel transforms factor a line into two
+    // radix-2 networks of at most 16 points
+    if (p->np_xyz[d] < 4 || p->np_xyz[d] > 8) return KAPSEL_EINVAL;
   if (p->eq != KAPSEL_EQ_NAVIER_STOKES && p->eq != KAPSEL_EQ_ELECTROLYTE && p->eq != KAPSEL_EQ_SHEAR_LE)
     return KAPSEL_EINVAL;
   if (p->eq == KAPSEL_EQ_SHEAR_LE && !std::isfinite(p->shear_rate)) return KAPSEL_EINVAL;
@@ -2810,7 +2849,7 @@ struct kapsel_batch {
   cudaEvent_t fork = nullptr, done = nullptr;
   std::vector<cudaEvent_t> ready, join;
   std::vector<std::vector<double>> x0;
-  // the autotuner's choices: NX, NY, NZ, z variant, y variant per shape
+  // the autotuner's choices: NX, NY, NZ, z variant, y variant, x split per shape
   std::vector<std::vector<int>> variants;
 };
 
@@ -2839,29 +2878,39 @@ int kapsel_batch_create(kapsel_ctx *const *boxes, int n, int autotune, kapsel_ba
   // y pass variants, by timing whole steps of the first box of that shape on
   // a copy of its state
   if (autotune) {
-    std::vector<std::pair<std::vector<int>, std::pair<int, int>>> chosen;
+    // per shape: {z variant, y variant, x radix split}
+    std::vector<std::pair<std::vector<int>, std::vector<int>>> chosen;
     for (int i = 0; i < n; ++i) {
       BoxBase *x = b->boxes[i]->box.get();
       if (x->prm.eq != KAPSEL_EQ_NAVIER_STOKES || x->Np == 0) continue;
       std::vector<int> key = {x->g.NX, x->g.NY, x->g.NZ, x->prm.precision, x->Np > 1024 ? 1 : 0};
-      int zp = -1, yp = -1;
+      int zp = -1, yp = -1, xp = 0;
       for (auto &c : chosen)
-        if (c.first == key) zp = c.second.first, yp = c.second.second;
+        if (c.first == key) zp = c.second[0], yp = c.second[1], xp = c.second[2];
       if (zp < 0) {
         float best = 0.f;
-        for (int zm = 0; zm < 2; ++zm)
-          for (int ym = 0; ym < 4; ++ym) {
-            if (!x->variant_ok(zm, ym)) continue;
-            const float t = x->time_variant(zm, ym, 5);
-            if (t > 0.f && (zp < 0 || t < best)) best = t, zp = zm, yp = ym;
-          }
-        if (zp < 0) continue;
-        chosen.push_back({key, {zp, yp}});
+        for (int xs = 0; xs < 2; ++xs) {
+          if (!x->xsplit_ok(xs)) continue;
+          x->set_xsplit(xs);
+          for (int zm = 0; zm < 2; ++zm)
+            for (int ym = 0; ym < 4; ++ym) {
+              if (!x->variant_ok(zm, ym)) continue;
+              const float t = x->time_variant(zm, ym, 5);
+              if (t > 0.f && (zp < 0 || t < best)) best = t, zp = zm, yp = ym, xp = xs;
+            }
+        }
+        if (zp < 0) {
+          x->set_xsplit(0);
+          continue;
+        }
+        chosen.push_back({key, {zp, yp, xp}});
       }
+      x->set_xsplit(xp);
       x->set_variant(zp, yp);
     }
     b->variants.clear();
-    for (auto &c : chosen) b->variants.push_back({c.first[0], c.first[1], c.first[2], c.second.first, c.second.second});
+    for (auto &c : chosen)
+      b->variants.push_back({c.first[0], c.first[1], c.first[2], c.second[0], c.second[1], c.second[2]});
   }
   // initial unwrapped positions for the mean-square displacement
   for (int i = 0; i < n; ++i) {
@@ -2959,6 +3008,15 @@ int kapsel_batch_msd(kapsel_batch *b, double *msd) {
   return 0;
 }
 
+int kapsel_gpu_set_x_split(kapsel_ctx *ctx, int split) {
+  if (!ctx) return KAPSEL_EINVAL;
+  BoxBase *x = ctx->box.get();
+  if (!x->xsplit_ok(split)) return KAPSEL_EINVAL;
+  if (cudaStreamSynchronize(x->stream) != cudaSuccess) return KAPSEL_ECUDA;
+  x->set_xsplit(split);
+  return 0;
+}
+
 int kapsel_gpu_set_pass_variant(kapsel_ctx *ctx, int zmode, int ymode) {
   if (!ctx) return KAPSEL_EINVAL;
   BoxBase *x = ctx->box.get();
@@ -2973,7 +3031,7 @@ int kapsel_batch_variants(kapsel_batch *b, int *out, int cap) {
   if (!b || cap < 0 || (cap > 0 && !out)) return KAPSEL_EINVAL;
   const int n = (int)b->variants.size();
   for (int i = 0; i < n && i < cap; ++i)
-    for (int k = 0; k < 5; ++k) out[5 * i + k] = b->variants[i][k];
+    for (int k = 0; k < 6; ++k) out[6 * i + k] = b->variants[i][k];
   return n;
 }
 

@@ -98,6 +98,21 @@ __device__ __forceinline__ int fft2_n1(int logn) {
   return 1 << (l1 > 4 ? 4 : l1);
 }
 
+// SPLIT = 1 takes the other factorisation of the same length (both factors
+// 2..16): 8 = 2 x 4, 16 = 8 x 2, 32 = 4 x 8, 64 = 16 x 4, 128 = 16 x 8;
+// 256 has only 16 x 16.  Which one is faster depends on the line count and
+// the precision; the batch autotuner times both.
+template <int SPLIT>
+__device__ __forceinline__ int fft2_n1_sel(int logn) {
+  if (SPLIT == 0) return fft2_n1(logn);
+  switch (logn) {
+    case 3: return 2;
+    case 4: return 8;
+    case 5: return 4;
+    default: return 16;
+  }
+}
+
 template <int L, typename R, int SIGN>
 __device__ __forceinline__ void phase1_item(const Cx<R> *data, Cx<R> *scr, int s, int t, int N, int N2, int nseq,
                                             int ss, int es, const Cx<R> *tw) {
@@ -129,11 +144,11 @@ __device__ __forceinline__ void phase2_item(Cx<R> *data, const Cx<R> *scr, int s
 // All threads of the block call it; it ends with a barrier.
 // LOGN > 0 fixes the length at compile time (constant indexing and loop
 // bounds); LOGN = 0 takes it from logn_rt.
-template <typename R, int SIGN, int NSEQ, int LOGN = 0>
+template <typename R, int SIGN, int NSEQ, int LOGN = 0, int SPLIT = 0>
 __device__ __forceinline__ void fft2_smem(Cx<R> *data, Cx<R> *scr, int logn_rt, int ss, int es, const Cx<R> *tw) {
   const int logn = LOGN > 0 ? LOGN : logn_rt;
   const int N = 1 << logn;
-  const int N1 = fft2_n1(logn), N2 = N / N1;
+  const int N1 = fft2_n1_sel<SPLIT>(logn), N2 = N / N1;
   for (int it = threadIdx.x; it < NSEQ * N2; it += blockDim.x) {
     const int s = it % NSEQ, t = it / NSEQ;
     switch (N1) {

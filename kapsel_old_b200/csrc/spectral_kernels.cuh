@@ -92,7 +92,7 @@ __device__ __forceinline__ void select_zeta(int KXi, int KYi, const Cx<R> w[3], 
 // ---------------------------------------------------------------------------
 // x pass, inverse: zeta -> u_k (Zeta_k2u_k) -> inverse x transform.
 // grid (KYc, ceil(TZ/KC)), out I1[3][NX][KYc][TZ].
-template <typename R, int KC, int LX = 0>
+template <typename R, int KC, int LX = 0, int XS = 0>
 __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, const Cx<R> *__restrict__ zeta,
                                                      const double *__restrict__ uk_dc, Cx<R> *__restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(256) k_x_zeta_to_u(Geo g, Twiddles<R> tw, cons
     U[i * W + 2 * KC + col] = u[2];
   }
   __syncthreads();
-  fft2_smem<R, -1, W, LX>(U, scr, LXv, 1, W, twx);
+  fft2_smem<R, -1, W, LX, XS>(U, scr, LXv, 1, W, twx);
   for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
     if (col < ncol)
@@ -495,7 +495,7 @@ __device__ __forceinline__ void advect_mode_update(const Geo &g, int KXi, int KY
 // NSsolute_solver_Euler (Add_zeta_viscous_term then Field_solver_Euler,
 // fluid_solver.cxx:122-135, operate_omega.cxx:172-184) instead of the slaved
 // step, and no u* output (the electrolyte rebuilds u after the Coulomb force).
-template <typename R, int KC, int EULER = 0, int LX = 0>
+template <typename R, int KC, int EULER = 0, int LX = 0, int XS = 0>
 __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ buf,
                                                          Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
   }
   cp_async_wait_all();
   __syncthreads();
-  fft2_smem<R, 1, W5, LX>(Pb, scr, LXv, 1, W5, twx);
+  fft2_smem<R, 1, W5, LX, XS>(Pb, scr, LXv, 1, W5, twx);
   const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
   const R ky = R(g.wave[1] * KYi);
   for (int it = threadIdx.x; it < g.KXc * KC; it += blockDim.x) {
@@ -581,7 +581,7 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
     Pb[i * W3 + 2 * KC + col] = u[2];
   }
   __syncthreads();
-  fft2_smem<R, -1, W3, LX>(Pb, scr, LXv, 1, W3, twx);
+  fft2_smem<R, -1, W3, LX, XS>(Pb, scr, LXv, 1, W3, twx);
   for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
     if (col < ncol) buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col] = Pb[x * W3 + c * KC + col];
@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
 // u_k = Zeta_k2u_k(zeta, uk_dc) of the updated values and the inverse x
 // transform, written over buf (as k_x_zeta_to_u writes it, with the same
 // arithmetic), so the next step starts at its y pass.
-template <typename R, int KC, int LX = 0, int NEXTU = 0>
+template <typename R, int KC, int LX = 0, int NEXTU = 0, int XS = 0>
 __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, Cx<R> *__restrict__ buf,
                                                          Cx<R> *__restrict__ zeta, double *__restrict__ uk_dc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -632,7 +632,7 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
   load_twiddles(twx, tw.x, NXv);
   cp_async_wait_all();
   __syncthreads();
-  fft2_smem<R, 1, W3, LX>(Pb, scr, LXv, 1, W3, twx);
+  fft2_smem<R, 1, W3, LX, XS>(Pb, scr, LXv, 1, W3, twx);
   const int KYi = signed_k(full_from_compact(iy, g.TY, g.KYc, g.NY), g.NY);
   const R ky = R(g.wave[1] * KYi);
   for (int it = threadIdx.x; it < g.KXc * KC; it += blockDim.x) {
@@ -701,7 +701,7 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
     Pb[i * W3 + 2 * KC + col] = u[2];
   }
   __syncthreads();
-  fft2_smem<R, -1, W3, LX>(Pb, scr, LXv, 1, W3, twx);
+  fft2_smem<R, -1, W3, LX, XS>(Pb, scr, LXv, 1, W3, twx);
   for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
     const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
     if (col < ncol) buf[(((size_t)c * NXv + x) * g.KYc + iy) * g.TS + kz0 + col] = Pb[x * W3 + c * KC + col];

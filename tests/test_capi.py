@@ -86,8 +86,10 @@ def test_invalid_arguments_rejected_without_gpu(lib):
     assert L.kapsel_gpu_create(None, None) == -1
     p = kg._Params()
     L.kapsel_params_default(ctypes.byref(p))
-    p.np_xyz[0] = 3  # grids are 16..512 per axis
+    p.np_xyz[0] = 3  # grids are 16..256 per axis
     h = ctypes.c_void_p()
+    assert L.kapsel_gpu_create(ctypes.byref(p), ctypes.byref(h)) == -1
+    p.np_xyz[0] = 9  # 512-point lines are beyond the in-kernel transforms
     assert L.kapsel_gpu_create(ctypes.byref(p), ctypes.byref(h)) == -1
     # NaN, Inf and out-of-range physical parameters are refused before any
     # device call (the reference would run on and produce NaN fields)

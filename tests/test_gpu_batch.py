@@ -101,6 +101,36 @@ def test_batch_pass_variants_match():
     ref.close()
 
 
+@pytest.mark.parametrize("shape", [(5, 5, 6), (6, 6, 7), (7, 7, 7), (6, 5, 6)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_x_split_matches_default(shape, precision):
+    """The other radix split of the block-level x transforms (32 = 4 x 8,
+    64 = 16 x 4, 128 = 16 x 8), which the batch autotuner may choose, gives
+    the same steps to roundoff (FP64 1e-12, mixed 1e-5); 256-point x lines
+    have no other split."""
+    import ctypes
+
+    import kapsel_old_b200 as kg
+
+    prec = kg.FP64 if precision == "fp64" else kg.MIXED
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    cfg = udf.ns_config(shape, 4, seed=26, a=5.0, kbt=1e-3)
+    a = kg.Simulation(cfg, precision=prec)
+    b = kg.Simulation(cfg, precision=prec)
+    fn = b.L.kapsel_gpu_set_x_split
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    assert fn(b.h, 1) == 0
+    a.step(4)
+    b.step(4, graph=True)
+    assert 0 < rel(b.zeta(), a.zeta()) < tol
+    assert rel(b.particles()["v"], a.particles()["v"]) < tol
+    a.close()
+    b.close()
+    big = kg.Simulation(udf.ns_config((8, 5, 5), 1, seed=27, a=5.0), precision=kg.FP64)
+    assert fn(big.h, 1) == -1
+    big.close()
+
+
 def _set_variant(sim, zmode, ymode):
     import ctypes
 
