@@ -14,7 +14,7 @@ with CUDA events on the library's stream; the state is device resident.
 `e2e` repeats K steps through the public C ABI with the per-step host work
 (thermostat normals generated on the host and copied in, particle records
 copied out) inside a wall-clock timed region.  Under torchrun each rank runs
-an independent replica (the north-star path is single-GPU: replicas only);
+an independent replica (the SPM step runs on one GPU: replicas only);
 the timed region is bracketed by a barrier and the max over ranks is used.
 
 Reference arm: the unmodified KAPSEL sources built by oracle/Makefile
