@@ -636,7 +636,10 @@ def run_reference(args, world: int = 1):
         "dtype": "f64",
         "data": "synthetic (seeded positions, PCG64 seed 2; MT19937 seed 0 thermostat)",
         "config": {"workload": WORKLOAD, "grid": [128, 128, 128], "particles": 256,
-                   "precision": "reference FP64 CPU"},
+                   "precision": "reference FP64 CPU",
+                   "l2": "no flush (host CPU run)",
+                   "parallelism": f"OpenMP on {cb['cores']} host cores",
+                   "cuda_graph": False},
         "cpu_baseline": cb,
         "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
