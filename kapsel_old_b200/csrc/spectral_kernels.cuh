@@ -483,6 +483,37 @@ __device__ __forceinline__ void advect_mode_update(const Geo &g, int KXi, int KY
 }
 
 // ---------------------------------------------------------------------------
+// Row tiles of the x passes move KC consecutive kz values per row.  With float
+// complex values a pair is one 16-byte transfer when both addresses are
+// 16-byte aligned (always, for the layouts here: row strides, plane strides
+// and kz0 are multiples of four values), else two 8-byte ones; `left` is the
+// number of values of the row that exist from this pair on (values past the
+// retained columns are zero-filled in shared memory, never read or written in
+// global memory).
+template <typename R>
+__device__ __forceinline__ bool aligned16(const void *a, const void *b) {
+  return ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 15u) == 0;
+}
+template <typename R>
+__device__ __forceinline__ void stage_pair(Cx<R> *d, const Cx<R> *s, int left) {
+  if (left >= 2 && aligned16<R>(d, s)) {
+    cp_async_16(d, s);
+    return;
+  }
+  if (left >= 1) cp_async_cx(d, s); else d[0] = {R(0), R(0)};
+  if (left >= 2) cp_async_cx(d + 1, s + 1); else d[1] = {R(0), R(0)};
+}
+template <typename R>
+__device__ __forceinline__ void store_pair(Cx<R> *o, const Cx<R> *p, int left) {
+  if (left >= 2 && aligned16<R>(o, p)) {
+    *reinterpret_cast<float4 *>(o) = *reinterpret_cast<const float4 *>(p);
+    return;
+  }
+  if (left >= 1) o[0] = p[0];
+  if (left >= 2) o[1] = p[1];
+}
+
+// ---------------------------------------------------------------------------
 // x pass, forward, of the five product spectra fused with the rest of
 // NS_solver_slavedEuler (fluid_solver.cxx:328-354) and the next inverse:
 //   Omega from the product spectra (operate_omega.cxx:60-97), its reduction
@@ -513,17 +544,30 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
   const size_t cstr = (size_t)NXv * g.KYc * g.TS;
   const size_t zplane = (size_t)g.KXc * g.KYc * g.TS;
   // stage the five product spectra (bit-reversed rows) and the zeta tile
-  for (int it = threadIdx.x; it < 5 * NXv * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
-    Cx<R> *d = Pb + x * W5 + c * KC + col;
-    if (col < ncol)
-      cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col);
-    else
-      *d = {R(0), R(0)};
-  }
-  for (int it = threadIdx.x; it < 2 * g.KXc * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
-    if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
+  if constexpr (sizeof(R) == 4 && KC % 2 == 0) {
+    constexpr int KP = KC / 2;
+    for (int it = threadIdx.x; it < 5 * NXv * KP; it += blockDim.x) {
+      const int col = 2 * (it % KP), rest = it / KP, x = rest & (NXv - 1), c = rest >> LXv;
+      stage_pair(Pb + x * W5 + c * KC + col, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col,
+                 ncol - col);
+    }
+    for (int it = threadIdx.x; it < 2 * g.KXc * KP; it += blockDim.x) {
+      const int col = 2 * (it % KP), rest = it / KP, ix = rest % g.KXc, c = rest / g.KXc;
+      stage_pair(Zs + rest * KC + col, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col, ncol - col);
+    }
+  } else {
+    for (int it = threadIdx.x; it < 5 * NXv * KC; it += blockDim.x) {
+      const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
+      Cx<R> *d = Pb + x * W5 + c * KC + col;
+      if (col < ncol)
+        cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col);
+      else
+        *d = {R(0), R(0)};
+    }
+    for (int it = threadIdx.x; it < 2 * g.KXc * KC; it += blockDim.x) {
+      const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
+      if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
+    }
   }
   load_twiddles(twx, tw.x, NXv);
   const bool has_k0 = (iy == 0 && blockIdx.y == 0);
@@ -582,9 +626,18 @@ __global__ void __launch_bounds__(256) k_x_advect_update(Geo g, Twiddles<R> tw, 
   }
   __syncthreads();
   fft2_smem<R, -1, W3, LX, XS>(Pb, scr, LXv, 1, W3, twx);
-  for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
-    if (col < ncol) buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col] = Pb[x * W3 + c * KC + col];
+  if constexpr (sizeof(R) == 4 && KC % 2 == 0) {
+    constexpr int KP = KC / 2;
+    for (int it = threadIdx.x; it < 3 * NXv * KP; it += blockDim.x) {
+      const int col = 2 * (it % KP), rest = it / KP, x = rest & (NXv - 1), c = rest >> LXv;
+      store_pair(buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col, Pb + x * W3 + c * KC + col,
+                 ncol - col);
+    }
+  } else {
+    for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
+      const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
+      if (col < ncol) buf[c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col] = Pb[x * W3 + c * KC + col];
+    }
   }
 }
 
@@ -617,17 +670,30 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
   const int ncol = min(KC, g.TZ - kz0);
   const size_t cstr = (size_t)NXv * g.KYc * g.TS;
   const size_t zplane = (size_t)g.KXc * g.KYc * g.TS;
-  for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
-    Cx<R> *d = Pb + x * W3 + c * KC + col;
-    if (col < ncol)
-      cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col);
-    else
-      *d = {R(0), R(0)};
-  }
-  for (int it = threadIdx.x; it < 2 * g.KXc * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
-    if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
+  if constexpr (sizeof(R) == 4 && KC % 2 == 0) {
+    constexpr int KP = KC / 2;
+    for (int it = threadIdx.x; it < 3 * NXv * KP; it += blockDim.x) {
+      const int col = 2 * (it % KP), rest = it / KP, x = rest & (NXv - 1), c = rest >> LXv;
+      stage_pair(Pb + x * W3 + c * KC + col, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col,
+                 ncol - col);
+    }
+    for (int it = threadIdx.x; it < 2 * g.KXc * KP; it += blockDim.x) {
+      const int col = 2 * (it % KP), rest = it / KP, ix = rest % g.KXc, c = rest / g.KXc;
+      stage_pair(Zs + rest * KC + col, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col, ncol - col);
+    }
+  } else {
+    for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
+      const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
+      Cx<R> *d = Pb + x * W3 + c * KC + col;
+      if (col < ncol)
+        cp_async_cx(d, buf + c * cstr + ((size_t)x * g.KYc + iy) * g.TS + kz0 + col);
+      else
+        *d = {R(0), R(0)};
+    }
+    for (int it = threadIdx.x; it < 2 * g.KXc * KC; it += blockDim.x) {
+      const int col = it % KC, rest = it / KC, ix = rest % g.KXc, c = rest / g.KXc;
+      if (col < ncol) cp_async_cx(Zs + it, zeta + c * zplane + ((size_t)ix * g.KYc + iy) * g.TS + kz0 + col);
+    }
   }
   load_twiddles(twx, tw.x, NXv);
   cp_async_wait_all();
@@ -702,9 +768,18 @@ __global__ void __launch_bounds__(256) k_x_force_to_zeta(Geo g, Twiddles<R> tw, 
   }
   __syncthreads();
   fft2_smem<R, -1, W3, LX, XS>(Pb, scr, LXv, 1, W3, twx);
-  for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
-    const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
-    if (col < ncol) buf[(((size_t)c * NXv + x) * g.KYc + iy) * g.TS + kz0 + col] = Pb[x * W3 + c * KC + col];
+  if constexpr (sizeof(R) == 4 && KC % 2 == 0) {
+    constexpr int KP = KC / 2;
+    for (int it = threadIdx.x; it < 3 * NXv * KP; it += blockDim.x) {
+      const int col = 2 * (it % KP), rest = it / KP, x = rest & (NXv - 1), c = rest >> LXv;
+      store_pair(buf + (((size_t)c * NXv + x) * g.KYc + iy) * g.TS + kz0 + col, Pb + x * W3 + c * KC + col,
+                 ncol - col);
+    }
+  } else {
+    for (int it = threadIdx.x; it < 3 * NXv * KC; it += blockDim.x) {
+      const int col = it % KC, rest = it / KC, x = rest & (NXv - 1), c = rest >> LXv;
+      if (col < ncol) buf[(((size_t)c * NXv + x) * g.KYc + iy) * g.TS + kz0 + col] = Pb[x * W3 + c * KC + col];
+    }
   }
 }
 
