@@ -254,3 +254,26 @@ def test_native_reader_reads_output_records(tmp_path):
         assert set(flat) == set(b)
         for k, x in flat.items():
             assert float(b[k]) == float(x), k
+
+
+def test_native_reader_refuses_malformed_input(tmp_path):
+    """Host-side fault injection on the UDF boundary: a missing file, a
+    truncated file and an input that lacks the keys of the step are refused
+    with a status (the reference would exit or read garbage); nothing
+    crashes."""
+    import kapsel_old_b200 as kg
+
+    with pytest.raises(kg.KapselError):
+        kg.read_udf_native(str(tmp_path / "missing.udf"))
+    src = _examples()[0]
+    text = open(src).read()
+    cut = tmp_path / "truncated.udf"
+    cut.write_text(text[: len(text) // 2])
+    try:
+        kg.read_udf_native(str(cut))  # either a status or a (partial) record set
+    except kg.KapselError:
+        pass
+    empty = tmp_path / "empty.udf"
+    empty.write_text("\\begin{data}\n\\end{data}\n")
+    with pytest.raises(kg.KapselError):
+        kg.params_from_udf_native(str(empty))
