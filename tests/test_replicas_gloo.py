@@ -57,3 +57,46 @@ def test_two_gloo_replicas_reduce_max():
     assert out[0][0] == out[1][0] == 2.0          # both ranks see the slowest rank's time
     assert out[0][1] == out[1][1] == 2 * world / 2.0  # all ranks' steps over the max time
     assert out[0][2] != out[1][2]                  # the replicas advanced different boxes
+
+
+def _worker_fail(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    import bench
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    dist.barrier()
+    if rank == 1:
+        # a replica that fails between steps: it leaves without taking part in
+        # the timing reduction
+        os._exit(3)
+    try:
+        bench.reduce_max(1.0, dist, device="cpu")
+        out[rank] = "completed"
+    except Exception as e:  # the short process-group timeout ends the wait
+        out[rank] = f"error: {type(e).__name__}"
+    os._exit(0)
+
+
+def test_failed_replica_ends_the_others_wait_with_an_error():
+    """Failure detection on the host: when one replica exits between steps,
+    the surviving rank's next collective (the max-over-ranks reduction of the
+    timing) ends with an error after the process group's short timeout
+    instead of waiting forever."""
+    world = 2
+    mgr = mp.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_worker_fail, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert procs[1].exitcode == 3
+    assert procs[0].exitcode == 0
+    assert str(out.get(0, "")).startswith("error"), out.get(0)
