@@ -154,7 +154,16 @@ class NvmlClockSampler:
 
         self.nv = pynvml
         pynvml.nvmlInit()
-        self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+        # the CUDA device's own GPU (by PCI address: NVML counts all GPUs of
+        # the node, CUDA only the visible ones), else NVML's device `index`
+        try:
+            import torch
+
+            pr = torch.cuda.get_device_properties(index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
         self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
         self.sm, self.bits, self.stop_ev, self.t = [], 0, None, None
 
