@@ -99,3 +99,49 @@ def test_invalid_arguments_rejected_without_gpu(lib):
         L.kapsel_params_default(ctypes.byref(q))
         setattr(q, name, value)
         assert L.kapsel_gpu_create(ctypes.byref(q), ctypes.byref(h)) == -1, name
+
+
+C_CALLER = r"""
+#include <stdio.h>
+#include <string.h>
+#include "kapsel_gpu.h"
+
+/* A plain C caller of the C ABI: the calls that need no GPU. */
+int main(void) {
+  kapsel_params p;
+  kapsel_ctx *ctx = NULL;
+  kapsel_udf *u = NULL;
+  kapsel_params_default(&p);
+  if (p.np_xyz[0] != 6 || !(p.dt > 0.0)) return 1;
+  p.dt = -1.0;
+  if (kapsel_gpu_create(&p, &ctx) != KAPSEL_EINVAL || ctx != NULL) return 2;
+  if (strlen(kapsel_gpu_strerror(KAPSEL_ETIMEOUT)) == 0) return 3;
+  if (kapsel_udf_read("/nonexistent/input.udf", &u) == 0) return 4;
+  printf("ok\n");
+  return 0;
+}
+"""
+
+
+def test_header_is_a_plain_c_interface(tmp_path):
+    """include/kapsel_gpu.h compiles as strict C99 (no C++ in the interface)
+    and a C program links against the library and calls it; the calls used
+    here need no GPU."""
+    import shutil
+    import subprocess
+
+    import kapsel_old_b200 as kg
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    src = tmp_path / "caller.c"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(kg.LIB_PATH)
+    inc = os.path.join(os.path.dirname(libdir), "include")
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", inc, str(src), "-L", libdir,
+                        "-lkapsel_gpu", f"-Wl,-rpath,{libdir}", "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout, r.stderr)
